@@ -1,0 +1,324 @@
+#!/usr/bin/env python
+"""Benchmark: SPH fluid particle-steps/s of the plain f64 WCSPH step on B200.
+
+Workload (default, `dam_break_1m`): the synthetic 3-D dam break at 1M fluid
+particles — a 100^3 lattice at dx = 0.01 m with seeded +-1e-4 m jitter in a
+4.0 x 1.6 x 2.4 m tank walled by a 1-layer Akinci shell (396,802 boundary
+samples); cubic spline h = 2 dx, rho0 = 1000, Tait gamma = 7 with a fixed
+c0 = 20 m/s, alpha = 0.01, XSPH 0.25, g = -9.81 z, dt = 1e-4 s. One "step" is
+one `WcsphWorld::step` (crates/pe-fluid/src/wcsph.rs:326) of the whole tank.
+Counted units are fluid particles x steps.
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+N > 1 runs under torch.distributed (one process per GPU); each rank advances
+its own independent tank (weak scaling, no data-path collective) and the
+job's value is the sum over ranks with the max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "physics-engine_b200"))
+
+METRIC = "SPH fluid particle-steps/s @1M (plain f64 WCSPH step)"
+UNIT = "particle-steps/s"
+
+WORKLOADS = {
+    # name: (fluid lattice nx, ny, nz), tank extent
+    "dam_break_1m": ((100, 100, 100), (4.0, 1.6, 2.4)),
+    # 160 x 0.01 from origin dx puts the top fluid row on the y = 1.60 wall; the
+    # tank grows to 1.62 m in y.
+    "dam_break_4m": ((160, 160, 160), (4.0, 1.62, 2.4)),
+    "dam_break_32k": ((32, 32, 32), (1.0, 0.4, 0.6)),
+}
+DX, DT, SEED, JITTER = 0.01, 1e-4, 0x5EED5EED, 1e-4
+
+# Algorithmic HBM bytes per fluid particle of the fused force + kick + drift
+# pass: read x, v, rho (56 B), write x, v (48 B).
+FORCE_BYTES_PER_FLUID = 104.0
+# Whole step, per fluid / per boundary particle (cell key 28 + sort 8 +
+# density 32 + XSPH 80 + forces 104; boundary 28 + 8 + 3 x 24).
+STEP_BYTES_FLUID, STEP_BYTES_BOUNDARY = 252.0, 108.0
+
+
+def _args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="dam_break_1m")
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def _peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def build_scene(pe, workload):
+    (nx, ny, nz), box = WORKLOADS[workload]
+    mass = pe.mass_from_spacing(1000.0, DX, 3)
+    p = pe.Particles(3, 1000.0, mass, 2.0 * DX)
+    p.fill_box((DX, DX, DX), nx, ny, nz, DX)
+    p.jitter_fluid(SEED, JITTER)
+    p.fill_box_boundary((0.0, 0.0, 0.0), box, DX, 1)
+    prm = pe.WcsphParams.water(1000.0, 20.0, (0.0, 0.0, -9.81))
+    prm.adapt_sound_speed = False
+    return p, prm, nx * ny * nz
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        try:
+            for line in open(self.path):
+                parts = [t.strip() for t in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    mx.append(float(parts[2]))
+                except ValueError:
+                    continue
+                for nm, val in zip(names, parts[5:9]):
+                    if val.lower().startswith("active"):
+                        reasons.add(nm)
+            os.unlink(self.path)
+        except Exception:
+            pass
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_baseline(steps=5):
+    """The oracle (CPU port of the reference step), single-threaded, on a bounded
+    sample: the 32^3 dam break (same dx, h, physics) for `steps` steps."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    s = O.dam_break_scene(32)
+    w = O.World(s, O.dam_break_params(materialize=True))
+    w.step(DT)  # first step outside the timing (allocation of neighbour lists)
+    t0 = time.perf_counter()
+    w.run(DT, steps)
+    sec = time.perf_counter() - t0
+    nf = 32 ** 3
+    return {"value": nf * steps / sec, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"32^3 dam break (32,768 fluid + 24,802 boundary, dx 0.01, h 2dx), {steps} "
+                      f"steps of the single-threaded C++ restatement of WcsphWorld::step, "
+                      f"-O2 -ffp-contract=off, neighbour lists materialised as the reference; "
+                      f"{sec:.1f} s",
+            "host_cpus": os.cpu_count()}
+
+
+def run_reference(args, ws, rank):
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    s = O.dam_break_scene(32)
+    w = O.World(s, O.dam_break_params(materialize=True))
+    for _ in range(args.warmup):
+        w.step(DT)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        w.step(DT)
+    sec = time.perf_counter() - t0
+    nf = 32 ** 3
+    value = nf * args.steps / sec
+    sample = ("one step of the 32^3 dam break per bench step (32,768 fluid + 24,802 boundary, "
+              "same dx, h and physics as the 1M tank); oracle port of WcsphWorld::step, single "
+              "thread (the reference path is single-threaded by design, docs/FLUID.md:104)")
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * sec / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": args.workload, "sample": "dam_break_32k"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = _args()
+    ws, rank, local = _dist()
+    if args.impl == "reference":
+        run_reference(args, ws, rank)
+        return
+
+    import numpy as np
+    import torch
+
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    import physics_engine_rs as pe
+
+    ps, prm, nf = build_scene(pe, args.workload)
+    nb = len(ps) - nf
+    world = pe.WcsphWorld(ps, prm, pe.WcsphConfig(device=local))
+    del ps
+    stream = torch.cuda.ExternalStream(world.stream_handle(), device=local)
+
+    world.run(DT, max(args.warmup, 3))
+    torch.cuda.synchronize()
+
+    def barrier():
+        if ws > 1:
+            torch.distributed.barrier()
+
+    # ---- device-timed region ----
+    sampler = ClockSampler(local)
+    sampler.start()
+    world.set_profiling(True)
+    world.profile(reset=True)
+    world.kernel_launches(reset=True)
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    start.record(stream)
+    world.run(DT, args.steps)
+    end.record(stream)
+    end.synchronize()
+    torch.cuda.synchronize()
+    barrier()
+    ms = start.elapsed_time(end)
+    launches = world.kernel_launches()
+    prof = world.profile(reset=True)
+    world.set_profiling(False)
+    clocks = sampler.stop()
+    status = world.status()
+    if ws > 1:
+        t = torch.tensor([ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    value = ws * nf * args.steps / (ms / 1e3)
+
+    # ---- end-to-end through the public API with host buffers ----
+    x_h = torch.empty((world.n, 3), dtype=torch.float64, pin_memory=True).numpy()
+    v_h = torch.empty((world.n, 3), dtype=torch.float64, pin_memory=True).numpy()
+    x_h[:] = world.positions()
+    v_h[:] = world.velocities()
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        world.set_positions(x_h)
+        world.set_velocities(v_h)
+        world.step(DT)
+        x_h[:] = world.positions()
+        v_h[:] = world.velocities()
+    torch.cuda.synchronize()
+    e2e_sec = time.perf_counter() - t0
+    if ws > 1:
+        t = torch.tensor([e2e_sec], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_sec = float(t.item())
+    e2e = ws * nf * args.e2e_steps / e2e_sec
+    io_bytes = 2 * world.n * 24
+
+    hbm_peak, peak_kind = _peaks()
+    f_ms, f_n = prof["forces"]
+    achieved = FORCE_BYTES_PER_FLUID * nf * f_n / (f_ms / 1e3) / 1e9 if f_ms > 0 else 0.0
+    total_prof = sum(v[0] for v in prof.values())
+    step_bytes = STEP_BYTES_FLUID * nf + STEP_BYTES_BOUNDARY * nb
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "fluid_particles": nf, "boundary_particles": nb,
+                   "dx": DX, "dt": DT, "h_over_dx": 2.0, "sound_speed": 20.0,
+                   "adapt_sound_speed": False, "xsph": 0.25, "visc_alpha": 0.01,
+                   "parallelism": f"{ws} independent tank(s), one per GPU",
+                   "l2": "state + neighbour lists (> 2 GB) exceed the 126 MB L2; no flush needed"},
+        "gpu_launches": int(launches),
+        "status": int(status),
+        "phases_ms_per_step": {k: v[0] / max(1, args.steps) for k, v in prof.items()},
+        "roofline": {"bound": "hbm", "kernel": "k_forces (force + kick + drift)",
+                     "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                     "frac": achieved / hbm_peak, "peak_kind": peak_kind, "traffic": None,
+                     "bytes_per_unit": FORCE_BYTES_PER_FLUID, "units_per_launch": nf,
+                     "launch_ms": f_ms / max(1, f_n),
+                     "note": "algorithmic bytes; the pass is FP64-ALU bound, not HBM bound"},
+        "step_roofline": {"algorithmic_bytes_per_step": step_bytes,
+                          "achieved_gbs": step_bytes / (ms / args.steps / 1e3) / 1e9,
+                          "profiled_ms_per_step": total_prof / max(1, args.steps)},
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": io_bytes,
+                "d2h_bytes_per_step": io_bytes, "steps": args.e2e_steps,
+                "pattern": "set_positions + set_velocities from pinned host buffers, step, "
+                           "get_positions + get_velocities (state round-trips through the host)"},
+        "clocks": clocks,
+    }
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline()
+    world.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

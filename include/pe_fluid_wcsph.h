@@ -1,0 +1,243 @@
+/*
+ * pe_fluid_wcsph.h — C ABI of the B200 WCSPH fluid step.
+ *
+ * Drop-in for the WCSPH solver path of eranyid/physics-engine's `pe-fluid`
+ * crate. The reference exposes that path only as a Rust API
+ * (`WcsphWorld`, crates/pe-fluid/src/wcsph.rs:58-370, and the particle
+ * builders of crates/pe-fluid/src/particles.rs); its C ABI crate `pe-ffi`
+ * (crates/pe-ffi/src/lib.rs) exports rigid-body worlds only. This header is
+ * the C surface a `pe-ffi`-style binding of the fluid path binds, following
+ * pe-ffi's conventions (docs/FFI.md:7-35):
+ *   - opaque handles, `int` return codes with the same integers as
+ *     crates/pe-ffi/src/error.rs:4-16 (one code added: PE_ERR_DEVICE);
+ *   - no exception/unwind crosses the boundary (crates/pe-ffi/src/lib.rs:68-80);
+ *   - non-finite inputs and dt <= 0 give PE_ERR_ARG, short buffers give
+ *     PE_ERR_BOUNDS, null required pointers give PE_ERR_NULL;
+ *   - caller-owned host buffers; getters and setters never allocate host
+ *     memory for the caller; device memory is owned by the handle;
+ *   - one owner thread per handle, no internal mutex.
+ *
+ * Arrays are in the original particle order (the order particles were pushed);
+ * vectors are `[n*3]` interleaved (x0, y0, z0, x1, ...), like
+ * `Particles::pack_positions` (particles.rs:137).
+ */
+#ifndef PE_FLUID_WCSPH_H
+#define PE_FLUID_WCSPH_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+/* Return codes (crates/pe-ffi/src/error.rs:4-16). */
+#define PE_OK 0
+#define PE_ERR_NULL 1
+#define PE_ERR_BOUNDS 2
+#define PE_ERR_ARG 3
+#define PE_ERR_PANIC 4
+#define PE_ERR_SCENE 5
+#define PE_ERR_UNSUPPORTED 6
+#define PE_ERR_DEVICE 7 /* added: a CUDA runtime call failed */
+
+/* Sticky status bits reported by pe_fluid_wcsph_status. */
+#define PE_STATUS_DOMAIN 1u            /* a particle left the dense grid domain */
+#define PE_STATUS_NEIGHBOUR_OVERFLOW 2u /* a neighbour list reached its capacity */
+#define PE_STATUS_NONFINITE 4u          /* a non-finite position reached the grid */
+#define PE_STATUS_SLOW_UNION 8u         /* informational: a cell took the slow list path */
+
+/* Dim (crates/pe-fluid/src/lib.rs:202). */
+#define PE_DIM_2 2
+#define PE_DIM_3 3
+
+/* KernelKind (crates/pe-fluid/src/kernels.rs:19); the WCSPH path supports the
+ * cubic spline, the reference's default (wcsph.rs:45). */
+#define PE_KERNEL_CUBIC_SPLINE 0
+
+/* ParticleKind (crates/pe-fluid/src/particles.rs:11). */
+#define PE_PARTICLE_FLUID 0
+#define PE_PARTICLE_BOUNDARY 1
+
+/* WcsphParams (crates/pe-fluid/src/wcsph.rs:24-39) flattened:
+ * TaitEos (eos.rs:32), MonaghanViscosity (viscosity.rs:30), Xsph
+ * (viscosity.rs:77), gravity, adapt_sound_speed, surface tension sigma
+ * (must be 0: the surface-tension branch, wcsph.rs:262, is not provided). */
+typedef struct PeWcsphParams {
+    int32_t density_kernel;
+    double eos_rest_density;
+    double eos_sound_speed;
+    double eos_gamma;
+    double visc_alpha;
+    double visc_beta;
+    double visc_eps;
+    double xsph_epsilon;
+    double gravity[3];
+    int32_t adapt_sound_speed;
+    double surface_tension_sigma;
+} PeWcsphParams;
+
+/* GPU placement and capacities (no reference counterpart; zeros = defaults). */
+typedef struct PeWcsphConfig {
+    int32_t device;               /* CUDA device ordinal; -1 = the current device */
+    uint32_t max_neighbours;      /* per-particle in-support list capacity (0 = 512) */
+    uint32_t max_lower;           /* lower-index list capacity (0 = max_neighbours) */
+    double domain_margin;         /* grid domain growth per side, fraction of extent (<0 = 0.25) */
+    uint32_t domain_margin_cells; /* minimum growth per side in cells (0 = 4) */
+} PeWcsphConfig;
+
+/* Conservation / error reductions (crates/pe-fluid/src/diagnostics.rs:35-102,
+ * wcsph.rs:350-369), computed in f64. */
+typedef struct PeFluidDiagnostics {
+    double total_mass;
+    double linear_momentum[3];
+    double kinetic_energy;
+    double gravitational_potential; /* m g z with g = -gravity.z */
+    double mean_density_error;
+    double max_density_error;
+    double v_max;
+    double a_max;
+    uint64_t hash64; /* particles_hash64 (diagnostics.rs:19) */
+} PeFluidDiagnostics;
+
+typedef struct PeParticles PeParticles; /* host-side Particles builder */
+typedef struct PeWcsph PeWcsph;         /* one WCSPH world on one GPU */
+
+/* ---- Particles (crates/pe-fluid/src/particles.rs) ---- */
+
+/* Particles::new (particles.rs:52). Returns NULL on bad arguments. */
+PeParticles* pe_fluid_particles_new(int32_t dim, double rest_density, double mass, double h);
+void pe_fluid_particles_free(PeParticles* p);
+int pe_fluid_particles_len(const PeParticles* p, uint64_t* out_len);
+/* push_fluid (particles.rs:90) */
+int pe_fluid_particles_push_fluid(PeParticles* p, const double x[3], const double v[3]);
+/* push_boundary (particles.rs:102) / push_boundary_oriented (particles.rs:107) */
+int pe_fluid_particles_push_boundary(PeParticles* p, const double x[3], double psi);
+int pe_fluid_particles_push_boundary_oriented(PeParticles* p, const double x[3], double psi,
+                                              const double n_out[3]);
+/* fill_box (particles.rs:220) */
+int pe_fluid_fill_box(PeParticles* p, const double origin[3], uint64_t nx, uint64_t ny, uint64_t nz,
+                      double dx, const double v0[3]);
+/* fill_box_boundary (particles.rs:286) */
+int pe_fluid_fill_box_boundary(PeParticles* p, const double min[3], const double max[3], double dx,
+                               uint64_t layers);
+/* recomputed_akinci_psi (particles.rs:252), same summation order. */
+int pe_fluid_recomputed_akinci_psi(PeParticles* p, int32_t kernel);
+/* Seeded lattice jitter of the fluid particles: xoshiro256** (pe-math
+ * rng.rs:14-72) seeded with `seed`, draws in particle order, x then y (then z
+ * in 3-D), each U(-amplitude, amplitude), added to the position. */
+int pe_fluid_particles_jitter_fluid(PeParticles* p, uint64_t seed, double amplitude);
+/* Copy out SoA arrays (any pointer may be NULL); n must equal the length. */
+int pe_fluid_particles_export(const PeParticles* p, double* x, double* v, uint8_t* kind, double* psi,
+                              double* n_out, uint64_t n);
+/* mass_from_spacing (particles.rs:166), mass_calibrated_to_rest (particles.rs:178). */
+double pe_fluid_mass_from_spacing(double rest_density, double dx, int32_t dim);
+double pe_fluid_mass_calibrated_to_rest(double rest_density, double dx, double h, int32_t dim,
+                                        int32_t kernel);
+
+/* ---- WCSPH world (crates/pe-fluid/src/wcsph.rs) ---- */
+
+/* WcsphParams::water (wcsph.rs:43-53). */
+int pe_fluid_wcsph_params_water(double rest_density, double sound_speed, const double gravity[3],
+                                PeWcsphParams* out);
+/* WcsphWorld::new (wcsph.rs:83). `cfg` may be NULL. */
+int pe_fluid_wcsph_create(const PeParticles* particles, const PeWcsphParams* params,
+                          const PeWcsphConfig* cfg, PeWcsph** out);
+/* Same from caller arrays: kind[i] in {0 fluid, 1 boundary}; psi and n_out may
+ * be NULL (0); v may be NULL (0). */
+int pe_fluid_wcsph_create_from_arrays(const PeWcsphParams* params, int32_t dim, double rest_density,
+                                      double mass, double h, uint64_t n, const double* x,
+                                      const double* v, const uint8_t* kind, const double* psi,
+                                      const double* n_out, const PeWcsphConfig* cfg, PeWcsph** out);
+void pe_fluid_wcsph_destroy(PeWcsph* w);
+
+/* WcsphWorld::step (wcsph.rs:326). Synchronous; returns PE_ERR_BOUNDS if the
+ * step raised PE_STATUS_DOMAIN or PE_STATUS_NEIGHBOUR_OVERFLOW. */
+int pe_fluid_wcsph_step(PeWcsph* w, double dt);
+/* `steps` calls of step, checked once at the end. */
+int pe_fluid_wcsph_run(PeWcsph* w, double dt, uint64_t steps);
+/* Phase methods (wcsph.rs:102, 117, 157, 181, 283). */
+int pe_fluid_wcsph_rebuild_grid(PeWcsph* w);
+int pe_fluid_wcsph_compute_density(PeWcsph* w);
+int pe_fluid_wcsph_compute_pressure(PeWcsph* w);
+int pe_fluid_wcsph_compute_forces(PeWcsph* w);
+int pe_fluid_wcsph_apply_xsph(PeWcsph* w);
+
+int pe_fluid_wcsph_len(const PeWcsph* w, uint64_t* out_len);
+int pe_fluid_wcsph_get_time(const PeWcsph* w, double* t);
+int pe_fluid_wcsph_set_time(PeWcsph* w, double t);
+/* Persisted sound speed (params.eos.sound_speed, updated by compute_pressure). */
+int pe_fluid_wcsph_get_sound_speed(PeWcsph* w, double* c);
+int pe_fluid_wcsph_get_params(PeWcsph* w, PeWcsphParams* out);
+int pe_fluid_wcsph_set_params(PeWcsph* w, const PeWcsphParams* params);
+
+/* State in original order. Vectors are [n*3]. */
+int pe_fluid_wcsph_get_positions(PeWcsph* w, double* out, uint64_t n);
+int pe_fluid_wcsph_get_velocities(PeWcsph* w, double* out, uint64_t n);
+int pe_fluid_wcsph_get_accelerations(PeWcsph* w, double* out, uint64_t n);
+int pe_fluid_wcsph_get_boundary_forces(PeWcsph* w, double* out, uint64_t n);
+int pe_fluid_wcsph_get_densities(PeWcsph* w, double* out, uint64_t n);
+int pe_fluid_wcsph_get_pressures(PeWcsph* w, double* out, uint64_t n);
+int pe_fluid_wcsph_get_kinds(PeWcsph* w, uint8_t* out, uint64_t n);
+/* Setting positions marks the grid stale (the next step rebuilds it). */
+int pe_fluid_wcsph_set_positions(PeWcsph* w, const double* in, uint64_t n);
+int pe_fluid_wcsph_set_velocities(PeWcsph* w, const double* in, uint64_t n);
+int pe_fluid_wcsph_set_densities(PeWcsph* w, const double* in, uint64_t n);
+int pe_fluid_wcsph_set_pressures(PeWcsph* w, const double* in, uint64_t n);
+
+/* UniformGrid (grid.rs:32-45): keys [n*3] per original index, order [n]
+ * (original indices sorted by (key, index)), occupied [m*3], ranges [m*2]
+ * with m <= occupied_cap; *n_occupied receives m. Any output may be NULL. */
+int pe_fluid_wcsph_get_grid(PeWcsph* w, int32_t* keys, uint64_t* order, uint64_t n,
+                            int32_t* occupied, uint64_t* ranges, uint64_t occupied_cap,
+                            uint64_t* n_occupied);
+/* Per particle: candidate count (= neigh_lists[i].len() of the reference,
+ * self included; 0 for boundary) and in-support count (j != i, r/h < 2). */
+int pe_fluid_wcsph_get_neighbour_counts(PeWcsph* w, uint32_t* candidates, uint32_t* in_support,
+                                        uint64_t n);
+
+int pe_fluid_wcsph_status(PeWcsph* w, uint32_t* status);
+int pe_fluid_wcsph_clear_status(PeWcsph* w);
+int pe_fluid_wcsph_diagnostics(PeWcsph* w, PeFluidDiagnostics* out);
+/* Per-phase device time, measured with CUDA events on the world's stream:
+ * 0 grid build, 1 neighbour lists, 2 density, 3 pressure, 4 forces + kick/drift,
+ * 5 boundary reaction forces, 6 XSPH (no reference counterpart). */
+#define PE_FLUID_NUM_PHASES 7
+typedef struct PeFluidProfile {
+    double ms[PE_FLUID_NUM_PHASES];
+    uint64_t count[PE_FLUID_NUM_PHASES];
+} PeFluidProfile;
+int pe_fluid_wcsph_profile(PeWcsph* w, int32_t enable);
+int pe_fluid_wcsph_profile_read(PeWcsph* w, PeFluidProfile* out, int32_t reset);
+/* The CUDA stream (cudaStream_t) all of the world's work is issued on. */
+int pe_fluid_wcsph_stream(PeWcsph* w, void** out);
+/* Kernel launches issued since creation or the last reset (accounting aid). */
+int pe_fluid_wcsph_kernel_launches(PeWcsph* w, uint64_t* out, int32_t reset);
+
+/* ---- stateless helpers ---- */
+/* kernels.rs:40 w and kernels.rs:56 grad_w (cubic spline), eos.rs:65 pressure. */
+double pe_fluid_kernel_w(int32_t kernel, double r, double h, int32_t dim);
+int pe_fluid_grad_w(int32_t kernel, const double rij[3], double h, int32_t dim, double out[3]);
+double pe_fluid_tait_pressure(double rest_density, double sound_speed, double gamma, double density);
+/* viscosity.rs:51 pi_ij */
+double pe_fluid_pi_ij(double alpha, double beta, double eps, double h, double sound_speed,
+                      const double xi[3], const double xj[3], const double vi[3], const double vj[3],
+                      double rho_i, double rho_j);
+/* cfl.rs:36 suggested_dt */
+double pe_fluid_suggested_dt(double h, double sound_speed, double v_max, double a_max,
+                             double lambda_v, double lambda_f);
+/* Library version string. */
+const char* pe_fluid_version(void);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PE_FLUID_WCSPH_H */

@@ -1,0 +1,921 @@
+// TEST INFRASTRUCTURE — NOT PART OF THE PRODUCT.
+//
+// CPU oracle: an order-exact C++ restatement of eranyid/physics-engine's
+// `pe-fluid` WCSPH solver path (Rust). Only the test suite, the smoke check
+// and the CPU-baseline leg of bench.py load this library; the product
+// (physics-engine_b200/) never links, calls or falls back to it.
+//
+// Every function names the reference file:line it restates. Floating-point
+// statements keep the reference's operand order and association exactly
+// (Rust evaluates `a * b * c` as `(a * b) * c`), and the file is compiled
+// with `-ffp-contract=off` (no FMA), matching the reference's determinism
+// policy (`.cargo/config.toml`, `docs/DETERMINISM.md`).
+//
+// Elementary functions: the reference calls the pure-Rust `libm` crate
+// 0.2.16 (`Cargo.lock:524-525`), whose source is not vendored. `sqrt` is
+// IEEE correctly rounded everywhere, so the C library's sqrt is bit-identical.
+// `pow` (Tait EOS, `eos.rs:68`; poly6/spiky normalisation, `kernels.rs:164,190`)
+// is restated as a correctly rounded integer power evaluated in binary128
+// (`oracle_pow`), falling back to the C library for non-integer exponents.
+// The crate's pow is documented as "nearly rounded", so the two agree except
+// in rare last-ulp cases; parity at the pow boundary is therefore unpinned.
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <limits>
+#include <new>
+#include <vector>
+
+namespace oracle {
+
+// ---------------------------------------------------------------------------
+// pe-math Vec3 (crates/pe-math/src/vec3.rs:9-183): component-wise ops.
+// ---------------------------------------------------------------------------
+struct V3 {
+    double x, y, z;
+};
+static inline V3 v3(double x, double y, double z) { return V3{x, y, z}; }
+static inline V3 zero3() { return V3{0.0, 0.0, 0.0}; }
+static inline V3 operator+(V3 a, V3 b) { return V3{a.x + b.x, a.y + b.y, a.z + b.z}; }
+static inline V3 operator-(V3 a, V3 b) { return V3{a.x - b.x, a.y - b.y, a.z - b.z}; }
+static inline V3 operator*(V3 a, double s) { return V3{a.x * s, a.y * s, a.z * s}; }
+static inline V3& operator+=(V3& a, V3 b) { a = a + b; return a; }
+static inline V3& operator-=(V3& a, V3 b) { a = a - b; return a; }
+// vec3.rs:69 norm_squared = x*x + y*y + z*z (left to right)
+static inline double norm2(V3 a) { return a.x * a.x + a.y * a.y + a.z * a.z; }
+// vec3.rs:63 norm = sqrt(norm_squared)
+static inline double norm(V3 a) { return std::sqrt(norm2(a)); }
+// vec3.rs:81 dot
+static inline double dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+
+// ---------------------------------------------------------------------------
+// pow restatement (see header): correctly rounded x^n for integer n.
+// ---------------------------------------------------------------------------
+static double pow_int_binary128(double x, long n) {
+    __float128 b = x;
+    __float128 r = 1;
+    unsigned long e = n < 0 ? (unsigned long)(-n) : (unsigned long)n;
+    while (e) {
+        if (e & 1UL) r *= b;
+        b *= b;
+        e >>= 1;
+    }
+    if (n < 0) r = (__float128)1 / r;
+    return (double)r;
+}
+
+double oracle_pow(double x, double y) {
+    if (std::isfinite(x) && x > 0.0 && std::isfinite(y) && y == std::floor(y) &&
+        std::fabs(y) <= 64.0) {
+        return pow_int_binary128(x, (long)y);
+    }
+    return std::pow(x, y);
+}
+
+// ---------------------------------------------------------------------------
+// pe-math xoshiro256** (crates/pe-math/src/rng.rs:14-72).
+// ---------------------------------------------------------------------------
+struct Xoshiro {
+    uint64_t s[4];
+};
+static inline uint64_t rotl(uint64_t x, int k) { return (x << k) | (x >> (64 - k)); }
+// rng.rs:25 splitmix64
+static inline uint64_t splitmix64(uint64_t* st) {
+    *st += 0x9e3779b97f4a7c15ULL;
+    uint64_t z = *st;
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+    return z ^ (z >> 31);
+}
+// rng.rs:35 seed
+static Xoshiro xoshiro_seed(uint64_t seed) {
+    Xoshiro r;
+    uint64_t sm = seed;
+    for (int i = 0; i < 4; ++i) r.s[i] = splitmix64(&sm);
+    if (r.s[0] == 0 && r.s[1] == 0 && r.s[2] == 0 && r.s[3] == 0) r.s[0] = 0x9e3779b97f4a7c15ULL;
+    return r;
+}
+// rng.rs:50 next_u64
+static inline uint64_t xoshiro_next(Xoshiro* r) {
+    uint64_t* s = r->s;
+    uint64_t result = rotl(s[1] * 5, 7) * 9;
+    uint64_t t = s[1] << 17;
+    s[2] ^= s[0];
+    s[3] ^= s[1];
+    s[1] ^= s[2];
+    s[0] ^= s[3];
+    s[2] ^= t;
+    s[3] = rotl(s[3], 45);
+    return result;
+}
+// rng.rs:64 next_f64, rng.rs:70 uniform
+static inline double xoshiro_f64(Xoshiro* r) {
+    return (double)(xoshiro_next(r) >> 11) * (1.0 / (double)(1ULL << 53));
+}
+static inline double xoshiro_uniform(Xoshiro* r, double lo, double hi) {
+    return lo + (hi - lo) * xoshiro_f64(r);
+}
+
+// ---------------------------------------------------------------------------
+// pe-fluid types
+// ---------------------------------------------------------------------------
+enum Dim { D2 = 2, D3 = 3 };                         // lib.rs:202
+enum Kind : uint8_t { FLUID = 0, BOUNDARY = 1 };      // particles.rs:11
+enum KernelKind { CUBIC = 0, WENDLAND = 1, POLY6 = 2, SPIKY = 3 };  // kernels.rs:19
+
+static const double PI = 3.14159265358979311599796346854;  // f64::consts::PI
+
+// kernels.rs:32 support_radius
+static double support_radius(KernelKind k, double h) {
+    return (k == CUBIC || k == WENDLAND) ? 2.0 * h : h;
+}
+// kernels.rs:79 cubic_alpha
+static double cubic_alpha(double h, Dim dim) {
+    return dim == D2 ? 10.0 / (7.0 * PI * h * h) : 1.0 / (PI * h * h * h);
+}
+// kernels.rs:86 cubic_spline_w
+static double cubic_spline_w(double r, double h, Dim dim) {
+    double q = r / h;
+    if (q >= 2.0) return 0.0;
+    double a = cubic_alpha(h, dim);
+    if (q < 1.0) {
+        return a * (1.0 - 1.5 * q * q + 0.75 * q * q * q);
+    }
+    double t = 2.0 - q;
+    return a * 0.25 * t * t * t;
+}
+// kernels.rs:102 cubic_spline_dwdr
+static double cubic_spline_dwdr(double r, double h, Dim dim) {
+    double q = r / h;
+    if (q >= 2.0 || q <= 0.0) return 0.0;
+    double a = cubic_alpha(h, dim);
+    double dwdq;
+    if (q < 1.0) {
+        dwdq = a * (-3.0 * q + 2.25 * q * q);
+    } else {
+        double t = 2.0 - q;
+        dwdq = a * (-0.75 * t * t);
+    }
+    return dwdq / h;
+}
+// kernels.rs:121 wendland_alpha, :129 wendland_c2_w, :139 wendland_c2_dwdr
+static double wendland_alpha(double h, Dim dim) {
+    return dim == D2 ? 7.0 / (4.0 * PI * h * h) : 21.0 / (16.0 * PI * h * h * h);
+}
+static double wendland_c2_w(double r, double h, Dim dim) {
+    double q = r / h;
+    if (q >= 2.0) return 0.0;
+    double a = wendland_alpha(h, dim);
+    double t = 1.0 - 0.5 * q;
+    return a * t * t * t * t * (2.0 * q + 1.0);
+}
+static double wendland_c2_dwdr(double r, double h, Dim dim) {
+    double q = r / h;
+    if (q >= 2.0 || q <= 0.0) return 0.0;
+    double a = wendland_alpha(h, dim);
+    double t = 1.0 - 0.5 * q;
+    double dwdq = a * (-5.0 * q) * t * t * t;
+    return dwdq / h;
+}
+// kernels.rs:161 poly6_alpha, :169 poly6_w, :178 poly6_dwdr
+static double poly6_alpha(double h, Dim dim) {
+    return dim == D2 ? 4.0 / (PI * oracle_pow(h, 8.0)) : 315.0 / (64.0 * PI * oracle_pow(h, 9.0));
+}
+static double poly6_w(double r, double h, Dim dim) {
+    if (r >= h) return 0.0;
+    double a = poly6_alpha(h, dim);
+    double t = h * h - r * r;
+    return a * t * t * t;
+}
+static double poly6_dwdr(double r, double h, Dim dim) {
+    if (r >= h || r <= 0.0) return 0.0;
+    double a = poly6_alpha(h, dim);
+    double t = h * h - r * r;
+    return a * (-6.0 * r * t * t);
+}
+// kernels.rs:188 spiky_alpha, :196 spiky_w, :205 spiky_dwdr
+static double spiky_alpha(double h, Dim dim) {
+    return dim == D2 ? 10.0 / (PI * oracle_pow(h, 5.0)) : 15.0 / (PI * oracle_pow(h, 6.0));
+}
+static double spiky_w(double r, double h, Dim dim) {
+    if (r >= h) return 0.0;
+    double a = spiky_alpha(h, dim);
+    double t = h - r;
+    return a * t * t * t;
+}
+static double spiky_dwdr(double r, double h, Dim dim) {
+    if (r >= h || r <= 0.0) return 0.0;
+    double a = spiky_alpha(h, dim);
+    double t = h - r;
+    return a * (-3.0 * t * t);
+}
+// kernels.rs:40 w
+static double kern_w(KernelKind k, double r, double h, Dim dim) {
+    if (h <= 0.0 || r < 0.0) return 0.0;
+    switch (k) {
+        case CUBIC: return cubic_spline_w(r, h, dim);
+        case WENDLAND: return wendland_c2_w(r, h, dim);
+        case POLY6: return poly6_w(r, h, dim);
+        default: return spiky_w(r, h, dim);
+    }
+}
+// kernels.rs:56 grad_w (rij = r_j - r_i; returns grad_i W)
+static V3 grad_w(KernelKind k, V3 rij, double h, Dim dim) {
+    if (h <= 0.0) return zero3();
+    double r2 = norm2(rij);
+    double r = std::sqrt(r2);
+    double dwdr;
+    switch (k) {
+        case CUBIC: dwdr = cubic_spline_dwdr(r, h, dim); break;
+        case WENDLAND: dwdr = wendland_c2_dwdr(r, h, dim); break;
+        case POLY6: dwdr = poly6_dwdr(r, h, dim); break;
+        default: dwdr = spiky_dwdr(r, h, dim); break;
+    }
+    if (r < 1e-30) return zero3();
+    return rij * (-dwdr / r);
+}
+
+// ---------------------------------------------------------------------------
+// Particles (particles.rs:20-162)
+// ---------------------------------------------------------------------------
+struct Particles {
+    Dim dim;
+    double rest_density, mass, h;
+    std::vector<V3> x, v, a;
+    std::vector<double> rho, p;
+    std::vector<uint8_t> kind;
+    std::vector<double> psi;
+    std::vector<V3> n_out;
+    size_t len() const { return x.size(); }
+    // particles.rs:90 push_fluid
+    void push_fluid(V3 px, V3 pv) {
+        x.push_back(px); v.push_back(pv); a.push_back(zero3());
+        rho.push_back(rest_density); p.push_back(0.0);
+        kind.push_back(FLUID); psi.push_back(0.0); n_out.push_back(zero3());
+    }
+    // particles.rs:102/107 push_boundary(_oriented)
+    void push_boundary(V3 px, double ps, V3 n = V3{0, 0, 0}) {
+        x.push_back(px); v.push_back(zero3()); a.push_back(zero3());
+        rho.push_back(rest_density); p.push_back(0.0);
+        kind.push_back(BOUNDARY); psi.push_back(ps); n_out.push_back(n);
+    }
+    // particles.rs:126 boundary_sees_fluid
+    bool boundary_sees_fluid(size_t b, V3 xf) const {
+        V3 n = n_out[b];
+        double n2 = norm2(n);
+        if (n2 <= 0.0) return true;
+        double eps = 0.15 * h * std::sqrt(std::fmax(n2, 0.0));
+        return dot(xf - x[b], n) > -eps;
+    }
+    size_t fluid_count() const {
+        size_t c = 0;
+        for (auto k : kind) c += (k == FLUID);
+        return c;
+    }
+};
+
+// particles.rs:166 mass_from_spacing
+static double mass_from_spacing(double rho0, double dx, Dim dim) {
+    return dim == D2 ? rho0 * dx * dx : rho0 * dx * dx * dx;
+}
+// particles.rs:178 mass_calibrated_to_rest
+static double mass_calibrated_to_rest(double rho0, double dx, double h, Dim dim, KernelKind k) {
+    double support = support_radius(k, h);
+    int n = (int)std::ceil(support / dx) + 1;
+    double sum_w = kern_w(k, 0.0, h, dim);
+    for (int ix = -n; ix <= n; ++ix)
+        for (int iy = -n; iy <= n; ++iy) {
+            int z0 = dim == D2 ? 0 : -n, z1 = dim == D2 ? 0 : n;
+            for (int iz = z0; iz <= z1; ++iz) {
+                if (ix == 0 && iy == 0 && iz == 0) continue;
+                double r = std::sqrt(((double)ix * dx) * ((double)ix * dx) +
+                                     ((double)iy * dx) * ((double)iy * dx) +
+                                     ((double)iz * dx) * ((double)iz * dx));
+                if (r < support) sum_w += kern_w(k, r, h, dim);
+            }
+        }
+    return sum_w < 1e-30 ? mass_from_spacing(rho0, dx, dim) : rho0 / sum_w;
+}
+// particles.rs:220 fill_box (iz -> iy -> ix fill order)
+static void fill_box(Particles& p, V3 origin, size_t nx, size_t ny, size_t nz, double dx, V3 v0) {
+    if (p.dim == D2) nz = 1;
+    for (size_t iz = 0; iz < nz; ++iz)
+        for (size_t iy = 0; iy < ny; ++iy)
+            for (size_t ix = 0; ix < nx; ++ix)
+                p.push_fluid(v3(origin.x + (double)ix * dx, origin.y + (double)iy * dx,
+                                origin.z + (double)iz * dx), v0);
+}
+// particles.rs:252 recomputed_akinci_psi (O(N_b^2), index order)
+static void recomputed_akinci_psi(Particles& p, KernelKind k) {
+    double h = p.h;
+    double support = support_radius(k, h);
+    std::vector<size_t> bound;
+    for (size_t i = 0; i < p.len(); ++i)
+        if (p.kind[i] == BOUNDARY) bound.push_back(i);
+    for (size_t bi : bound) {
+        V3 xb = p.x[bi];
+        double delta = kern_w(k, 0.0, h, p.dim);
+        for (size_t bj : bound) {
+            if (bj == bi) continue;
+            double r = norm(p.x[bj] - xb);
+            if (r < support) delta += kern_w(k, r, h, p.dim);
+        }
+        p.psi[bi] = delta > 1e-30 ? 1.0 / delta : 0.0;
+    }
+}
+// particles.rs:286 fill_box_boundary
+static void fill_box_boundary(Particles& p, V3 mn, V3 mx, double dx, size_t layers) {
+    double psi = p.dim == D2 ? dx * dx : dx * dx * dx;
+    if (layers < 1) layers = 1;
+    if (p.dim == D2) {
+        size_t nx = (size_t)std::round((mx.x - mn.x) / dx) + 1;
+        size_t ny = (size_t)std::round((mx.y - mn.y) / dx) + 1;
+        for (size_t layer = 0; layer < layers; ++layer) {
+            double off = (double)layer * dx;
+            for (size_t i = 0; i < nx; ++i) {
+                double x = mn.x + (double)i * dx;
+                p.push_boundary(v3(x, mn.y - off, 0.0), psi);
+                p.push_boundary(v3(x, mx.y + off, 0.0), psi);
+            }
+            for (size_t j = 1; j + 1 < ny; ++j) {
+                double y = mn.y + (double)j * dx;
+                p.push_boundary(v3(mn.x - off, y, 0.0), psi);
+                p.push_boundary(v3(mx.x + off, y, 0.0), psi);
+            }
+        }
+        return;
+    }
+    size_t nx = (size_t)std::round((mx.x - mn.x) / dx) + 1;
+    size_t ny = (size_t)std::round((mx.y - mn.y) / dx) + 1;
+    size_t nz = (size_t)std::round((mx.z - mn.z) / dx) + 1;
+    for (size_t layer = 0; layer < layers; ++layer) {
+        double off = (double)layer * dx;
+        for (size_t i = 0; i < nx; ++i)
+            for (size_t j = 0; j < ny; ++j) {
+                double x = mn.x + (double)i * dx, y = mn.y + (double)j * dx;
+                p.push_boundary(v3(x, y, mn.z - off), psi);
+                p.push_boundary(v3(x, y, mx.z + off), psi);
+            }
+        for (size_t i = 0; i < nx; ++i)
+            for (size_t k = 1; k + 1 < nz; ++k) {
+                double x = mn.x + (double)i * dx, z = mn.z + (double)k * dx;
+                p.push_boundary(v3(x, mn.y - off, z), psi);
+                p.push_boundary(v3(x, mx.y + off, z), psi);
+            }
+        for (size_t j = 1; j + 1 < ny; ++j)
+            for (size_t k = 1; k + 1 < nz; ++k) {
+                double y = mn.y + (double)j * dx, z = mn.z + (double)k * dx;
+                p.push_boundary(v3(mn.x - off, y, z), psi);
+                p.push_boundary(v3(mx.x + off, y, z), psi);
+            }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Uniform grid (grid.rs:13-157)
+// ---------------------------------------------------------------------------
+struct CellKey {
+    int32_t ix, iy, iz;
+};
+// Derived Ord on {ix, iy, iz}: lexicographic, ix-major (grid.rs:12).
+static inline bool key_lt(const CellKey& a, const CellKey& b) {
+    if (a.ix != b.ix) return a.ix < b.ix;
+    if (a.iy != b.iy) return a.iy < b.iy;
+    return a.iz < b.iz;
+}
+static inline bool key_eq(const CellKey& a, const CellKey& b) {
+    return a.ix == b.ix && a.iy == b.iy && a.iz == b.iz;
+}
+// grid.rs:144 floor_i32
+static inline int32_t floor_i32(double x) {
+    if (!std::isfinite(x)) return 0;
+    const double lo = (double)std::numeric_limits<int32_t>::min() + 1.0;
+    const double hi = (double)std::numeric_limits<int32_t>::max() - 1.0;
+    double c = x < lo ? lo : (x > hi ? hi : x);
+    int32_t t = (int32_t)c;  // truncation toward zero; c is in range
+    if ((double)t > c) return t == std::numeric_limits<int32_t>::min() ? t : t - 1;
+    return t;
+}
+
+struct UniformGrid {
+    double cell_size;
+    Dim dim;
+    std::vector<size_t> order;
+    std::vector<CellKey> keys;
+    std::vector<CellKey> occupied;
+    std::vector<std::pair<size_t, size_t>> ranges;
+
+    // grid.rs:62 key_of
+    CellKey key_of(V3 p) const {
+        double inv = 1.0 / cell_size;
+        int32_t ix = floor_i32(p.x * inv);
+        int32_t iy = floor_i32(p.y * inv);
+        int32_t iz = dim == D2 ? 0 : floor_i32(p.z * inv);
+        return CellKey{ix, iy, iz};
+    }
+    // grid.rs:76 rebuild: sort by (key, index), run-length occupied cells
+    void rebuild(const std::vector<V3>& pos) {
+        size_t n = pos.size();
+        keys.resize(n);
+        order.clear();
+        order.reserve(n);
+        for (size_t i = 0; i < n; ++i) {
+            keys[i] = key_of(pos[i]);
+            order.push_back(i);
+        }
+        const std::vector<CellKey>& k = keys;
+        std::stable_sort(order.begin(), order.end(), [&k](size_t a, size_t b) {
+            if (key_lt(k[a], k[b])) return true;
+            if (key_lt(k[b], k[a])) return false;
+            return a < b;
+        });
+        occupied.clear();
+        ranges.clear();
+        if (n == 0) return;
+        size_t start = 0;
+        CellKey cur = keys[order[0]];
+        for (size_t s = 1; s < n; ++s) {
+            CellKey kk = keys[order[s]];
+            if (!key_eq(kk, cur)) {
+                occupied.push_back(cur);
+                ranges.push_back({start, s});
+                start = s;
+                cur = kk;
+            }
+        }
+        occupied.push_back(cur);
+        ranges.push_back({start, n});
+    }
+    // grid.rs:111 cell_range: binary search of the occupied keys
+    bool cell_range(CellKey key, size_t* a, size_t* b) const {
+        auto it = std::lower_bound(occupied.begin(), occupied.end(), key, key_lt);
+        if (it == occupied.end() || !key_eq(*it, key)) return false;
+        size_t idx = (size_t)(it - occupied.begin());
+        *a = ranges[idx].first;
+        *b = ranges[idx].second;
+        return true;
+    }
+    // grid.rs:122 neighbours: cells in (dz, dy, dx) order, appends order[a..b]
+    void neighbours(size_t i, std::vector<size_t>& out) const {
+        CellKey key = keys[i];
+        int dz0 = dim == D2 ? 0 : -1, dz1 = dim == D2 ? 0 : 1;
+        for (int dz = dz0; dz <= dz1; ++dz)
+            for (int dy = -1; dy <= 1; ++dy)
+                for (int dx = -1; dx <= 1; ++dx) {
+                    CellKey nk{key.ix + dx, key.iy + dy, key.iz + dz};
+                    size_t a, b;
+                    if (cell_range(nk, &a, &b))
+                        for (size_t s = a; s < b; ++s) out.push_back(order[s]);
+                }
+    }
+};
+
+// ---------------------------------------------------------------------------
+// WCSPH (wcsph.rs:24-370, eos.rs:59-80, viscosity.rs:30-100)
+// ---------------------------------------------------------------------------
+struct WParams {
+    int32_t kernel;            // KernelKind (wcsph.rs:26)
+    double eos_rest_density;   // eos.rs:34
+    double eos_sound_speed;    // eos.rs:36
+    double eos_gamma;          // eos.rs:38
+    double visc_alpha, visc_beta, visc_eps;  // viscosity.rs:30
+    double xsph_epsilon;       // viscosity.rs:77
+    double gravity[3];         // wcsph.rs:34
+    int32_t adapt_sound_speed; // wcsph.rs:36
+    int32_t materialize_neigh_lists;  // wcsph.rs:102-113 (1 = as the reference)
+};
+
+struct World {
+    Particles parts;
+    UniformGrid grid;
+    WParams prm;
+    double t = 0.0;
+    std::vector<size_t> neigh;
+    std::vector<std::vector<size_t>> neigh_lists;
+    std::vector<V3> xsph_dv;
+    std::vector<V3> boundary_force;
+
+    KernelKind kk() const { return (KernelKind)prm.kernel; }
+
+    // wcsph.rs:102 rebuild_grid
+    void rebuild_grid() {
+        grid.rebuild(parts.x);
+        size_t n = parts.len();
+        if (neigh_lists.size() != n) neigh_lists.resize(n);
+        for (size_t i = 0; i < n; ++i) {
+            neigh_lists[i].clear();
+            if (prm.materialize_neigh_lists && parts.kind[i] == FLUID)
+                grid.neighbours(i, neigh_lists[i]);
+        }
+    }
+    // wcsph.rs:117 compute_density
+    void compute_density() {
+        size_t n = parts.len();
+        double h = parts.h, mass = parts.mass, rho0 = parts.rest_density;
+        Dim dim = parts.dim;
+        for (size_t i = 0; i < n; ++i) {
+            if (parts.kind[i] != FLUID) {
+                parts.rho[i] = rho0;
+                continue;
+            }
+            neigh.clear();
+            grid.neighbours(i, neigh);
+            V3 xi = parts.x[i];
+            double rho = 0.0;
+            rho += mass * kern_w(kk(), 0.0, h, dim);
+            for (size_t j : neigh) {
+                if (j == i) continue;
+                double r = norm(parts.x[j] - xi);
+                double wij = kern_w(kk(), r, h, dim);
+                if (parts.kind[j] == FLUID) {
+                    rho += mass * wij;
+                } else if (parts.boundary_sees_fluid(j, xi)) {
+                    rho += rho0 * parts.psi[j] * wij;
+                }
+            }
+            parts.rho[i] = std::fmax(rho, 1e-12);  // f64::max (NaN -> other)
+        }
+    }
+    // viscosity.rs:89 max_speed over fluid
+    double max_speed() const {
+        double m = 0.0;
+        for (size_t i = 0; i < parts.len(); ++i) {
+            if (parts.kind[i] != FLUID) continue;
+            double s = norm2(parts.v[i]);
+            if (s > m) m = s;
+        }
+        return std::sqrt(m);
+    }
+    // eos.rs:59 stiffness_b, eos.rs:65 pressure
+    double eos_pressure(double density) const {
+        double ratio = density / prm.eos_rest_density;
+        double b = prm.eos_rest_density * prm.eos_sound_speed * prm.eos_sound_speed / prm.eos_gamma;
+        return b * (oracle_pow(ratio, prm.eos_gamma) - 1.0);
+    }
+    // wcsph.rs:157 compute_pressure (+ eos.rs:74 ensure_sound_speed)
+    void compute_pressure() {
+        double c = prm.eos_sound_speed;
+        if (prm.adapt_sound_speed) {
+            double vmax = max_speed();
+            double min_c = 10.0 * std::fmax(vmax, 0.0);
+            c = c < min_c ? min_c : c;
+            prm.eos_sound_speed = c;
+        }
+        for (size_t i = 0; i < parts.len(); ++i)
+            parts.p[i] = parts.kind[i] == FLUID ? eos_pressure(parts.rho[i]) : 0.0;
+    }
+    // viscosity.rs:51 pi_ij
+    double pi_ij(double h, double c, V3 xi, V3 xj, V3 vi, V3 vj, double rhoi, double rhoj) const {
+        V3 rij = xi - xj;
+        V3 vij = vi - vj;
+        double vr = dot(vij, rij);
+        if (vr >= 0.0) return 0.0;
+        double r2 = norm2(rij);
+        double mu = h * vr / (r2 + prm.visc_eps * h * h);
+        double rho_bar = 0.5 * (rhoi + rhoj);
+        double c_bar = c;
+        return (-prm.visc_alpha * c_bar * mu + prm.visc_beta * mu * mu) / rho_bar;
+    }
+    // wcsph.rs:181 compute_forces (surface tension branch not restated: sigma = 0)
+    void compute_forces() {
+        size_t n = parts.len();
+        double h = parts.h, mass = parts.mass, rho0 = parts.rest_density;
+        double c0 = prm.eos_sound_speed;
+        Dim dim = parts.dim;
+        V3 g = v3(prm.gravity[0], prm.gravity[1], prm.gravity[2]);
+        for (auto& a : parts.a) a = zero3();
+        if (boundary_force.size() != n) boundary_force.resize(n);
+        for (auto& f : boundary_force) f = zero3();
+        for (size_t i = 0; i < n; ++i) {
+            if (parts.kind[i] != FLUID) continue;
+            neigh.clear();
+            grid.neighbours(i, neigh);
+            V3 xi = parts.x[i], vi = parts.v[i];
+            double rho_i = parts.rho[i], p_i = parts.p[i];
+            for (size_t j : neigh) {
+                if (j == i) continue;
+                V3 xj = parts.x[j];
+                V3 rij = xj - xi;
+                double r = norm(rij);
+                if (r < 1e-30) continue;
+                V3 gw = grad_w(kk(), rij, h, dim);
+                if (parts.kind[j] == FLUID) {
+                    if (j < i) continue;
+                    double rho_j = parts.rho[j], p_j = parts.p[j];
+                    V3 vj = parts.v[j];
+                    double press = p_i / (rho_i * rho_i) + p_j / (rho_j * rho_j);
+                    V3 f_press = gw * (-mass * press);
+                    double pi = pi_ij(h, c0, xi, xj, vi, vj, rho_i, rho_j);
+                    V3 f_visc = gw * (-mass * pi);
+                    V3 f = f_press + f_visc;
+                    parts.a[i] += f;
+                    parts.a[j] -= f;
+                } else {
+                    if (!parts.boundary_sees_fluid(j, xi)) continue;
+                    double press = p_i / (rho_i * rho_i);
+                    V3 f = gw * (-(rho0 * parts.psi[j]) * press);
+                    parts.a[i] += f;
+                    boundary_force[j] += f * (-mass);
+                }
+            }
+            parts.a[i] += g;
+        }
+    }
+    // wcsph.rs:283 apply_xsph
+    void apply_xsph() {
+        double eps = prm.xsph_epsilon;
+        if (eps == 0.0) return;
+        size_t n = parts.len();
+        double h = parts.h, mass = parts.mass;
+        Dim dim = parts.dim;
+        xsph_dv.assign(n, zero3());
+        for (size_t i = 0; i < n; ++i) {
+            if (parts.kind[i] != FLUID) continue;
+            neigh.clear();
+            grid.neighbours(i, neigh);
+            V3 xi = parts.x[i], vi = parts.v[i];
+            double rho_i = parts.rho[i];
+            V3 dv = zero3();
+            for (size_t j : neigh) {
+                if (j == i || parts.kind[j] != FLUID) continue;
+                double r = norm(parts.x[j] - xi);
+                double wij = kern_w(kk(), r, h, dim);
+                double rho_bar = 0.5 * (rho_i + parts.rho[j]);
+                dv += (parts.v[j] - vi) * (mass / rho_bar * wij);
+            }
+            xsph_dv[i] = dv * eps;
+        }
+        for (size_t i = 0; i < n; ++i)
+            if (parts.kind[i] == FLUID) parts.v[i] += xsph_dv[i];
+    }
+    // wcsph.rs:326 step
+    void step(double dt) {
+        rebuild_grid();
+        compute_density();
+        compute_pressure();
+        compute_forces();
+        size_t n = parts.len();
+        for (size_t i = 0; i < n; ++i) {
+            if (parts.kind[i] != FLUID) continue;
+            parts.v[i] += parts.a[i] * dt;
+            parts.x[i] += parts.v[i] * dt;
+            if (parts.dim == D2) {
+                parts.x[i].z = 0.0;
+                parts.v[i].z = 0.0;
+            }
+        }
+        rebuild_grid();
+        compute_density();
+        apply_xsph();
+        t += dt;
+    }
+    // wcsph.rs:361 a_max
+    double a_max() const {
+        double m = 0.0;
+        for (size_t i = 0; i < parts.len(); ++i)
+            if (parts.kind[i] == FLUID) m = std::fmax(m, norm2(parts.a[i]));
+        return std::sqrt(m);
+    }
+};
+
+// diagnostics.rs:10-33 FNV-1a over fluid (x, v) bits, little-endian bytes
+static inline void fnv1a_f64(uint64_t* hsh, double x) {
+    uint64_t bits;
+    std::memcpy(&bits, &x, 8);
+    for (int k = 0; k < 8; ++k) {
+        *hsh ^= (bits >> (8 * k)) & 0xffULL;
+        *hsh *= 0x100000001b3ULL;
+    }
+}
+static uint64_t particles_hash64(const Particles& p) {
+    uint64_t h = 0xcbf29ce484222325ULL;
+    for (size_t i = 0; i < p.len(); ++i) {
+        if (p.kind[i] != FLUID) continue;
+        fnv1a_f64(&h, p.x[i].x); fnv1a_f64(&h, p.x[i].y); fnv1a_f64(&h, p.x[i].z);
+        fnv1a_f64(&h, p.v[i].x); fnv1a_f64(&h, p.v[i].y); fnv1a_f64(&h, p.v[i].z);
+    }
+    return h;
+}
+
+}  // namespace oracle
+
+// ===========================================================================
+// C ABI used by the test suite (ctypes). Buffers are caller-owned, SoA in
+// original particle order, `[n*3]` for vectors.
+// ===========================================================================
+using namespace oracle;
+
+extern "C" {
+
+struct OScene;  // opaque particle builder
+OScene* oscene_new(int dim, double rho0, double mass, double h) {
+    Particles* p = new (std::nothrow) Particles();
+    if (!p) return nullptr;
+    p->dim = dim == 2 ? D2 : D3;
+    p->rest_density = rho0;
+    p->mass = mass;
+    p->h = h;
+    return reinterpret_cast<OScene*>(p);
+}
+void oscene_free(OScene* s) { delete reinterpret_cast<Particles*>(s); }
+long oscene_len(OScene* s) { return (long)reinterpret_cast<Particles*>(s)->len(); }
+void oscene_push_fluid(OScene* s, const double* x, const double* v) {
+    reinterpret_cast<Particles*>(s)->push_fluid(v3(x[0], x[1], x[2]), v3(v[0], v[1], v[2]));
+}
+void oscene_push_boundary(OScene* s, const double* x, double psi, const double* n_out) {
+    V3 n = n_out ? v3(n_out[0], n_out[1], n_out[2]) : zero3();
+    reinterpret_cast<Particles*>(s)->push_boundary(v3(x[0], x[1], x[2]), psi, n);
+}
+void oscene_fill_box(OScene* s, const double* origin, long nx, long ny, long nz, double dx,
+                     const double* v0) {
+    fill_box(*reinterpret_cast<Particles*>(s), v3(origin[0], origin[1], origin[2]), (size_t)nx,
+             (size_t)ny, (size_t)nz, dx, v3(v0[0], v0[1], v0[2]));
+}
+void oscene_fill_box_boundary(OScene* s, const double* mn, const double* mx, double dx, long layers) {
+    fill_box_boundary(*reinterpret_cast<Particles*>(s), v3(mn[0], mn[1], mn[2]),
+                      v3(mx[0], mx[1], mx[2]), dx, (size_t)layers);
+}
+void oscene_recompute_psi(OScene* s, int kernel) {
+    recomputed_akinci_psi(*reinterpret_cast<Particles*>(s), (KernelKind)kernel);
+}
+// Seeded lattice jitter of the fluid particles: xoshiro256** draws in particle
+// order, x then y (then z in 3-D), each U(-amp, amp), added component-wise.
+void oscene_jitter_fluid(OScene* s, uint64_t seed, double amp) {
+    Particles& p = *reinterpret_cast<Particles*>(s);
+    Xoshiro r = xoshiro_seed(seed);
+    for (size_t i = 0; i < p.len(); ++i) {
+        if (p.kind[i] != FLUID) continue;
+        double jx = xoshiro_uniform(&r, -amp, amp);
+        double jy = xoshiro_uniform(&r, -amp, amp);
+        double jz = p.dim == D3 ? xoshiro_uniform(&r, -amp, amp) : 0.0;
+        p.x[i] = p.x[i] + v3(jx, jy, jz);
+    }
+}
+void oscene_export(OScene* s, double* x, double* v, uint8_t* kind, double* psi, double* n_out) {
+    Particles& p = *reinterpret_cast<Particles*>(s);
+    for (size_t i = 0; i < p.len(); ++i) {
+        if (x) { x[3 * i] = p.x[i].x; x[3 * i + 1] = p.x[i].y; x[3 * i + 2] = p.x[i].z; }
+        if (v) { v[3 * i] = p.v[i].x; v[3 * i + 1] = p.v[i].y; v[3 * i + 2] = p.v[i].z; }
+        if (kind) kind[i] = p.kind[i];
+        if (psi) psi[i] = p.psi[i];
+        if (n_out) { n_out[3 * i] = p.n_out[i].x; n_out[3 * i + 1] = p.n_out[i].y; n_out[3 * i + 2] = p.n_out[i].z; }
+    }
+}
+
+double o_mass_from_spacing(double rho0, double dx, int dim) {
+    return mass_from_spacing(rho0, dx, dim == 2 ? D2 : D3);
+}
+double o_mass_calibrated_to_rest(double rho0, double dx, double h, int dim, int kernel) {
+    return mass_calibrated_to_rest(rho0, dx, h, dim == 2 ? D2 : D3, (KernelKind)kernel);
+}
+double o_kernel_w(int kernel, double r, double h, int dim) {
+    return kern_w((KernelKind)kernel, r, h, dim == 2 ? D2 : D3);
+}
+void o_grad_w(int kernel, const double* rij, double h, int dim, double* out) {
+    V3 g = grad_w((KernelKind)kernel, v3(rij[0], rij[1], rij[2]), h, dim == 2 ? D2 : D3);
+    out[0] = g.x; out[1] = g.y; out[2] = g.z;
+}
+double o_pow(double x, double y) { return oracle_pow(x, y); }
+int32_t o_floor_i32(double x) { return floor_i32(x); }
+uint64_t o_xoshiro_first(uint64_t seed, long n, uint64_t* out) {
+    Xoshiro r = xoshiro_seed(seed);
+    uint64_t last = 0;
+    for (long i = 0; i < n; ++i) { last = xoshiro_next(&r); if (out) out[i] = last; }
+    return last;
+}
+
+struct OWorld;
+OWorld* ow_create(OScene* s, const WParams* prm) {
+    World* w = new (std::nothrow) World();
+    if (!w) return nullptr;
+    w->parts = *reinterpret_cast<Particles*>(s);
+    w->prm = *prm;
+    w->grid.cell_size = support_radius((KernelKind)prm->kernel, w->parts.h);
+    w->grid.dim = w->parts.dim;
+    w->neigh_lists.resize(w->parts.len());
+    w->boundary_force.assign(w->parts.len(), zero3());
+    return reinterpret_cast<OWorld*>(w);
+}
+void ow_free(OWorld* w) { delete reinterpret_cast<World*>(w); }
+static inline World& W(OWorld* w) { return *reinterpret_cast<World*>(w); }
+long ow_len(OWorld* w) { return (long)W(w).parts.len(); }
+void ow_step(OWorld* w, double dt) { W(w).step(dt); }
+void ow_run(OWorld* w, double dt, long steps) { for (long k = 0; k < steps; ++k) W(w).step(dt); }
+void ow_rebuild_grid(OWorld* w) { W(w).rebuild_grid(); }
+void ow_compute_density(OWorld* w) { W(w).compute_density(); }
+void ow_compute_pressure(OWorld* w) { W(w).compute_pressure(); }
+void ow_compute_forces(OWorld* w) { W(w).compute_forces(); }
+void ow_apply_xsph(OWorld* w) { W(w).apply_xsph(); }
+double ow_time(OWorld* w) { return W(w).t; }
+double ow_sound_speed(OWorld* w) { return W(w).prm.eos_sound_speed; }
+double ow_a_max(OWorld* w) { return W(w).a_max(); }
+double ow_v_max(OWorld* w) { return W(w).max_speed(); }
+uint64_t ow_hash(OWorld* w) { return particles_hash64(W(w).parts); }
+
+static void put3(const std::vector<V3>& src, double* out) {
+    for (size_t i = 0; i < src.size(); ++i) {
+        out[3 * i] = src[i].x; out[3 * i + 1] = src[i].y; out[3 * i + 2] = src[i].z;
+    }
+}
+static void get3(std::vector<V3>& dst, const double* in) {
+    for (size_t i = 0; i < dst.size(); ++i) dst[i] = v3(in[3 * i], in[3 * i + 1], in[3 * i + 2]);
+}
+void ow_get_x(OWorld* w, double* out) { put3(W(w).parts.x, out); }
+void ow_get_v(OWorld* w, double* out) { put3(W(w).parts.v, out); }
+void ow_get_a(OWorld* w, double* out) { put3(W(w).parts.a, out); }
+void ow_get_boundary_force(OWorld* w, double* out) { put3(W(w).boundary_force, out); }
+void ow_get_rho(OWorld* w, double* out) { std::copy(W(w).parts.rho.begin(), W(w).parts.rho.end(), out); }
+void ow_get_p(OWorld* w, double* out) { std::copy(W(w).parts.p.begin(), W(w).parts.p.end(), out); }
+void ow_set_x(OWorld* w, const double* in) { get3(W(w).parts.x, in); }
+void ow_set_v(OWorld* w, const double* in) { get3(W(w).parts.v, in); }
+void ow_set_rho(OWorld* w, const double* in) { std::copy(in, in + W(w).parts.len(), W(w).parts.rho.begin()); }
+void ow_set_p(OWorld* w, const double* in) { std::copy(in, in + W(w).parts.len(), W(w).parts.p.begin()); }
+
+// Grid export: keys [n*3] per original index, order [n], occupied [m*3],
+// ranges [m*2]; ow_grid_occupied_count gives m.
+long ow_grid_occupied_count(OWorld* w) { return (long)W(w).grid.occupied.size(); }
+void ow_get_grid(OWorld* w, int32_t* keys, int64_t* order, int32_t* occupied, int64_t* ranges) {
+    UniformGrid& g = W(w).grid;
+    for (size_t i = 0; i < g.keys.size(); ++i) {
+        if (keys) { keys[3 * i] = g.keys[i].ix; keys[3 * i + 1] = g.keys[i].iy; keys[3 * i + 2] = g.keys[i].iz; }
+    }
+    for (size_t s = 0; s < g.order.size(); ++s) if (order) order[s] = (int64_t)g.order[s];
+    for (size_t c = 0; c < g.occupied.size(); ++c) {
+        if (occupied) { occupied[3 * c] = g.occupied[c].ix; occupied[3 * c + 1] = g.occupied[c].iy; occupied[3 * c + 2] = g.occupied[c].iz; }
+        if (ranges) { ranges[2 * c] = (int64_t)g.ranges[c].first; ranges[2 * c + 1] = (int64_t)g.ranges[c].second; }
+    }
+}
+// Per-particle candidate count (= neigh_lists[i].len(), self included; 0 for
+// boundary) and in-support count (j != i with q = r/h < 2, kernel support).
+void ow_neighbour_counts(OWorld* w, int32_t* candidates, int32_t* in_support) {
+    World& wd = W(w);
+    std::vector<size_t> tmp;
+    double h = wd.parts.h;
+    for (size_t i = 0; i < wd.parts.len(); ++i) {
+        if (wd.parts.kind[i] != FLUID) {
+            if (candidates) candidates[i] = 0;
+            if (in_support) in_support[i] = 0;
+            continue;
+        }
+        tmp.clear();
+        wd.grid.neighbours(i, tmp);
+        if (candidates) candidates[i] = (int32_t)tmp.size();
+        if (in_support) {
+            int32_t c = 0;
+            for (size_t j : tmp) {
+                if (j == i) continue;
+                double r = norm(wd.parts.x[j] - wd.parts.x[i]);
+                if (r / h < 2.0) ++c;
+            }
+            in_support[i] = c;
+        }
+    }
+}
+
+// Diagnostics (diagnostics.rs:35-102), cfl.rs:36 suggested_dt.
+double o_total_mass(OWorld* w) { return W(w).parts.mass * (double)W(w).parts.fluid_count(); }
+void o_linear_momentum(OWorld* w, double* out) {
+    Particles& p = W(w).parts;
+    V3 m = zero3();
+    for (size_t i = 0; i < p.len(); ++i) if (p.kind[i] == FLUID) m += p.v[i] * p.mass;
+    out[0] = m.x; out[1] = m.y; out[2] = m.z;
+}
+double o_kinetic_energy(OWorld* w) {
+    Particles& p = W(w).parts;
+    double ke = 0.0;
+    for (size_t i = 0; i < p.len(); ++i) if (p.kind[i] == FLUID) ke += 0.5 * p.mass * norm2(p.v[i]);
+    return ke;
+}
+double o_gravitational_potential(OWorld* w, double g) {
+    Particles& p = W(w).parts;
+    double pe = 0.0;
+    for (size_t i = 0; i < p.len(); ++i) if (p.kind[i] == FLUID) pe += p.mass * g * p.x[i].z;
+    return pe;
+}
+double o_mean_density_error(OWorld* w) {
+    Particles& p = W(w).parts;
+    double s = 0.0;
+    size_t n = 0;
+    for (size_t i = 0; i < p.len(); ++i)
+        if (p.kind[i] == FLUID) { s += std::fabs(p.rho[i] - p.rest_density) / p.rest_density; ++n; }
+    return n == 0 ? 0.0 : s / (double)n;
+}
+double o_max_density_error(OWorld* w) {
+    Particles& p = W(w).parts;
+    double m = 0.0;
+    for (size_t i = 0; i < p.len(); ++i)
+        if (p.kind[i] == FLUID) {
+            double e = std::fabs(p.rho[i] - p.rest_density) / p.rest_density;
+            if (e > m) m = e;
+        }
+    return m;
+}
+double o_suggested_dt(double h, double c, double vmax, double amax, double lv, double lf) {
+    double dt_v = lv * h / std::fmax(c + vmax, 1e-12);
+    double dt_f = amax > 1e-12 ? lf * std::sqrt(h / amax) : std::numeric_limits<double>::infinity();
+    return std::fmin(dt_v, dt_f);
+}
+
+}  // extern "C"

@@ -1,0 +1,344 @@
+// The f64 SPH passes of the WCSPH step, one thread per cell-sorted slot.
+//
+// Each pass walks the slot's neighbour list and reproduces the reference's
+// floating-point sequence exactly (compiled with --fmad=false):
+//   density   — wcsph.rs:117-154 (visiting order)
+//   pressure  — wcsph.rs:157-178, eos.rs:59-80, viscosity.rs:89
+//   forces    — wcsph.rs:181-259 + the kick/drift of wcsph.rs:332-342
+//   xsph      — wcsph.rs:283-323
+//
+// Force-order argument. The reference accumulates a[i] by a symmetric
+// scatter: for each fluid i in ascending index, for each neighbour j in
+// visiting order, a fluid j > i adds f to a[i] and subtracts it from a[j].
+// Hence the final a[k] is the sequence
+//     0  -  f(i1,k) - f(i2,k) - ...      (fluid i < k, ascending i)
+//        +  f(k,j) ...                   (fluid j > k and boundary j, visiting order)
+//        +  g.
+// Every factor of f(i,k) is symmetric in (i,k) bit for bit (sums commute,
+// (-a)(-b) = ab exactly) except grad W, which flips sign exactly, so
+// f(i,k) = -f(k,i) bitwise and x - f(i,k) = x + f(k,i). A gather that adds
+// f(k,i) over the "lower" list (ascending original index) and then f(k,j)
+// over the visiting-order list, skipping entries flagged lower, therefore
+// yields the reference's bits. Pairs outside the support contribute +-0,
+// which leaves a sum that started at +0 unchanged, so the lists may omit them.
+#include "pe_math.cuh"
+#include "wcsph_device.cuh"
+
+namespace pe {
+
+namespace {
+
+constexpr int kThreads = 128;
+
+inline uint32_t blocks_for(uint64_t n, uint32_t t) { return (uint32_t)((n + t - 1) / t); }
+
+// particles.rs:126 boundary_sees_fluid
+__device__ __forceinline__ bool sees_fluid(const StepConst& k, double4 xb, double4 nb,
+                                           double xfx, double xfy, double xfz) {
+    double n2 = nb.x * nb.x + nb.y * nb.y + nb.z * nb.z;
+    if (n2 <= 0.0) return true;
+    double eps = k.boundary_eps_h * sqrt(fmax(n2, 0.0));
+    double d = (xfx - xb.x) * nb.x + (xfy - xb.y) * nb.y + (xfz - xb.z) * nb.z;
+    return d > -eps;
+}
+
+__global__ void __launch_bounds__(kThreads) k_density(uint32_t n, StepConst k, StateBufs s,
+                                                      ListBufs l) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (s.flags[i] & kFlagBoundary) {
+        s.vel[i].w = k.rho0;  // wcsph.rs:127
+        return;
+    }
+    const double4 xi = s.pos[i];
+    double rho = k.rho_self;  // 0.0 + mass * W(0)
+    const uint32_t nv = l.nvisit[i];
+    for (uint32_t t = 0; t < nv; ++t) {
+        uint32_t e = l.visit[list_index(i, t, l.capv)];
+        uint32_t j = e & kEntrySlotMask;
+        double4 xj = s.pos[j];
+        double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
+        double r = sqrt(dx * dx + dy * dy + dz * dz);
+        double wij = cubic_w(r, k.h, k.alpha);
+        if (e & kEntryBoundary) {
+            if ((e & kEntryOriented) && !sees_fluid(k, xj, s.nout[j], xi.x, xi.y, xi.z)) continue;
+            rho += k.rho0 * xj.w * wij;
+        } else {
+            rho += k.mass * wij;
+        }
+    }
+    s.vel[i].w = fmax(rho, 1e-12);  // wcsph.rs:152 (f64::max)
+}
+
+__global__ void k_vmax(uint32_t n, StateBufs s, DeviceScalars* sc) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    double m = 0.0;
+    if (i < n && !(s.flags[i] & kFlagBoundary)) {
+        double4 v = s.vel[i];
+        double q = v.x * v.x + v.y * v.y + v.z * v.z;
+        if (q > m) m = q;  // viscosity.rs:91-96 (NaN never exceeds m)
+    }
+    unsigned long long b = __double_as_longlong(m);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        unsigned long long x = __shfl_xor_sync(0xffffffffu, b, o);
+        b = x > b ? x : b;
+    }
+    // Non-negative doubles order like their bit patterns.
+    if ((threadIdx.x & 31u) == 0 && b != 0ull) atomicMax(&sc->vmax2_bits, b);
+}
+
+__global__ void k_pressure(uint32_t n, StepConst k, StateBufs s, DeviceScalars* sc) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    // compute_pressure (wcsph.rs:158-169): c = max(c, 10 * v_max), persisted.
+    // Every thread derives the same c; re-reading an already-updated c gives
+    // the same value (the update is idempotent), so the write is race-free in
+    // effect.
+    double c = sc->sound_speed;
+    if (k.adapt_sound_speed) {
+        double vmax = sqrt(__longlong_as_double((long long)sc->vmax2_bits));
+        double min_c = 10.0 * fmax(vmax, 0.0);
+        c = c < min_c ? min_c : c;
+    }
+    if (i == 0) sc->sound_speed = c;
+    if (i >= n) return;
+    if (s.flags[i] & kFlagBoundary) {
+        s.p[i] = 0.0;
+        return;
+    }
+    double rho = s.vel[i].w;
+    double ratio = rho / k.eos_rho0;
+    double b = k.eos_rho0 * c * c / k.eos_gamma;
+    double pw = k.gamma_is_int ? pow_int_dd(ratio, k.gamma_int) : pow(ratio, k.eos_gamma);
+    double p = b * (pw - 1.0);
+    s.p[i] = p;
+    s.pos[i].w = p / (rho * rho);  // p_i / (rho_i * rho_i), used by every pair of i
+}
+
+// Pressure + Monaghan viscosity force of fluid pair (k, j), seen from k:
+// rx = x_j - x_k (wcsph.rs:219), pi_ij(x_k, x_j, v_k, v_j, rho_k, rho_j).
+__device__ __forceinline__ void fluid_pair(const StepConst& kc, double c0, double4 xk, double4 vk,
+                                           double4 xj, double4 vj, double& ax, double& ay,
+                                           double& az) {
+    double rx = xj.x - xk.x, ry = xj.y - xk.y, rz = xj.z - xk.z;
+    double r2 = rx * rx + ry * ry + rz * rz;
+    double r = sqrt(r2);
+    if (r < 1e-30) return;
+    double dwdr = cubic_dwdr(r, kc.h, kc.alpha);
+    double sc = -dwdr / r;
+    double gx = rx * sc, gy = ry * sc, gz = rz * sc;
+    double press = xk.w + xj.w;  // p_k/rho_k^2 + p_j/rho_j^2
+    double mp = -kc.mass * press;
+    double fx = gx * mp, fy = gy * mp, fz = gz * mp;
+    // viscosity.rs:51-73 with r_ij = x_k - x_j, v_ij = v_k - v_j
+    double qx = xk.x - xj.x, qy = xk.y - xj.y, qz = xk.z - xj.z;
+    double wx = vk.x - vj.x, wy = vk.y - vj.y, wz = vk.z - vj.z;
+    double vr = wx * qx + wy * qy + wz * qz;
+    double pi = 0.0;
+    if (!(vr >= 0.0)) {
+        double q2 = qx * qx + qy * qy + qz * qz;
+        double mu = kc.h * vr / (q2 + kc.eps_h2);
+        double rho_bar = 0.5 * (vk.w + vj.w);
+        pi = (-kc.visc_alpha * c0 * mu + kc.visc_beta * mu * mu) / rho_bar;
+    }
+    double mv = -kc.mass * pi;
+    ax += fx + gx * mv;
+    ay += fy + gy * mv;
+    az += fz + gz * mv;
+}
+
+// Akinci boundary pressure of fluid k against boundary sample j (wcsph.rs:244-255).
+__device__ __forceinline__ void boundary_pair(const StepConst& kc, double4 xk, double4 xj,
+                                              bool oriented, const double4* nout, uint32_t j,
+                                              double& ax, double& ay, double& az) {
+    double rx = xj.x - xk.x, ry = xj.y - xk.y, rz = xj.z - xk.z;
+    double r2 = rx * rx + ry * ry + rz * rz;
+    double r = sqrt(r2);
+    if (r < 1e-30) return;
+    if (oriented && !sees_fluid(kc, xj, nout[j], xk.x, xk.y, xk.z)) return;
+    double dwdr = cubic_dwdr(r, kc.h, kc.alpha);
+    double sc = -dwdr / r;
+    double gx = rx * sc, gy = ry * sc, gz = rz * sc;
+    double m = -(kc.rho0 * xj.w) * xk.w;  // -(rho0 psi_j) * p_k/rho_k^2
+    ax += gx * m;
+    ay += gy * m;
+    az += gz * m;
+}
+
+template <bool INTEGRATE, int DIM>
+__global__ void __launch_bounds__(kThreads) k_forces(uint32_t n, StepConst kc, StateBufs s,
+                                                     ListBufs l, const DeviceScalars* sc,
+                                                     double dt, double4* __restrict__ pos_next,
+                                                     double4* __restrict__ vel_next) {
+    uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    if (s.flags[k] & kFlagBoundary) return;
+    const double c0 = sc->sound_speed;
+    const double4 xk = s.pos[k];
+    const double4 vk = s.vel[k];
+    double ax = 0.0, ay = 0.0, az = 0.0;
+    // fluid i < k, ascending original index
+    const uint32_t nl = l.nlower[k];
+    for (uint32_t t = 0; t < nl; ++t) {
+        uint32_t j = l.lower[list_index(k, t, l.capl)];
+        fluid_pair(kc, c0, xk, vk, s.pos[j], s.vel[j], ax, ay, az);
+    }
+    // fluid j > k and boundary j, visiting order
+    const uint32_t nv = l.nvisit[k];
+    for (uint32_t t = 0; t < nv; ++t) {
+        uint32_t e = l.visit[list_index(k, t, l.capv)];
+        if (e & kEntryLower) continue;
+        uint32_t j = e & kEntrySlotMask;
+        if (e & kEntryBoundary) {
+            boundary_pair(kc, xk, s.pos[j], (e & kEntryOriented) != 0u, s.nout, j, ax, ay, az);
+        } else {
+            fluid_pair(kc, c0, xk, vk, s.pos[j], s.vel[j], ax, ay, az);
+        }
+    }
+    ax += kc.gx;
+    ay += kc.gy;
+    az += kc.gz;
+    s.acc[k] = make_double4(ax, ay, az, 0.0);
+    if (INTEGRATE) {
+        // wcsph.rs:336-341 symplectic Euler
+        double vx = vk.x + ax * dt, vy = vk.y + ay * dt, vz = vk.z + az * dt;
+        double px = xk.x + vx * dt, py = xk.y + vy * dt, pz = xk.z + vz * dt;
+        if (DIM == 2) {
+            pz = 0.0;
+            vz = 0.0;
+        }
+        pos_next[k] = make_double4(px, py, pz, xk.w);
+        vel_next[k] = make_double4(vx, vy, vz, vk.w);
+    }
+}
+
+// boundary_force[j] (wcsph.rs:254): sum over fluid i in ascending index of
+// f(i,j) * (-m) with f = gradW(x_j - x_i) * (-(rho0 psi_j) * p_i/rho_i^2).
+__global__ void __launch_bounds__(kThreads) k_boundary_force(uint32_t n, StepConst kc, StateBufs s,
+                                                             ListBufs l) {
+    uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= n) return;
+    if (!(s.flags[b] & kFlagBoundary)) return;
+    const double4 xb = s.pos[b];
+    const bool oriented = (s.flags[b] & kFlagOriented) != 0;
+    const double4 nb = oriented ? s.nout[b] : make_double4(0, 0, 0, 0);
+    const double mpsi = -(kc.rho0 * xb.w);
+    const double mneg = -kc.mass;
+    double fx = 0.0, fy = 0.0, fz = 0.0;
+    const uint32_t nl = l.nlower[b];
+    for (uint32_t t = 0; t < nl; ++t) {
+        uint32_t i = l.lower[list_index(b, t, l.capl)];
+        double4 xi = s.pos[i];
+        double rx = xb.x - xi.x, ry = xb.y - xi.y, rz = xb.z - xi.z;
+        double r2 = rx * rx + ry * ry + rz * rz;
+        double r = sqrt(r2);
+        if (r < 1e-30) continue;
+        if (oriented && !sees_fluid(kc, xb, nb, xi.x, xi.y, xi.z)) continue;
+        double dwdr = cubic_dwdr(r, kc.h, kc.alpha);
+        double sc = -dwdr / r;
+        double m = mpsi * xi.w;
+        double ffx = (rx * sc) * m, ffy = (ry * sc) * m, ffz = (rz * sc) * m;
+        fx += ffx * mneg;
+        fy += ffy * mneg;
+        fz += ffz * mneg;
+    }
+    s.bf[b] = make_double4(fx, fy, fz, 0.0);
+}
+
+__global__ void __launch_bounds__(kThreads) k_xsph(uint32_t n, StepConst kc, StateBufs s,
+                                                   ListBufs l, double4* __restrict__ vel_out) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double4 vi = s.vel[i];
+    if (s.flags[i] & kFlagBoundary) {
+        vel_out[i] = vi;
+        return;
+    }
+    const double4 xi = s.pos[i];
+    double dvx = 0.0, dvy = 0.0, dvz = 0.0;
+    const uint32_t nv = l.nvisit[i];
+    for (uint32_t t = 0; t < nv; ++t) {
+        uint32_t e = l.visit[list_index(i, t, l.capv)];
+        if (e & kEntryBoundary) continue;
+        uint32_t j = e & kEntrySlotMask;
+        double4 xj = s.pos[j];
+        double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
+        double r = sqrt(dx * dx + dy * dy + dz * dz);
+        double wij = cubic_w(r, kc.h, kc.alpha);
+        double4 vj = s.vel[j];
+        double rho_bar = 0.5 * (vi.w + vj.w);
+        double f = kc.mass / rho_bar * wij;
+        dvx += (vj.x - vi.x) * f;
+        dvy += (vj.y - vi.y) * f;
+        dvz += (vj.z - vi.z) * f;
+    }
+    vel_out[i] = make_double4(vi.x + dvx * kc.xsph_eps, vi.y + dvy * kc.xsph_eps,
+                              vi.z + dvz * kc.xsph_eps, vi.w);
+}
+
+__global__ void k_in_support(uint32_t n, StepConst kc, StateBufs s, ListBufs l, uint32_t* out) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (s.flags[i] & kFlagBoundary) {
+        out[i] = 0;
+        return;
+    }
+    const double4 xi = s.pos[i];
+    uint32_t c = 0;
+    const uint32_t nv = l.nvisit[i];
+    for (uint32_t t = 0; t < nv; ++t) {
+        uint32_t j = l.visit[list_index(i, t, l.capv)] & kEntrySlotMask;
+        double4 xj = s.pos[j];
+        double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
+        double r = sqrt(dx * dx + dy * dy + dz * dz);
+        c += (r / kc.h) < 2.0;
+    }
+    out[i] = c;
+}
+
+}  // namespace
+
+void launch_density(uint32_t n, const StepConst& k, const StateBufs& s, const ListBufs& l,
+                    cudaStream_t st) {
+    if (n) k_density<<<blocks_for(n, kThreads), kThreads, 0, st>>>(n, k, s, l);
+}
+
+void launch_vmax(uint32_t n, const StateBufs& s, DeviceScalars* sc, cudaStream_t st) {
+    if (n) k_vmax<<<blocks_for(n, 256), 256, 0, st>>>(n, s, sc);
+}
+
+void launch_pressure(uint32_t n, const StepConst& k, const StateBufs& s, DeviceScalars* sc,
+                     cudaStream_t st) {
+    k_pressure<<<blocks_for(n ? n : 1, 256), 256, 0, st>>>(n, k, s, sc);
+}
+
+void launch_forces(uint32_t n, const StepConst& k, const StateBufs& s, const ListBufs& l,
+                   const DeviceScalars* sc, bool integrate, double dt, double4* pos_next,
+                   double4* vel_next, cudaStream_t st) {
+    if (!n) return;
+    uint32_t b = blocks_for(n, kThreads);
+    if (k.dim == 3) {
+        if (integrate) k_forces<true, 3><<<b, kThreads, 0, st>>>(n, k, s, l, sc, dt, pos_next, vel_next);
+        else k_forces<false, 3><<<b, kThreads, 0, st>>>(n, k, s, l, sc, dt, pos_next, vel_next);
+    } else {
+        if (integrate) k_forces<true, 2><<<b, kThreads, 0, st>>>(n, k, s, l, sc, dt, pos_next, vel_next);
+        else k_forces<false, 2><<<b, kThreads, 0, st>>>(n, k, s, l, sc, dt, pos_next, vel_next);
+    }
+}
+
+void launch_boundary_force(uint32_t n, const StepConst& k, const StateBufs& s, const ListBufs& l,
+                           cudaStream_t st) {
+    if (n) k_boundary_force<<<blocks_for(n, kThreads), kThreads, 0, st>>>(n, k, s, l);
+}
+
+void launch_xsph(uint32_t n, const StepConst& k, const StateBufs& s, const ListBufs& l,
+                 double4* vel_out, cudaStream_t st) {
+    if (n) k_xsph<<<blocks_for(n, kThreads), kThreads, 0, st>>>(n, k, s, l, vel_out);
+}
+
+void launch_in_support_counts(uint32_t n, const StepConst& k, const StateBufs& s,
+                              const ListBufs& l, uint32_t* out, cudaStream_t st) {
+    if (n) k_in_support<<<blocks_for(n, 256), 256, 0, st>>>(n, k, s, l, out);
+}
+
+}  // namespace pe

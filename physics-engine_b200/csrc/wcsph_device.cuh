@@ -1,0 +1,149 @@
+// Device data layout and kernel entry points of the B200 WCSPH step.
+//
+// Layout in HBM (one world):
+//   * particle state in cell-sorted order ("slots"), structure of double4:
+//       pos4[s] = (x, y, z, w)   w = psi for boundary samples,
+//                                w = p / rho^2 for fluid (written by the
+//                                pressure pass, read by the force pass)
+//       vel4[s] = (vx, vy, vz, rho)
+//     plus acc4 (a), bf4 (boundary reaction force), p (pressure), flags (u8:
+//     bit0 boundary, bit1 oriented boundary), orig (slot -> original index),
+//     nout4 (outward normal of oriented boundary samples), key4 (cell key).
+//   * a dense cell grid over a fixed key box (ix-major linearisation, so the
+//     linear cell order equals the reference's CellKey order), cell_start,
+//     and the list of occupied cells.
+//   * per-slot neighbour lists (warp-interleaved, see list_index): the
+//     "visit" list holds in-support candidates in the reference's visiting
+//     order; the "lower" list holds, for fluid slots, the fluid neighbours
+//     with a lower original index in ascending original-index order, and,
+//     for boundary slots, all fluid neighbours in ascending original index.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace pe {
+
+constexpr uint8_t kFlagBoundary = 1u;
+constexpr uint8_t kFlagOriented = 2u;
+
+// List entry: slot in bits 0..28, flags above.
+constexpr uint32_t kEntrySlotMask = (1u << 29) - 1u;
+constexpr uint32_t kEntryOriented = 1u << 29;
+constexpr uint32_t kEntryLower = 1u << 30;
+constexpr uint32_t kEntryBoundary = 1u << 31;
+constexpr uint64_t kMaxParticles = (1ull << 29) - 1ull;
+
+// Sticky device status bits.
+constexpr uint32_t kStatusDomain = 1u;        // a particle left the grid domain
+constexpr uint32_t kStatusListOverflow = 2u;  // a neighbour list hit its capacity
+constexpr uint32_t kStatusNonFinite = 4u;     // non-finite position seen by the grid
+constexpr uint32_t kStatusSlowUnion = 8u;     // informational: a cell used the slow list path
+
+struct GridDesc {
+    int32_t kx0, ky0, kz0;  // key of dense cell (0,0,0)
+    int32_t nx, ny, nz;     // dense extents
+    uint32_t ncell;         // nx*ny*nz
+    double inv_cell;        // 1.0 / cell_size (grid.rs:63)
+    double cell_size;
+    int dim;
+};
+
+struct StepConst {
+    int dim;
+    double h, mass, rho0;      // particles.h, .mass, .rest_density
+    double alpha;              // cubic_alpha(h, dim)
+    double rho_self;           // 0.0 + mass * W(0)
+    double visc_alpha, visc_beta, eps_h2;  // eps_h2 = visc.eps * h * h
+    double eos_rho0, eos_gamma;
+    int gamma_int, gamma_is_int;
+    double gx, gy, gz;
+    double xsph_eps;
+    double boundary_eps_h;     // 0.15 * h (particles.rs:132)
+    int adapt_sound_speed;
+    float r2_filter;           // conservative single-precision (2h)^2 bound
+};
+
+struct StateBufs {
+    double4* pos;
+    double4* vel;
+    double4* acc;
+    double4* bf;
+    double* p;
+    uint8_t* flags;
+    uint32_t* orig;
+    double4* nout;
+    int4* key;
+};
+
+struct ListBufs {
+    uint32_t* visit;
+    uint32_t* lower;
+    uint32_t* nvisit;
+    uint32_t* nlower;
+    uint32_t* ncand;
+    uint32_t capv, capl;
+};
+
+// Warp-interleaved list storage: entry t of slot s.
+__host__ __device__ __forceinline__ size_t list_index(uint32_t s, uint32_t t, uint32_t cap) {
+    return ((size_t)(s >> 5) * cap + t) * 32u + (s & 31u);
+}
+
+struct DeviceScalars {
+    unsigned long long vmax2_bits;  // max |v|^2 of fluid as u64 bits
+    double sound_speed;             // persisted c (wcsph.rs:168)
+    uint32_t status;
+    uint32_t nocc;                  // occupied cells
+    uint32_t max_union;             // largest neighbour-cell union seen by the list build
+    uint32_t pad;
+};
+
+// ----- grid build -----
+void launch_cell_ids(const GridDesc& g, uint32_t n, const double4* pos_cur, const double4* pos_next,
+                     const uint8_t* flags, uint32_t* cellid, int4* key_tmp, uint32_t* count,
+                     DeviceScalars* sc, cudaStream_t st);
+size_t scan_temp_bytes(uint32_t ncell);
+void launch_scan_cells(uint32_t ncell, const uint32_t* count, uint32_t* cell_start, uint32_t* occ,
+                       DeviceScalars* sc, void* temp, cudaStream_t st);
+void launch_place(uint32_t n, const uint32_t* cellid, const uint32_t* cell_start, uint32_t* fill,
+                  const uint32_t* orig, uint32_t* tmp_old, uint32_t* tmp_orig, cudaStream_t st);
+void launch_cellsort(uint32_t ncell_max, const uint32_t* occ, const DeviceScalars* sc,
+                     const uint32_t* cell_start, const uint32_t* tmp_old, const uint32_t* tmp_orig,
+                     uint32_t* perm, cudaStream_t st);
+void launch_gather(uint32_t n, const uint32_t* perm, const StateBufs& src, const double4* pos_next,
+                   const double4* vel_next, const int4* key_tmp, const StateBufs& dst,
+                   uint32_t* slot_of_orig, double rho0, cudaStream_t st);
+
+// ----- neighbour lists -----
+uint32_t nlist_union_capacity(uint32_t max_union);
+size_t nlist_smem_bytes(uint32_t ucap);
+// Sets the dynamic shared-memory limit of the list kernel for this stage size
+// and returns how many of its CTAs fit on one SM.
+uint32_t nlist_prepare(int dim, uint32_t ucap);
+void launch_nlist(const GridDesc& g, const StepConst& k, uint32_t ucap, uint32_t nblocks,
+                  const uint32_t* occ, const uint32_t* cell_start, const StateBufs& s,
+                  const ListBufs& l, DeviceScalars* sc, cudaStream_t st);
+
+// ----- SPH passes -----
+void launch_density(uint32_t n, const StepConst& k, const StateBufs& s, const ListBufs& l,
+                    cudaStream_t st);
+void launch_vmax(uint32_t n, const StateBufs& s, DeviceScalars* sc, cudaStream_t st);
+void launch_pressure(uint32_t n, const StepConst& k, const StateBufs& s, DeviceScalars* sc,
+                     cudaStream_t st);
+void launch_forces(uint32_t n, const StepConst& k, const StateBufs& s, const ListBufs& l,
+                   const DeviceScalars* sc, bool integrate, double dt, double4* pos_next,
+                   double4* vel_next, cudaStream_t st);
+void launch_boundary_force(uint32_t n, const StepConst& k, const StateBufs& s, const ListBufs& l,
+                           cudaStream_t st);
+void launch_xsph(uint32_t n, const StepConst& k, const StateBufs& s, const ListBufs& l,
+                 double4* vel_out, cudaStream_t st);
+
+// ----- exports / diagnostics -----
+void launch_occupied_export(const GridDesc& g, const uint32_t* occ, const DeviceScalars* sc,
+                            const uint32_t* cell_start, const int4* key, int32_t* occ_keys,
+                            uint64_t* ranges, cudaStream_t st);
+void launch_in_support_counts(uint32_t n, const StepConst& k, const StateBufs& s,
+                              const ListBufs& l, uint32_t* out, cudaStream_t st);
+
+}  // namespace pe

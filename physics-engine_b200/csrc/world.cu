@@ -1,0 +1,643 @@
+// Host runtime of the WCSPH world: allocation, the step schedule and the
+// original-order import/export of state. See world.cuh.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <limits>
+
+#include "pe_math.cuh"
+#include "world.cuh"
+
+namespace pe {
+
+namespace {
+
+inline uint32_t blocks_for(uint64_t n, uint32_t t) { return (uint32_t)((n + t - 1) / t); }
+
+// out[orig * 3 + c] = src[slot_of_orig[orig]].{x,y,z}
+__global__ void k_export_vec(uint32_t n, const uint32_t* __restrict__ slot_of_orig,
+                             const double4* __restrict__ src, double* __restrict__ out) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double4 v = src[slot_of_orig[i]];
+    out[3 * (size_t)i] = v.x;
+    out[3 * (size_t)i + 1] = v.y;
+    out[3 * (size_t)i + 2] = v.z;
+}
+
+// component 3 of a double4 array (rho lives in vel.w) or a plain array
+__global__ void k_export_w(uint32_t n, const uint32_t* __restrict__ slot_of_orig,
+                           const double4* __restrict__ src4, const double* __restrict__ src1,
+                           double* __restrict__ out) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint32_t s = slot_of_orig[i];
+    out[i] = src4 ? src4[s].w : src1[s];
+}
+
+__global__ void k_import_vec(uint32_t n, const uint32_t* __restrict__ slot_of_orig,
+                             const double* __restrict__ in, double4* __restrict__ dst,
+                             const uint8_t* __restrict__ flags, int only_fluid) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint32_t s = slot_of_orig[i];
+    if (only_fluid && (flags[s] & kFlagBoundary)) return;
+    double4 v = dst[s];
+    v.x = in[3 * (size_t)i];
+    v.y = in[3 * (size_t)i + 1];
+    v.z = in[3 * (size_t)i + 2];
+    dst[s] = v;
+}
+
+__global__ void k_import_w(uint32_t n, const uint32_t* __restrict__ slot_of_orig,
+                           const double* __restrict__ in, double4* __restrict__ dst4,
+                           double* __restrict__ dst1) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint32_t s = slot_of_orig[i];
+    if (dst4) dst4[s].w = in[i];
+    else dst1[s] = in[i];
+}
+
+__global__ void k_export_u32(uint32_t n, const uint32_t* __restrict__ slot_of_orig,
+                             const uint32_t* __restrict__ src, uint32_t* __restrict__ out) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    out[i] = src[slot_of_orig[i]];
+}
+
+__global__ void k_export_keys(uint32_t n, const uint32_t* __restrict__ slot_of_orig,
+                              const int4* __restrict__ key, int32_t* __restrict__ out) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int4 k = key[slot_of_orig[i]];
+    out[3 * (size_t)i] = k.x;
+    out[3 * (size_t)i + 1] = k.y;
+    out[3 * (size_t)i + 2] = k.z;
+}
+
+__global__ void k_export_kind(uint32_t n, const uint32_t* __restrict__ slot_of_orig,
+                              const uint8_t* __restrict__ flags, uint8_t* __restrict__ out) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    out[i] = flags[slot_of_orig[i]] & kFlagBoundary;
+}
+
+// Fluid slots cache p / rho^2 in pos.w; refresh it after p or rho were set.
+__global__ void k_refresh_pr2(uint32_t n, const uint8_t* __restrict__ flags,
+                              const double* __restrict__ p, double4* __restrict__ pos,
+                              const double4* __restrict__ vel) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || (flags[i] & kFlagBoundary)) return;
+    double rho = vel[i].w;
+    pos[i].w = p[i] / (rho * rho);
+}
+
+}  // namespace
+
+void World::check(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) {
+        throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
+    }
+}
+
+template <typename T>
+T* World::alloc(size_t count) {
+    void* p = nullptr;
+    size_t bytes = std::max<size_t>(count * sizeof(T), 256);
+    check(cudaMalloc(&p, bytes), "cudaMalloc");
+    allocs_.push_back(p);
+    check(cudaMemsetAsync(p, 0, bytes, st_), "cudaMemsetAsync");
+    return static_cast<T*>(p);
+}
+
+World::World(const WorldParams& prm, const WorldConfig& cfg, int dim, double rest_density,
+             double mass, double h, uint64_t n, const double* x, const double* v,
+             const uint8_t* kind, const double* psi, const double* n_out)
+    : dim_(dim), rho0_(rest_density), mass_(mass), h_(h), n_(n), prm_(prm), cfg_(cfg) {
+    if (cfg_.device >= 0) check(cudaSetDevice(cfg_.device), "cudaSetDevice");
+    check(cudaGetDevice(&device_), "cudaGetDevice");
+    check(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking), "cudaStreamCreate");
+    try {
+        // ---- grid domain from the initial keys (grid.rs:62 key_of) ----
+        const double cell = 2.0 * h_;  // support_radius(CubicSpline, h), kernels.rs:32
+        const double inv = 1.0 / cell;
+        long long lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+        for (uint64_t i = 0; i < n_; ++i) {
+            long long k3[3] = {floor_i32(x[3 * i] * inv), floor_i32(x[3 * i + 1] * inv),
+                               dim_ == 2 ? 0 : floor_i32(x[3 * i + 2] * inv)};
+            for (int a = 0; a < 3; ++a) {
+                if (i == 0 || k3[a] < lo[a]) lo[a] = k3[a];
+                if (i == 0 || k3[a] > hi[a]) hi[a] = k3[a];
+            }
+        }
+        double frac = cfg_.domain_margin < 0.0 ? 0.25 : cfg_.domain_margin;
+        long long minc = cfg_.domain_margin_cells ? cfg_.domain_margin_cells : 4;
+        long long ext[3];
+        for (int a = 0; a < 3; ++a) {
+            if (dim_ == 2 && a == 2) {
+                lo[a] = hi[a] = 0;
+                ext[a] = 1;
+                continue;
+            }
+            long long span = hi[a] - lo[a] + 1;
+            long long m = std::max<long long>(minc, (long long)std::ceil(frac * (double)span));
+            lo[a] = std::max<long long>(lo[a] - m, -2147483647LL);
+            hi[a] = std::min<long long>(hi[a] + m, 2147483646LL);
+            ext[a] = hi[a] - lo[a] + 1;
+        }
+        double ncell = (double)ext[0] * (double)ext[1] * (double)ext[2];
+        if (ncell > (double)(1u << 28)) throw std::length_error("grid domain too large");
+        g_.kx0 = (int32_t)lo[0];
+        g_.ky0 = (int32_t)lo[1];
+        g_.kz0 = (int32_t)lo[2];
+        g_.nx = (int32_t)ext[0];
+        g_.ny = (int32_t)ext[1];
+        g_.nz = (int32_t)ext[2];
+        g_.ncell = (uint32_t)ncell;
+        g_.inv_cell = inv;
+        g_.cell_size = cell;
+        g_.dim = dim_;
+
+        refresh_step_const();
+
+        // ---- union stage capacity from the largest initial neighbour-cell union ----
+        std::vector<uint32_t> cnt(g_.ncell, 0);
+        for (uint64_t i = 0; i < n_; ++i) {
+            long long kx = floor_i32(x[3 * i] * inv) - g_.kx0, ky = floor_i32(x[3 * i + 1] * inv) - g_.ky0;
+            long long kz = dim_ == 2 ? 0 : floor_i32(x[3 * i + 2] * inv) - g_.kz0;
+            ++cnt[(uint32_t)((kx * g_.ny + ky) * g_.nz + kz)];
+        }
+        uint32_t max_union = 1;
+        for (int cx = 0; cx < g_.nx; ++cx)
+            for (int cy = 0; cy < g_.ny; ++cy)
+                for (int cz = 0; cz < g_.nz; ++cz) {
+                    if (!cnt[((size_t)cx * g_.ny + cy) * g_.nz + cz]) continue;
+                    uint32_t u = 0;
+                    for (int dx = -1; dx <= 1; ++dx)
+                        for (int dy = -1; dy <= 1; ++dy)
+                            for (int dz = (dim_ == 2 ? 0 : -1); dz <= (dim_ == 2 ? 0 : 1); ++dz) {
+                                int qx = cx + dx, qy = cy + dy, qz = cz + dz;
+                                if (qx < 0 || qy < 0 || qz < 0 || qx >= g_.nx || qy >= g_.ny || qz >= g_.nz) continue;
+                                u += cnt[((size_t)qx * g_.ny + qy) * g_.nz + qz];
+                            }
+                    max_union = std::max(max_union, u);
+                }
+        ucap_ = nlist_union_capacity(max_union);
+
+        // ---- allocations ----
+        const size_t N = std::max<uint64_t>(n_, 1);
+        const size_t npad = (N + 31) / 32 * 32;
+        auto make_state = [&](StateBufs& s) {
+            s.pos = alloc<double4>(N);
+            s.vel = alloc<double4>(N);
+            s.acc = alloc<double4>(N);
+            s.bf = alloc<double4>(N);
+            s.p = alloc<double>(N);
+            s.flags = alloc<uint8_t>(N);
+            s.orig = alloc<uint32_t>(N);
+            s.nout = alloc<double4>(N);
+            s.key = alloc<int4>(N);
+        };
+        make_state(cur_);
+        make_state(alt_);
+        pos_nx_ = alloc<double4>(N);
+        vel_nx_ = alloc<double4>(N);
+        slot_of_orig_ = alloc<uint32_t>(N);
+        cellid_ = alloc<uint32_t>(N);
+        tmp_old_ = alloc<uint32_t>(N);
+        tmp_orig_ = alloc<uint32_t>(N);
+        perm_ = alloc<uint32_t>(N);
+        key_tmp_ = alloc<int4>(N);
+        count_ = alloc<uint32_t>(g_.ncell);
+        fill_ = alloc<uint32_t>(g_.ncell);
+        cell_start_ = alloc<uint32_t>((size_t)g_.ncell + 1);
+        occ_ = alloc<uint32_t>(g_.ncell);
+        scan_tmp_ = alloc<unsigned char>(scan_temp_bytes(g_.ncell));
+        lists_.capv = cfg_.max_neighbours ? cfg_.max_neighbours : 512u;
+        lists_.capl = cfg_.max_lower ? cfg_.max_lower : lists_.capv;
+        lists_.visit = alloc<uint32_t>(npad * lists_.capv);
+        lists_.lower = alloc<uint32_t>(npad * lists_.capl);
+        lists_.nvisit = alloc<uint32_t>(N);
+        lists_.nlower = alloc<uint32_t>(N);
+        lists_.ncand = alloc<uint32_t>(N);
+        insup_ = alloc<uint32_t>(N);
+        sc_ = alloc<DeviceScalars>(1);
+        xfer_ = alloc<double>(N * 4);
+
+        // ---- upload in original order (slot = original index) ----
+        std::vector<double4> hp(N), hv(N), hn(N);
+        std::vector<uint8_t> hf(N, 0);
+        std::vector<uint32_t> ho(N);
+        for (uint64_t i = 0; i < n_; ++i) {
+            bool b = kind[i] != 0;
+            double nx = n_out ? n_out[3 * i] : 0.0, ny = n_out ? n_out[3 * i + 1] : 0.0,
+                   nz = n_out ? n_out[3 * i + 2] : 0.0;
+            hp[i] = make_double4(x[3 * i], x[3 * i + 1], x[3 * i + 2], b ? psi[i] : 0.0);
+            hv[i] = make_double4(v ? v[3 * i] : 0.0, v ? v[3 * i + 1] : 0.0, v ? v[3 * i + 2] : 0.0,
+                                 rest_density);
+            hn[i] = make_double4(nx, ny, nz, 0.0);
+            bool oriented = b && (nx * nx + ny * ny + nz * nz) > 0.0;
+            hf[i] = (b ? kFlagBoundary : 0) | (oriented ? kFlagOriented : 0);
+            ho[i] = (uint32_t)i;
+        }
+        check(cudaMemcpyAsync(cur_.pos, hp.data(), N * sizeof(double4), cudaMemcpyHostToDevice, st_), "upload");
+        check(cudaMemcpyAsync(cur_.vel, hv.data(), N * sizeof(double4), cudaMemcpyHostToDevice, st_), "upload");
+        check(cudaMemcpyAsync(cur_.nout, hn.data(), N * sizeof(double4), cudaMemcpyHostToDevice, st_), "upload");
+        check(cudaMemcpyAsync(cur_.flags, hf.data(), N, cudaMemcpyHostToDevice, st_), "upload");
+        check(cudaMemcpyAsync(cur_.orig, ho.data(), N * sizeof(uint32_t), cudaMemcpyHostToDevice, st_), "upload");
+        check(cudaMemcpyAsync(slot_of_orig_, ho.data(), N * sizeof(uint32_t), cudaMemcpyHostToDevice, st_), "upload");
+        DeviceScalars hs{};
+        hs.sound_speed = prm_.eos_sound_speed;
+        check(cudaMemcpyAsync(sc_, &hs, sizeof(hs), cudaMemcpyHostToDevice, st_), "upload");
+
+        // ---- launch geometry of the list build: a persistent grid ----
+        int sms = 148;
+        check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_), "attribute");
+        sms_ = (uint32_t)sms;
+        configure_lists();
+        check(cudaStreamSynchronize(st_), "create");
+    } catch (...) {
+        for (void* p : allocs_) cudaFree(p);
+        allocs_.clear();
+        if (st_) cudaStreamDestroy(st_);
+        st_ = nullptr;
+        throw;
+    }
+}
+
+World::~World() {
+    if (st_) cudaStreamSynchronize(st_);
+    for (auto& r : recs_) {
+        cudaEventDestroy(r.a);
+        cudaEventDestroy(r.b);
+    }
+    for (cudaEvent_t e : event_pool_) cudaEventDestroy(e);
+    for (void* p : allocs_) cudaFree(p);
+    if (st_) cudaStreamDestroy(st_);
+}
+
+cudaEvent_t World::take_event() {
+    if (!event_pool_.empty()) {
+        cudaEvent_t e = event_pool_.back();
+        event_pool_.pop_back();
+        return e;
+    }
+    cudaEvent_t e;
+    check(cudaEventCreate(&e), "cudaEventCreate");
+    return e;
+}
+
+void World::prof_begin(int phase) {
+    if (!profiling_) return;
+    PhaseRec r{phase, take_event(), take_event()};
+    check(cudaEventRecord(r.a, st_), "cudaEventRecord");
+    recs_.push_back(r);
+}
+
+void World::prof_end() {
+    if (!profiling_ || recs_.empty()) return;
+    check(cudaEventRecord(recs_.back().b, st_), "cudaEventRecord");
+    if (recs_.size() >= 4096) prof_collect();
+}
+
+void World::prof_collect() {
+    check(cudaStreamSynchronize(st_), "profile");
+    for (auto& r : recs_) {
+        float ms = 0.f;
+        check(cudaEventElapsedTime(&ms, r.a, r.b), "cudaEventElapsedTime");
+        prof_ms_[r.phase] += ms;
+        prof_n_[r.phase] += 1;
+        event_pool_.push_back(r.a);
+        event_pool_.push_back(r.b);
+    }
+    recs_.clear();
+}
+
+void World::profile_read(double* ms, uint64_t* count, bool reset) {
+    prof_collect();
+    for (int p = 0; p < kNumPhases; ++p) {
+        if (ms) ms[p] = prof_ms_[p];
+        if (count) count[p] = prof_n_[p];
+        if (reset) {
+            prof_ms_[p] = 0.0;
+            prof_n_[p] = 0;
+        }
+    }
+}
+
+void World::refresh_step_const() {
+    StepConst k{};
+    k.dim = dim_;
+    k.h = h_;
+    k.mass = mass_;
+    k.rho0 = rho0_;
+    k.alpha = cubic_alpha(h_, dim_);
+    // wcsph.rs:133-135: rho = 0.0; rho += mass * w(kern, 0.0, h, dim)
+    k.rho_self = 0.0 + mass_ * cubic_w(0.0, h_, k.alpha);
+    k.visc_alpha = prm_.visc_alpha;
+    k.visc_beta = prm_.visc_beta;
+    k.eps_h2 = prm_.visc_eps * h_ * h_;  // viscosity.rs:63
+    k.eos_rho0 = prm_.eos_rest_density;
+    k.eos_gamma = prm_.eos_gamma;
+    bool is_int = false;
+    k.gamma_int = integer_exponent(prm_.eos_gamma, &is_int);
+    k.gamma_is_int = is_int ? 1 : 0;
+    k.gx = prm_.gravity[0];
+    k.gy = prm_.gravity[1];
+    k.gz = prm_.gravity[2];
+    k.xsph_eps = prm_.xsph_epsilon;
+    k.boundary_eps_h = 0.15 * h_;  // particles.rs:132
+    k.adapt_sound_speed = prm_.adapt_sound_speed;
+    double sup = 2.0 * h_;
+    k.r2_filter = std::nextafter((float)(sup * sup * (1.0 + 1e-4)), std::numeric_limits<float>::infinity());
+    kc_ = k;
+}
+
+void World::set_params(const WorldParams& p) {
+    bool c_changed = p.eos_sound_speed != prm_.eos_sound_speed;
+    prm_ = p;
+    refresh_step_const();
+    if (c_changed) set_sound_speed(p.eos_sound_speed);
+}
+
+double World::sound_speed() {
+    double c = 0.0;
+    check(cudaMemcpyAsync(&c, &sc_->sound_speed, sizeof(double), cudaMemcpyDeviceToHost, st_), "get c");
+    check(cudaStreamSynchronize(st_), "get c");
+    prm_.eos_sound_speed = c;
+    return c;
+}
+
+void World::set_sound_speed(double c) {
+    prm_.eos_sound_speed = c;
+    check(cudaMemcpyAsync(&sc_->sound_speed, &c, sizeof(double), cudaMemcpyHostToDevice, st_), "set c");
+    check(cudaStreamSynchronize(st_), "set c");
+}
+
+void World::synchronize() { check(cudaStreamSynchronize(st_), "synchronize"); }
+
+void World::build_grid(const double4* pos_next, const double4* vel_next) {
+    const uint32_t n = (uint32_t)n_;
+    prof_begin(kGrid);
+    check(cudaMemsetAsync(count_, 0, sizeof(uint32_t) * g_.ncell, st_), "memset");
+    check(cudaMemsetAsync(fill_, 0, sizeof(uint32_t) * g_.ncell, st_), "memset");
+    launch_cell_ids(g_, n, cur_.pos, pos_next, cur_.flags, cellid_, key_tmp_, count_, sc_, st_);
+    launch_scan_cells(g_.ncell, count_, cell_start_, occ_, sc_, scan_tmp_, st_);
+    launch_place(n, cellid_, cell_start_, fill_, cur_.orig, tmp_old_, tmp_orig_, st_);
+    launch_cellsort(std::min<uint32_t>(g_.ncell, n ? n : 1), occ_, sc_, cell_start_, tmp_old_, tmp_orig_,
+                    perm_, st_);
+    launch_gather(n, perm_, cur_, pos_next, vel_next, key_tmp_, alt_, slot_of_orig_, rho0_, st_);
+    launches_ += 7;
+    prof_end();
+    std::swap(cur_, alt_);
+    grid_built_ = true;
+    lists_valid_ = false;
+    check(cudaGetLastError(), "grid build");
+}
+
+void World::ensure_lists() {
+    if (lists_valid_) return;
+    if (!grid_built_) {
+        // No grid yet: every neighbour query of the reference returns nothing.
+        check(cudaMemsetAsync(lists_.nvisit, 0, sizeof(uint32_t) * n_, st_), "memset");
+        check(cudaMemsetAsync(lists_.nlower, 0, sizeof(uint32_t) * n_, st_), "memset");
+        check(cudaMemsetAsync(lists_.ncand, 0, sizeof(uint32_t) * n_, st_), "memset");
+    } else {
+        prof_begin(kLists);
+        launch_nlist(g_, kc_, ucap_, nl_blocks_, occ_, cell_start_, cur_, lists_, sc_, st_);
+        prof_end();
+        launches_ += 1;
+    }
+    check(cudaGetLastError(), "neighbour lists");
+    lists_valid_ = true;
+}
+
+void World::run_density() {
+    ensure_lists();
+    prof_begin(kDensity);
+    launch_density((uint32_t)n_, kc_, cur_, lists_, st_);
+    prof_end();
+    launches_ += 1;
+    check(cudaGetLastError(), "density");
+}
+
+void World::run_pressure() {
+    prof_begin(kPressure);
+    check(cudaMemsetAsync(&sc_->vmax2_bits, 0, sizeof(unsigned long long), st_), "memset");
+    if (kc_.adapt_sound_speed) {
+        launch_vmax((uint32_t)n_, cur_, sc_, st_);
+        launches_ += 1;
+    }
+    launch_pressure((uint32_t)n_, kc_, cur_, sc_, st_);
+    prof_end();
+    launches_ += 1;
+    check(cudaGetLastError(), "pressure");
+}
+
+void World::run_forces(bool integrate, double dt) {
+    ensure_lists();
+    prof_begin(kForces);
+    launch_forces((uint32_t)n_, kc_, cur_, lists_, sc_, integrate, dt, pos_nx_, vel_nx_, st_);
+    prof_end();
+    prof_begin(kBoundaryForce);
+    launch_boundary_force((uint32_t)n_, kc_, cur_, lists_, st_);
+    prof_end();
+    launches_ += 2;
+    check(cudaGetLastError(), "forces");
+}
+
+void World::run_xsph() {
+    if (prm_.xsph_epsilon == 0.0) return;  // wcsph.rs:285
+    ensure_lists();
+    prof_begin(kXsph);
+    launch_xsph((uint32_t)n_, kc_, cur_, lists_, vel_nx_, st_);
+    prof_end();
+    launches_ += 1;
+    check(cudaGetLastError(), "xsph");
+    std::swap(cur_.vel, vel_nx_);
+    // the swapped-out buffer of the alternate state must stay a valid full copy
+    // only for the current layout, which vel_nx_ is not needed for.
+}
+
+void World::rebuild_grid() {
+    build_grid(nullptr, nullptr);
+    grid_current_ = true;
+    rho_current_ = false;
+}
+
+void World::compute_density() {
+    run_density();
+    rho_current_ = grid_current_;
+}
+
+void World::compute_pressure() { run_pressure(); }
+
+void World::compute_forces() { run_forces(false, 0.0); }
+
+void World::apply_xsph() { run_xsph(); }
+
+void World::step(double dt) {
+    // wcsph.rs:327-328. When the previous step ended with a grid and densities
+    // of the current positions, rebuilding them reproduces the same bits, so
+    // they are reused.
+    if (!(grid_current_ && rho_current_)) {
+        build_grid(nullptr, nullptr);
+        run_density();
+    }
+    run_pressure();               // wcsph.rs:329
+    run_forces(true, dt);         // wcsph.rs:330-342 (kick + drift fused)
+    build_grid(pos_nx_, vel_nx_); // wcsph.rs:343
+    run_density();                // wcsph.rs:344
+    run_xsph();                   // wcsph.rs:345
+    t_ += dt;                     // wcsph.rs:346
+    grid_current_ = true;
+    rho_current_ = true;
+}
+
+void World::run(double dt, uint64_t steps) {
+    for (uint64_t s = 0; s < steps; ++s) {
+        step(dt);
+        if ((s & 63u) == 63u) status();  // lets the list stage grow if needed
+    }
+}
+
+void World::configure_lists() {
+    uint32_t per_sm = nlist_prepare(dim_, ucap_);
+    check(cudaGetLastError(), "nlist prepare");
+    nl_blocks_ = sms_ * std::max<uint32_t>(per_sm, 1u) * 4u;
+}
+
+uint32_t World::status() {
+    DeviceScalars hs{};
+    check(cudaMemcpyAsync(&hs, sc_, sizeof(hs), cudaMemcpyDeviceToHost, st_), "status");
+    check(cudaStreamSynchronize(st_), "status");
+    // Grow the shared-memory stage of the list build when the fluid has
+    // packed more particles into a neighbourhood than it holds.
+    if (hs.max_union > ucap_) {
+        uint32_t want = nlist_union_capacity(hs.max_union);
+        if (want > ucap_) {
+            ucap_ = want;
+            configure_lists();
+        }
+    }
+    return hs.status;
+}
+
+void World::clear_status() {
+    check(cudaMemsetAsync(&sc_->status, 0, sizeof(uint32_t), st_), "status");
+    check(cudaStreamSynchronize(st_), "status");
+}
+
+void World::gather_orig_vec(const double4* src, double* out) {
+    uint32_t n = (uint32_t)n_;
+    if (!n) return;
+    k_export_vec<<<blocks_for(n, 256), 256, 0, st_>>>(n, slot_of_orig_, src, xfer_);
+    check(cudaMemcpyAsync(out, xfer_, sizeof(double) * 3 * n_, cudaMemcpyDeviceToHost, st_), "export");
+    check(cudaStreamSynchronize(st_), "export");
+}
+
+void World::get_vec(int which, double* out) {
+    const double4* src = which == 0 ? cur_.pos : which == 1 ? cur_.vel : which == 2 ? cur_.acc : cur_.bf;
+    gather_orig_vec(src, out);
+}
+
+void World::set_vec(int which, const double* in) {
+    uint32_t n = (uint32_t)n_;
+    if (!n) return;
+    check(cudaMemcpyAsync(xfer_, in, sizeof(double) * 3 * n_, cudaMemcpyHostToDevice, st_), "import");
+    // Velocities of boundary samples are part of the state too (the reference
+    // stores them; they never move), so both kinds are written.
+    k_import_vec<<<blocks_for(n, 256), 256, 0, st_>>>(n, slot_of_orig_, xfer_,
+                                                      which == 0 ? cur_.pos : cur_.vel, cur_.flags, 0);
+    check(cudaStreamSynchronize(st_), "import");
+    if (which == 0) {
+        grid_current_ = false;
+        rho_current_ = false;
+        lists_valid_ = false;
+    }
+}
+
+void World::get_scalar(int which, double* out) {
+    uint32_t n = (uint32_t)n_;
+    if (!n) return;
+    k_export_w<<<blocks_for(n, 256), 256, 0, st_>>>(n, slot_of_orig_, which == 0 ? cur_.vel : nullptr,
+                                                    cur_.p, xfer_);
+    check(cudaMemcpyAsync(out, xfer_, sizeof(double) * n_, cudaMemcpyDeviceToHost, st_), "export");
+    check(cudaStreamSynchronize(st_), "export");
+}
+
+void World::set_scalar(int which, const double* in) {
+    uint32_t n = (uint32_t)n_;
+    if (!n) return;
+    check(cudaMemcpyAsync(xfer_, in, sizeof(double) * n_, cudaMemcpyHostToDevice, st_), "import");
+    k_import_w<<<blocks_for(n, 256), 256, 0, st_>>>(n, slot_of_orig_, xfer_,
+                                                    which == 0 ? cur_.vel : nullptr, cur_.p);
+    k_refresh_pr2<<<blocks_for(n, 256), 256, 0, st_>>>(n, cur_.flags, cur_.p, cur_.pos, cur_.vel);
+    check(cudaStreamSynchronize(st_), "import");
+    if (which == 0) rho_current_ = false;
+}
+
+void World::get_kind(uint8_t* out) {
+    uint32_t n = (uint32_t)n_;
+    if (!n) return;
+    uint8_t* d = reinterpret_cast<uint8_t*>(xfer_);
+    k_export_kind<<<blocks_for(n, 256), 256, 0, st_>>>(n, slot_of_orig_, cur_.flags, d);
+    check(cudaMemcpyAsync(out, d, n_, cudaMemcpyDeviceToHost, st_), "export");
+    check(cudaStreamSynchronize(st_), "export");
+}
+
+void World::get_grid(int32_t* keys, uint64_t* order, int32_t* occupied, uint64_t* ranges,
+                     uint64_t occ_cap, uint64_t* n_occupied) {
+    uint32_t n = (uint32_t)n_;
+    if (!grid_built_) {
+        if (n_occupied) *n_occupied = 0;
+        return;
+    }
+    DeviceScalars hs{};
+    check(cudaMemcpyAsync(&hs, sc_, sizeof(hs), cudaMemcpyDeviceToHost, st_), "grid");
+    check(cudaStreamSynchronize(st_), "grid");
+    if (n_occupied) *n_occupied = hs.nocc;
+    if (keys && n) {
+        int32_t* d = reinterpret_cast<int32_t*>(xfer_);
+        k_export_keys<<<blocks_for(n, 256), 256, 0, st_>>>(n, slot_of_orig_, cur_.key, d);
+        check(cudaMemcpyAsync(keys, d, sizeof(int32_t) * 3 * n_, cudaMemcpyDeviceToHost, st_), "grid");
+        check(cudaStreamSynchronize(st_), "grid");
+    }
+    if (order && n) {
+        std::vector<uint32_t> o(n);
+        check(cudaMemcpyAsync(o.data(), cur_.orig, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, st_), "grid");
+        check(cudaStreamSynchronize(st_), "grid");
+        for (uint32_t s = 0; s < n; ++s) order[s] = o[s];
+    }
+    if ((occupied || ranges) && hs.nocc && occ_cap >= hs.nocc) {
+        int32_t* dk = reinterpret_cast<int32_t*>(xfer_);
+        uint64_t* dr = reinterpret_cast<uint64_t*>(pos_nx_);
+        launch_occupied_export(g_, occ_, sc_, cell_start_, cur_.key, dk, dr, st_);
+        if (occupied)
+            check(cudaMemcpyAsync(occupied, dk, sizeof(int32_t) * 3 * hs.nocc, cudaMemcpyDeviceToHost, st_), "grid");
+        if (ranges)
+            check(cudaMemcpyAsync(ranges, dr, sizeof(uint64_t) * 2 * hs.nocc, cudaMemcpyDeviceToHost, st_), "grid");
+        check(cudaStreamSynchronize(st_), "grid");
+    }
+}
+
+void World::get_neighbour_counts(uint32_t* candidates, uint32_t* in_support) {
+    uint32_t n = (uint32_t)n_;
+    if (!n) return;
+    ensure_lists();
+    uint32_t* d = reinterpret_cast<uint32_t*>(xfer_);
+    if (candidates) {
+        k_export_u32<<<blocks_for(n, 256), 256, 0, st_>>>(n, slot_of_orig_, lists_.ncand, d);
+        check(cudaMemcpyAsync(candidates, d, sizeof(uint32_t) * n_, cudaMemcpyDeviceToHost, st_), "counts");
+        check(cudaStreamSynchronize(st_), "counts");
+    }
+    if (in_support) {
+        launch_in_support_counts(n, kc_, cur_, lists_, insup_, st_);
+        k_export_u32<<<blocks_for(n, 256), 256, 0, st_>>>(n, slot_of_orig_, insup_, d);
+        check(cudaMemcpyAsync(in_support, d, sizeof(uint32_t) * n_, cudaMemcpyDeviceToHost, st_), "counts");
+        check(cudaStreamSynchronize(st_), "counts");
+    }
+}
+
+}  // namespace pe

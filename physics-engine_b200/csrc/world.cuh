@@ -1,0 +1,160 @@
+// Host runtime of one WCSPH world on one GPU (the state machine behind the
+// C ABI). Mirrors `WcsphWorld` (crates/pe-fluid/src/wcsph.rs:58-370): the
+// same phase methods, the same step, the persisted sound speed, and
+// caller-owned host buffers for every getter/setter.
+#pragma once
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "wcsph_device.cuh"
+
+namespace pe {
+
+struct WorldParams {
+    int kernel;  // 0 = cubic spline
+    double eos_rest_density, eos_sound_speed, eos_gamma;
+    double visc_alpha, visc_beta, visc_eps;
+    double xsph_epsilon;
+    double gravity[3];
+    int adapt_sound_speed;
+    double surface_tension_sigma;
+};
+
+struct WorldConfig {
+    int device;                 // CUDA device ordinal (-1 = current)
+    uint32_t max_neighbours;    // visit-list capacity per particle (0 = 512)
+    uint32_t max_lower;         // lower-list capacity per particle (0 = max_neighbours)
+    double domain_margin;       // extra grid domain per side, fraction of extent (<0 = 0.25)
+    uint32_t domain_margin_cells;  // minimum extra cells per side (0 = 4)
+};
+
+class CudaError : public std::runtime_error {
+   public:
+    explicit CudaError(const std::string& s) : std::runtime_error(s) {}
+};
+
+class World {
+   public:
+    World(const WorldParams& prm, const WorldConfig& cfg, int dim, double rest_density, double mass,
+          double h, uint64_t n, const double* x, const double* v, const uint8_t* kind,
+          const double* psi, const double* n_out);
+    ~World();
+    World(const World&) = delete;
+    World& operator=(const World&) = delete;
+
+    // Phase methods (wcsph.rs:102, 117, 157, 181, 283) and the step (wcsph.rs:326).
+    void rebuild_grid();
+    void compute_density();
+    void compute_pressure();
+    void compute_forces();
+    void apply_xsph();
+    void step(double dt);
+    void run(double dt, uint64_t steps);
+    void synchronize();
+
+    uint64_t len() const { return n_; }
+    int dim() const { return dim_; }
+    double time() const { return t_; }
+    void set_time(double t) { t_ = t; }
+    double sound_speed();
+    void set_sound_speed(double c);
+    const WorldParams& params() const { return prm_; }
+    void set_params(const WorldParams& p);
+    double mass() const { return mass_; }
+    double rest_density() const { return rho0_; }
+    double smoothing_length() const { return h_; }
+
+    // Host-buffer access in original particle order.
+    void get_vec(int which, double* out);         // 0 x, 1 v, 2 a, 3 boundary force
+    void set_vec(int which, const double* in);    // 0 x, 1 v
+    void get_scalar(int which, double* out);      // 0 rho, 1 p
+    void set_scalar(int which, const double* in); // 0 rho, 1 p
+    void get_kind(uint8_t* out);
+    void get_grid(int32_t* keys, uint64_t* order, int32_t* occupied, uint64_t* ranges,
+                  uint64_t occ_cap, uint64_t* n_occupied);
+    void get_neighbour_counts(uint32_t* candidates, uint32_t* in_support);
+    uint32_t status();
+    void clear_status();
+
+    // Device views (advanced use: zero-copy access from the same process).
+    const StateBufs& device_state() const { return cur_; }
+    const uint32_t* device_slot_of_orig() const { return slot_of_orig_; }
+    cudaStream_t stream() const { return st_; }
+    uint32_t kernel_launches() const { return launches_; }
+    void reset_launch_count() { launches_ = 0; }
+
+    // Per-phase device time with CUDA events on the world's stream.
+    enum Phase { kGrid = 0, kLists, kDensity, kPressure, kForces, kBoundaryForce, kXsph, kNumPhases };
+    void set_profiling(bool on) { profiling_ = on; }
+    // Accumulated milliseconds and event-bracketed launches per phase since the
+    // last reset; synchronises the stream.
+    void profile_read(double* ms, uint64_t* count, bool reset);
+
+   private:
+    void check(cudaError_t e, const char* what);
+    void build_grid(const double4* pos_next, const double4* vel_next);
+    void ensure_lists();
+    void run_density();
+    void run_pressure();
+    void run_forces(bool integrate, double dt);
+    void run_xsph();
+    void refresh_step_const();
+    void configure_lists();
+    template <typename T>
+    T* alloc(size_t count);
+    void gather_orig_vec(const double4* src, double* out);
+
+    int dim_;
+    double rho0_, mass_, h_;
+    uint64_t n_;
+    WorldParams prm_;
+    WorldConfig cfg_;
+    double t_ = 0.0;
+    int device_ = 0;
+    cudaStream_t st_ = nullptr;
+
+    GridDesc g_{};
+    StepConst kc_{};
+    uint32_t ucap_ = 0, nl_blocks_ = 0, sms_ = 148;
+
+    StateBufs cur_{}, alt_{};
+    double4* pos_nx_ = nullptr;
+    double4* vel_nx_ = nullptr;
+    uint32_t* slot_of_orig_ = nullptr;
+    uint32_t *cellid_ = nullptr, *tmp_old_ = nullptr, *tmp_orig_ = nullptr, *perm_ = nullptr;
+    int4* key_tmp_ = nullptr;
+    uint32_t *count_ = nullptr, *fill_ = nullptr, *cell_start_ = nullptr, *occ_ = nullptr;
+    void* scan_tmp_ = nullptr;
+    ListBufs lists_{};
+    uint32_t* insup_ = nullptr;
+    DeviceScalars* sc_ = nullptr;
+    double* xfer_ = nullptr;  // n * 4 doubles of export/import staging
+    std::vector<void*> allocs_;
+
+    bool grid_built_ = false;    // a grid exists (rebuild_grid ran at least once)
+    bool grid_current_ = false;  // grid built from the current positions
+    bool rho_current_ = false;   // densities computed from the current grid and positions
+    bool lists_valid_ = false;   // neighbour lists match the grid and positions
+    uint32_t launches_ = 0;
+
+    struct PhaseRec {
+        int phase;
+        cudaEvent_t a, b;
+    };
+    bool profiling_ = false;
+    std::vector<PhaseRec> recs_;
+    std::vector<cudaEvent_t> event_pool_;
+    double prof_ms_[kNumPhases] = {};
+    uint64_t prof_n_[kNumPhases] = {};
+    cudaEvent_t take_event();
+    void prof_begin(int phase);
+    void prof_end();
+    void prof_collect();
+};
+
+}  // namespace pe
