@@ -38,6 +38,8 @@ WORKLOADS = {
     # tank grows to 1.62 m in y.
     "dam_break_4m": ((160, 160, 160), (4.0, 1.62, 2.4)),
     "dam_break_32k": ((32, 32, 32), (1.0, 0.4, 0.6)),
+    # mid-size case for profiler captures (~1.5 GB on the device)
+    "dam_break_262k": ((64, 64, 64), (2.56, 1.0, 1.5)),
 }
 DX, DT, SEED, JITTER = 0.01, 1e-4, 0x5EED5EED, 1e-4
 

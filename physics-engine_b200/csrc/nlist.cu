@@ -32,12 +32,7 @@ namespace pe {
 namespace {
 
 constexpr int kNlThreads = 128;
-constexpr uint32_t kMaxUnionStage = 8192;  // 8192 * 24 B = 192 KB of shared memory
-
-__device__ __forceinline__ uint32_t next_pow2(uint32_t v) {
-    if (v <= 1u) return 1u;
-    return 1u << (32 - __clz(v - 1u));
-}
+constexpr uint32_t kMaxUnionStage = 8192;  // 8192 * 24 B + 4 KB = 196 KB of shared memory
 
 __device__ __forceinline__ void emit(uint32_t* list, uint32_t slot, uint32_t t, uint32_t cap,
                                      uint32_t value) {
@@ -62,10 +57,39 @@ __device__ __forceinline__ uint32_t slot_of_union(const uint32_t* s_off, const u
     return s_cstart[lo] + (u - s_off[lo]);
 }
 
+// Block-wide exclusive scan (kNlThreads threads).
+__device__ __forceinline__ void block_exclusive_scan(uint32_t v, uint32_t* ex, uint32_t* total) {
+    __shared__ uint32_t warp_sums[kNlThreads / 32];
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    uint32_t incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t x = __shfl_up_sync(0xffffffffu, incl, o);
+        if ((int)lane >= o) incl += x;
+    }
+    if (lane == 31) warp_sums[warp] = incl;
+    __syncthreads();
+    uint32_t before = 0, tot = 0;
+#pragma unroll
+    for (uint32_t w = 0; w < kNlThreads / 32; ++w) {
+        if (w < warp) before += warp_sums[w];
+        tot += warp_sums[w];
+    }
+    *ex = before + incl - v;
+    *total = tot;
+}
+
 __device__ __forceinline__ uint32_t entry_flags(uint32_t w) {
     return ((w & kStageBoundary) ? kEntryBoundary : 0u) | ((w & kStageOriented) ? kEntryOriented : 0u);
 }
 
+// Shared-memory layout of one CTA (ucap = staged union capacity):
+//   float4   s_pos[ucap]     local coordinates, w = original index | kind flags
+//   uint32   s_ent[ucap]     list entry (slot | boundary | oriented) per position
+//   uint16   s_sorted[ucap]  union positions of the fluid entries, ascending
+//                            original index (radix ping-pong buffer A)
+//   uint16   s_tmp[ucap]     radix ping-pong buffer B
+//   uint16   s_cnt[16][kNlThreads]  radix digit counters
 template <int DIM>
 __global__ void __launch_bounds__(kNlThreads) k_nlist(GridDesc g, StepConst k, uint32_t ucap,
                                                       const uint32_t* __restrict__ occ,
@@ -74,11 +98,14 @@ __global__ void __launch_bounds__(kNlThreads) k_nlist(GridDesc g, StepConst k, u
     constexpr int NC = DIM == 3 ? 27 : 9;
     constexpr int CENTER = DIM == 3 ? 13 : 4;
     extern __shared__ __align__(16) unsigned char smem[];
-    float4* s_pos = reinterpret_cast<float4*>(smem);                                 // ucap
-    unsigned long long* s_key = reinterpret_cast<unsigned long long*>(s_pos + ucap);  // ucap
+    float4* s_pos = reinterpret_cast<float4*>(smem);
+    uint32_t* s_ent = reinterpret_cast<uint32_t*>(s_pos + ucap);
+    uint16_t* s_sorted = reinterpret_cast<uint16_t*>(s_ent + ucap);
+    uint16_t* s_tmp = s_sorted + ucap;
+    uint16_t* s_cnt = s_tmp + ucap;  // 16 * kNlThreads
     __shared__ uint32_t s_cstart[NC];
     __shared__ uint32_t s_off[NC + 1];
-    __shared__ uint32_t s_nf;
+    __shared__ uint32_t s_nf, s_omin, s_omax;
 
     const float r2f = k.r2_filter;
     const uint32_t nocc = sc->nocc;
@@ -117,12 +144,14 @@ __global__ void __launch_bounds__(kNlThreads) k_nlist(GridDesc g, StepConst k, u
             if (tid == 0) {
                 s_off[0] = 0;
                 s_nf = 0;
+                s_omin = 0xffffffffu;
+                s_omax = 0u;
             }
         }
         __syncthreads();
         const uint32_t U = s_off[NC];
         const uint32_t cs = s_cstart[CENTER];
-        const uint32_t ce = cs + (s_off[CENTER + 1] - s_off[CENTER]);
+        const uint32_t ncenter = s_off[CENTER + 1] - s_off[CENTER];
         const double ox = (double)(g.kx0 + cx) * g.cell_size;
         const double oy = (double)(g.ky0 + cy) * g.cell_size;
         const double oz = DIM == 3 ? (double)(g.kz0 + cz) * g.cell_size : 0.0;
@@ -131,104 +160,166 @@ __global__ void __launch_bounds__(kNlThreads) k_nlist(GridDesc g, StepConst k, u
         if (U <= ucap) {
             // ---- stage the union in visiting order ----
             for (uint32_t u = tid; u < U; u += blockDim.x) {
-                uint32_t slot = slot_of_union<NC>(s_off, s_cstart, u);
-                double4 p = s.pos[slot];
-                uint8_t fl = s.flags[slot];
-                uint32_t o = s.orig[slot];
-                uint32_t w = o | ((fl & kFlagBoundary) ? kStageBoundary : 0u) |
-                             ((fl & kFlagOriented) ? kStageOriented : 0u);
+                const uint32_t slot = slot_of_union<NC>(s_off, s_cstart, u);
+                const double4 p = s.pos[slot];
+                const uint8_t fl = s.flags[slot];
+                const uint32_t o = s.orig[slot];
+                const uint32_t w = o | ((fl & kFlagBoundary) ? kStageBoundary : 0u) |
+                                   ((fl & kFlagOriented) ? kStageOriented : 0u);
                 s_pos[u] = make_float4((float)(p.x - ox), (float)(p.y - oy),
                                        DIM == 3 ? (float)(p.z - oz) : 0.0f, __uint_as_float(w));
+                s_ent[u] = slot | entry_flags(w);
                 if (!(fl & kFlagBoundary)) {
-                    uint32_t idx = atomicAdd(&s_nf, 1u);
-                    s_key[idx] = ((unsigned long long)o << 32) | u;
+                    const uint32_t idx = atomicAdd(&s_nf, 1u);
+                    s_sorted[idx] = (uint16_t)u;
+                    atomicMin(&s_omin, o);
+                    atomicMax(&s_omax, o);
                 }
             }
             __syncthreads();
-            // ---- sort the fluid entries by original index (bitonic) ----
+            // ---- sort the fluid positions by original index: LSD radix sort on
+            // 4-bit digits of (orig - min), keys read through the positions ----
             const uint32_t nf = s_nf;
-            const uint32_t P = next_pow2(nf);
-            for (uint32_t i = nf + tid; i < P; i += blockDim.x) s_key[i] = ULLONG_MAX;
-            __syncthreads();
-            for (uint32_t kk = 2; kk <= P; kk <<= 1) {
-                for (uint32_t j = kk >> 1; j > 0; j >>= 1) {
-                    for (uint32_t pr = tid; pr < (P >> 1); pr += blockDim.x) {
-                        uint32_t i = 2u * j * (pr / j) + (pr % j);
-                        uint32_t ij = i + j;
-                        unsigned long long a = s_key[i], b = s_key[ij];
-                        bool up = (i & kk) == 0u;
-                        if ((a > b) == up) {
-                            s_key[i] = b;
-                            s_key[ij] = a;
+            {
+                const uint32_t omin = s_omin;
+                const uint32_t span = nf ? s_omax - omin : 0u;
+                const int npass = span ? (32 - __clz(span) + 3) / 4 : 0;
+                const uint32_t chunk = (nf + kNlThreads - 1) / kNlThreads;
+                const uint32_t e0 = min(nf, tid * chunk), e1 = min(nf, e0 + chunk);
+                uint16_t *src = s_sorted, *dst = s_tmp;
+                for (int pass = 0; pass < npass; ++pass) {
+                    const int shift = 4 * pass;
+#pragma unroll
+                    for (int d = 0; d < 16; ++d) s_cnt[d * kNlThreads + tid] = 0;
+                    for (uint32_t e = e0; e < e1; ++e) {
+                        const uint32_t o = __float_as_uint(s_pos[src[e]].w) & kStageOrigMask;
+                        ++s_cnt[(((o - omin) >> shift) & 15u) * kNlThreads + tid];
+                    }
+                    __syncthreads();
+                    {
+                        // exclusive scan of the counters in (digit, thread) order
+                        uint32_t v[16], sum = 0;
+#pragma unroll
+                        for (int q = 0; q < 16; ++q) {
+                            v[q] = s_cnt[tid * 16 + q];
+                            sum += v[q];
+                        }
+                        uint32_t ex, tot;
+                        block_exclusive_scan(sum, &ex, &tot);
+#pragma unroll
+                        for (int q = 0; q < 16; ++q) {
+                            s_cnt[tid * 16 + q] = (uint16_t)ex;
+                            ex += v[q];
                         }
                     }
                     __syncthreads();
+                    for (uint32_t e = e0; e < e1; ++e) {
+                        const uint16_t pu = src[e];
+                        const uint32_t o = __float_as_uint(s_pos[pu].w) & kStageOrigMask;
+                        const uint32_t d = ((o - omin) >> shift) & 15u;
+                        dst[s_cnt[d * kNlThreads + tid]++] = pu;
+                    }
+                    __syncthreads();
+                    uint16_t* t = src;
+                    src = dst;
+                    dst = t;
+                }
+                if (src != s_sorted) {
+                    for (uint32_t i = tid; i < nf; i += blockDim.x) s_sorted[i] = src[i];
+                    __syncthreads();
                 }
             }
-            // ---- per centre particle ----
-            for (uint32_t kslot = cs + tid; kslot < ce; kslot += blockDim.x) {
-                const uint32_t myu = s_off[CENTER] + (kslot - cs);
+            // ---- per centre particle: a "visit" thread and a "lower" thread in
+            // different warps, working independently ----
+            const uint32_t W = (U + 31u) >> 5;
+            const bool lower_role = tid >= kNlThreads / 2;
+            for (uint32_t pi = tid % (kNlThreads / 2); pi < ncenter; pi += kNlThreads / 2) {
+                const uint32_t kslot = cs + pi;
+                const uint32_t myu = s_off[CENTER] + pi;
                 const float4 me = s_pos[myu];
                 const uint32_t mw = __float_as_uint(me.w);
                 const uint32_t myo = mw & kStageOrigMask;
                 const bool fluid = !(mw & kStageBoundary);
-                uint32_t nl = 0;
-                if (fluid) {
-                    uint32_t nv = 0;
-                    for (uint32_t u = 0; u < U; ++u) {
-                        float4 q = s_pos[u];
-                        float dx = q.x - me.x, dy = q.y - me.y, dz = q.z - me.z;
-                        float d2 = dx * dx + dy * dy + dz * dz;
-                        if (d2 <= r2f && u != myu) {
-                            uint32_t w = __float_as_uint(q.w);
-                            uint32_t e = slot_of_union<NC>(s_off, s_cstart, u) | entry_flags(w);
-                            if (!(w & kStageBoundary) && (w & kStageOrigMask) < myo) e |= kEntryLower;
-                            emit(l.visit, kslot, nv, l.capv, e);
-                            ++nv;
-                        }
-                    }
-                    for (uint32_t i = 0; i < nf; ++i) {
-                        unsigned long long key = s_key[i];
-                        if ((uint32_t)(key >> 32) >= myo) break;
-                        uint32_t u = (uint32_t)key;
-                        float4 q = s_pos[u];
-                        float dx = q.x - me.x, dy = q.y - me.y, dz = q.z - me.z;
-                        float d2 = dx * dx + dy * dy + dz * dz;
-                        if (d2 <= r2f) {
-                            emit(l.lower, kslot, nl, l.capl, slot_of_union<NC>(s_off, s_cstart, u));
-                            ++nl;
+                if (!lower_role) {
+                    uint32_t nv = 0, nu = 0;
+                    if (fluid) {
+                        for (uint32_t w = 0; w < W; ++w) {
+                            uint32_t m = 0;
+#pragma unroll
+                            for (int bit = 0; bit < 32; ++bit) {
+                                const uint32_t u = (w << 5) + bit;
+                                const float4 q = s_pos[u];
+                                const float dx = q.x - me.x, dy = q.y - me.y, dz = q.z - me.z;
+                                const float d2 = dx * dx + dy * dy + dz * dz;
+                                m |= (d2 <= r2f && u < U && u != myu) ? (1u << bit) : 0u;
+                            }
+                            while (m) {
+                                const uint32_t u = (w << 5) + (__ffs(m) - 1);
+                                m &= m - 1u;
+                                const uint32_t ow = __float_as_uint(s_pos[u].w);
+                                uint32_t e = s_ent[u];
+                                if (!(ow & kStageBoundary) && (ow & kStageOrigMask) < myo) {
+                                    e |= kEntryLower;
+                                } else {
+                                    emit(l.upper, kslot, nu, l.capv, e);
+                                    ++nu;
+                                }
+                                emit(l.visit, kslot, nv, l.capv, e);
+                                ++nv;
+                            }
                         }
                     }
                     if (nv > l.capv) { overflow = true; nv = l.capv; }
+                    if (nu > l.capv) nu = l.capv;
                     l.nvisit[kslot] = nv;
-                    l.ncand[kslot] = U;
+                    l.nupper[kslot] = nu;
+                    l.ncand[kslot] = fluid ? U : 0u;
                 } else {
-                    for (uint32_t i = 0; i < nf; ++i) {
-                        uint32_t u = (uint32_t)s_key[i];
-                        float4 q = s_pos[u];
-                        float dx = q.x - me.x, dy = q.y - me.y, dz = q.z - me.z;
-                        float d2 = dx * dx + dy * dy + dz * dz;
-                        if (d2 <= r2f) {
-                            emit(l.lower, kslot, nl, l.capl, slot_of_union<NC>(s_off, s_cstart, u));
+                    // R = number of fluid union entries with a smaller original index
+                    uint32_t R = nf;
+                    if (fluid) {
+                        uint32_t lo = 0, hi = nf;
+                        while (lo < hi) {
+                            const uint32_t mid = (lo + hi) >> 1;
+                            const uint32_t o = __float_as_uint(s_pos[s_sorted[mid]].w) & kStageOrigMask;
+                            if (o < myo) lo = mid + 1;
+                            else hi = mid;
+                        }
+                        R = lo;
+                    }
+                    uint32_t nl = 0;
+                    for (uint32_t i0 = 0; i0 < R; i0 += 32) {
+                        uint32_t m = 0;
+#pragma unroll
+                        for (int bit = 0; bit < 32; ++bit) {
+                            const uint32_t i = i0 + bit;
+                            const float4 q = s_pos[s_sorted[i < nf ? i : 0u]];
+                            const float dx = q.x - me.x, dy = q.y - me.y, dz = q.z - me.z;
+                            const float d2 = dx * dx + dy * dy + dz * dz;
+                            m |= (d2 <= r2f && i < R) ? (1u << bit) : 0u;
+                        }
+                        while (m) {
+                            const uint32_t i = i0 + (__ffs(m) - 1);
+                            m &= m - 1u;
+                            emit(l.lower, kslot, nl, l.capl, s_ent[s_sorted[i]] & kEntrySlotMask);
                             ++nl;
                         }
                     }
-                    l.nvisit[kslot] = 0;
-                    l.ncand[kslot] = 0;
+                    if (nl > l.capl) { overflow = true; nl = l.capl; }
+                    l.nlower[kslot] = nl;
                 }
-                if (nl > l.capl) { overflow = true; nl = l.capl; }
-                l.nlower[kslot] = nl;
             }
         } else {
             // ---- slow path: union larger than the shared-memory stage ----
             if (tid == 0) atomicOr(&sc->status, kStatusSlowUnion);
+            const uint32_t ce = cs + ncenter;
             for (uint32_t kslot = cs + tid; kslot < ce; kslot += blockDim.x) {
                 double4 pm = s.pos[kslot];
                 const float mx = (float)(pm.x - ox), my = (float)(pm.y - oy),
                             mz = DIM == 3 ? (float)(pm.z - oz) : 0.0f;
                 const uint32_t myo = s.orig[kslot];
                 const bool fluid = !(s.flags[kslot] & kFlagBoundary);
-                uint32_t nv = 0, nl = 0;
+                uint32_t nv = 0, nl = 0, nu = 0;
                 if (fluid) {
                     for (int q = 0; q < NC; ++q) {
                         uint32_t q0 = s_cstart[q], q1 = q0 + (s_off[q + 1] - s_off[q]);
@@ -241,7 +332,12 @@ __global__ void __launch_bounds__(kNlThreads) k_nlist(GridDesc g, StepConst k, u
                                 uint8_t fl = s.flags[slot];
                                 uint32_t e = slot | ((fl & kFlagBoundary) ? kEntryBoundary : 0u) |
                                              ((fl & kFlagOriented) ? kEntryOriented : 0u);
-                                if (!(fl & kFlagBoundary) && s.orig[slot] < myo) e |= kEntryLower;
+                                if (!(fl & kFlagBoundary) && s.orig[slot] < myo) {
+                                    e |= kEntryLower;
+                                } else {
+                                    emit(l.upper, kslot, nu, l.capv, e);
+                                    ++nu;
+                                }
                                 emit(l.visit, kslot, nv, l.capv, e);
                                 ++nv;
                             }
@@ -277,6 +373,8 @@ __global__ void __launch_bounds__(kNlThreads) k_nlist(GridDesc g, StepConst k, u
                 }
                 if (nv > l.capv) { overflow = true; nv = l.capv; }
                 if (nl > l.capl) { overflow = true; nl = l.capl; }
+                if (nu > l.capv) nu = l.capv;
+                l.nupper[kslot] = fluid ? nu : 0u;
                 l.nvisit[kslot] = fluid ? nv : 0u;
                 l.nlower[kslot] = nl;
                 l.ncand[kslot] = fluid ? U : 0u;
@@ -300,7 +398,8 @@ uint32_t nlist_union_capacity(uint32_t max_union) {
 }
 
 size_t nlist_smem_bytes(uint32_t ucap) {
-    return (size_t)ucap * (sizeof(float4) + sizeof(unsigned long long));
+    return (size_t)ucap * (sizeof(float4) + sizeof(uint32_t) + 2 * sizeof(uint16_t)) +
+           16 * kNlThreads * sizeof(uint16_t);
 }
 
 uint32_t nlist_prepare(int dim, uint32_t ucap) {

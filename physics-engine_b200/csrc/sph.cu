@@ -32,6 +32,63 @@ constexpr int kThreads = 128;
 
 inline uint32_t blocks_for(uint64_t n, uint32_t t) { return (uint32_t)((n + t - 1) / t); }
 
+// a / h, correctly rounded, in one multiply and two fused multiply-adds.
+// Markstein's theorem: with y = RN(1/h) and q0 = RN(a y) (within one ulp of
+// a/h), the remainder r = a - q0 h is exact in an fma and RN(q0 + r y) =
+// RN(a/h), for results in the normal range. The rare non-finite or tiny
+// operands take the IEEE division.
+__device__ __forceinline__ double div_h(double a, const StepConst& k) {
+    if (!(fabs(a) < 1e300) || fabs(a) < 1e-290) return a / k.h;
+    const double q0 = a * k.inv_h;
+    const double r = fma(-q0, k.h, a);
+    return fma(r, k.inv_h, q0);
+}
+
+// kernels.rs:86 cubic_spline_w with q = r / h by div_h (same bits)
+__device__ __forceinline__ double kern_w(double r, const StepConst& k) {
+    if (r < 0.0) return 0.0;
+    const double q = div_h(r, k);
+    if (q >= 2.0) return 0.0;
+    if (q < 1.0) return k.alpha * (1.0 - 1.5 * q * q + 0.75 * q * q * q);
+    const double t = 2.0 - q;
+    return k.alpha * 0.25 * t * t * t;
+}
+
+// kernels.rs:102 cubic_spline_dwdr with both divisions by h by div_h
+__device__ __forceinline__ double kern_dwdr(double r, const StepConst& k) {
+    const double q = div_h(r, k);
+    if (q >= 2.0 || q <= 0.0) return 0.0;
+    double dwdq;
+    if (q < 1.0) {
+        dwdq = k.alpha * (-3.0 * q + 2.25 * q * q);
+    } else {
+        const double t = 2.0 - q;
+        dwdq = k.alpha * (-0.75 * t * t);
+    }
+    return div_h(dwdq, k);
+}
+
+// Calls f(entry) for the n entries of slot s in order, loading four entries
+// per 16-byte load and issuing the load of the next group before the current
+// group is processed.
+template <class F>
+__device__ __forceinline__ void for_each_entry(const uint32_t* list, uint32_t s, uint32_t n,
+                                               uint32_t cap, F&& f) {
+    if (n == 0) return;
+    const uint32_t ng = (n + 3u) >> 2;
+    uint4 cur = list_group(list, s, 0, cap);
+    for (uint32_t g = 0; g < ng; ++g) {
+        uint4 nxt = cur;
+        if (g + 1 < ng) nxt = list_group(list, s, g + 1, cap);
+        const uint32_t base = g << 2;
+        f(cur.x);
+        if (base + 1 < n) f(cur.y);
+        if (base + 2 < n) f(cur.z);
+        if (base + 3 < n) f(cur.w);
+        cur = nxt;
+    }
+}
+
 // particles.rs:126 boundary_sees_fluid
 __device__ __forceinline__ bool sees_fluid(const StepConst& k, double4 xb, double4 nb,
                                            double xfx, double xfy, double xfz) {
@@ -52,22 +109,22 @@ __global__ void __launch_bounds__(kThreads) k_density(uint32_t n, StepConst k, S
     }
     const double4 xi = s.pos[i];
     double rho = k.rho_self;  // 0.0 + mass * W(0)
-    const uint32_t nv = l.nvisit[i];
-    for (uint32_t t = 0; t < nv; ++t) {
-        uint32_t e = l.visit[list_index(i, t, l.capv)];
-        uint32_t j = e & kEntrySlotMask;
-        double4 xj = s.pos[j];
-        double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
-        double r = sqrt(dx * dx + dy * dy + dz * dz);
-        double wij = cubic_w(r, k.h, k.alpha);
-        if (e & kEntryBoundary) {
-            if ((e & kEntryOriented) && !sees_fluid(k, xj, s.nout[j], xi.x, xi.y, xi.z)) continue;
-            rho += k.rho0 * xj.w * wij;
-        } else {
-            rho += k.mass * wij;
-        }
-    }
-    s.vel[i].w = fmax(rho, 1e-12);  // wcsph.rs:152 (f64::max)
+    for_each_entry(l.visit, i, l.nvisit[i], l.capv, [&](uint32_t e) {
+        const uint32_t j = e & kEntrySlotMask;
+        const double4 xj = s.pos[j];
+        const double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
+        const double r = sqrt(dx * dx + dy * dy + dz * dz);
+        const double wij = kern_w(r, k);
+        if ((e & kEntryOriented) && !sees_fluid(k, xj, s.nout[j], xi.x, xi.y, xi.z)) return;
+        // fluid: mass * W; boundary: (rho0 * psi_j) * W (wcsph.rs:143-148)
+        const double f = (e & kEntryBoundary) ? k.rho0 * xj.w : k.mass;
+        rho += f * wij;
+    });
+    rho = fmax(rho, 1e-12);  // wcsph.rs:152 (f64::max)
+    s.vel[i].w = rho;
+    // keep the cached p / rho^2 consistent with the new rho (the reference
+    // divides the stored p by the current rho in every force pair)
+    s.pos[i].w = s.p[i] / (rho * rho);
 }
 
 __global__ void k_vmax(uint32_t n, StateBufs s, DeviceScalars* sc) {
@@ -117,34 +174,33 @@ __global__ void k_pressure(uint32_t n, StepConst k, StateBufs s, DeviceScalars* 
 
 // Pressure + Monaghan viscosity force of fluid pair (k, j), seen from k:
 // rx = x_j - x_k (wcsph.rs:219), pi_ij(x_k, x_j, v_k, v_j, rho_k, rho_j).
-__device__ __forceinline__ void fluid_pair(const StepConst& kc, double c0, double4 xk, double4 vk,
+__device__ __forceinline__ void fluid_pair(const StepConst& kc, double nac, double4 xk, double4 vk,
                                            double4 xj, double4 vj, double& ax, double& ay,
                                            double& az) {
-    double rx = xj.x - xk.x, ry = xj.y - xk.y, rz = xj.z - xk.z;
-    double r2 = rx * rx + ry * ry + rz * rz;
-    double r = sqrt(r2);
+    const double rx = xj.x - xk.x, ry = xj.y - xk.y, rz = xj.z - xk.z;
+    const double r2 = rx * rx + ry * ry + rz * rz;
+    const double r = sqrt(r2);
     if (r < 1e-30) return;
-    double dwdr = cubic_dwdr(r, kc.h, kc.alpha);
-    double sc = -dwdr / r;
-    double gx = rx * sc, gy = ry * sc, gz = rz * sc;
-    double press = xk.w + xj.w;  // p_k/rho_k^2 + p_j/rho_j^2
-    double mp = -kc.mass * press;
-    double fx = gx * mp, fy = gy * mp, fz = gz * mp;
-    // viscosity.rs:51-73 with r_ij = x_k - x_j, v_ij = v_k - v_j
-    double qx = xk.x - xj.x, qy = xk.y - xj.y, qz = xk.z - xj.z;
-    double wx = vk.x - vj.x, wy = vk.y - vj.y, wz = vk.z - vj.z;
-    double vr = wx * qx + wy * qy + wz * qz;
-    double pi = 0.0;
-    if (!(vr >= 0.0)) {
-        double q2 = qx * qx + qy * qy + qz * qz;
-        double mu = kc.h * vr / (q2 + kc.eps_h2);
-        double rho_bar = 0.5 * (vk.w + vj.w);
-        pi = (-kc.visc_alpha * c0 * mu + kc.visc_beta * mu * mu) / rho_bar;
-    }
-    double mv = -kc.mass * pi;
-    ax += fx + gx * mv;
-    ay += fy + gy * mv;
-    az += fz + gz * mv;
+    const double dwdr = kern_dwdr(r, kc);
+    const double sc = -dwdr / r;
+    const double gx = rx * sc, gy = ry * sc, gz = rz * sc;
+    const double press = xk.w + xj.w;  // p_k/rho_k^2 + p_j/rho_j^2
+    const double mp = -kc.mass * press;
+    // viscosity.rs:51-73 with r_ij = x_k - x_j, v_ij = v_k - v_j. Evaluated for
+    // every pair and selected, so that approaching and receding pairs do not
+    // split the warp; a receding pair's value is discarded (pi = 0 exactly).
+    const double qx = xk.x - xj.x, qy = xk.y - xj.y, qz = xk.z - xj.z;
+    const double wx = vk.x - vj.x, wy = vk.y - vj.y, wz = vk.z - vj.z;
+    const double vr = wx * qx + wy * qy + wz * qz;
+    const double q2 = qx * qx + qy * qy + qz * qz;
+    const double mu = kc.h * vr / (q2 + kc.eps_h2);
+    const double rho_bar = 0.5 * (vk.w + vj.w);
+    const double pic = (nac * mu + kc.visc_beta * mu * mu) / rho_bar;
+    const double pi = vr >= 0.0 ? 0.0 : pic;
+    const double mv = -kc.mass * pi;
+    ax += gx * mp + gx * mv;
+    ay += gy * mp + gy * mv;
+    az += gz * mp + gz * mv;
 }
 
 // Akinci boundary pressure of fluid k against boundary sample j (wcsph.rs:244-255).
@@ -156,7 +212,7 @@ __device__ __forceinline__ void boundary_pair(const StepConst& kc, double4 xk, d
     double r = sqrt(r2);
     if (r < 1e-30) return;
     if (oriented && !sees_fluid(kc, xj, nout[j], xk.x, xk.y, xk.z)) return;
-    double dwdr = cubic_dwdr(r, kc.h, kc.alpha);
+    double dwdr = kern_dwdr(r, kc);
     double sc = -dwdr / r;
     double gx = rx * sc, gy = ry * sc, gz = rz * sc;
     double m = -(kc.rho0 * xj.w) * xk.w;  // -(rho0 psi_j) * p_k/rho_k^2
@@ -174,27 +230,23 @@ __global__ void __launch_bounds__(kThreads) k_forces(uint32_t n, StepConst kc, S
     if (k >= n) return;
     if (s.flags[k] & kFlagBoundary) return;
     const double c0 = sc->sound_speed;
+    const double nac = -kc.visc_alpha * c0;  // (-alpha) * c_bar, viscosity.rs:72
     const double4 xk = s.pos[k];
     const double4 vk = s.vel[k];
     double ax = 0.0, ay = 0.0, az = 0.0;
     // fluid i < k, ascending original index
-    const uint32_t nl = l.nlower[k];
-    for (uint32_t t = 0; t < nl; ++t) {
-        uint32_t j = l.lower[list_index(k, t, l.capl)];
-        fluid_pair(kc, c0, xk, vk, s.pos[j], s.vel[j], ax, ay, az);
-    }
+    for_each_entry(l.lower, k, l.nlower[k], l.capl, [&](uint32_t j) {
+        fluid_pair(kc, nac, xk, vk, s.pos[j], s.vel[j], ax, ay, az);
+    });
     // fluid j > k and boundary j, visiting order
-    const uint32_t nv = l.nvisit[k];
-    for (uint32_t t = 0; t < nv; ++t) {
-        uint32_t e = l.visit[list_index(k, t, l.capv)];
-        if (e & kEntryLower) continue;
-        uint32_t j = e & kEntrySlotMask;
+    for_each_entry(l.upper, k, l.nupper[k], l.capv, [&](uint32_t e) {
+        const uint32_t j = e & kEntrySlotMask;
         if (e & kEntryBoundary) {
             boundary_pair(kc, xk, s.pos[j], (e & kEntryOriented) != 0u, s.nout, j, ax, ay, az);
         } else {
-            fluid_pair(kc, c0, xk, vk, s.pos[j], s.vel[j], ax, ay, az);
+            fluid_pair(kc, nac, xk, vk, s.pos[j], s.vel[j], ax, ay, az);
         }
-    }
+    });
     ax += kc.gx;
     ay += kc.gy;
     az += kc.gz;
@@ -225,23 +277,21 @@ __global__ void __launch_bounds__(kThreads) k_boundary_force(uint32_t n, StepCon
     const double mpsi = -(kc.rho0 * xb.w);
     const double mneg = -kc.mass;
     double fx = 0.0, fy = 0.0, fz = 0.0;
-    const uint32_t nl = l.nlower[b];
-    for (uint32_t t = 0; t < nl; ++t) {
-        uint32_t i = l.lower[list_index(b, t, l.capl)];
+    for_each_entry(l.lower, b, l.nlower[b], l.capl, [&](uint32_t i) {
         double4 xi = s.pos[i];
         double rx = xb.x - xi.x, ry = xb.y - xi.y, rz = xb.z - xi.z;
         double r2 = rx * rx + ry * ry + rz * rz;
         double r = sqrt(r2);
-        if (r < 1e-30) continue;
-        if (oriented && !sees_fluid(kc, xb, nb, xi.x, xi.y, xi.z)) continue;
-        double dwdr = cubic_dwdr(r, kc.h, kc.alpha);
+        if (r < 1e-30) return;
+        if (oriented && !sees_fluid(kc, xb, nb, xi.x, xi.y, xi.z)) return;
+        double dwdr = kern_dwdr(r, kc);
         double sc = -dwdr / r;
         double m = mpsi * xi.w;
         double ffx = (rx * sc) * m, ffy = (ry * sc) * m, ffz = (rz * sc) * m;
         fx += ffx * mneg;
         fy += ffy * mneg;
         fz += ffz * mneg;
-    }
+    });
     s.bf[b] = make_double4(fx, fy, fz, 0.0);
 }
 
@@ -256,22 +306,20 @@ __global__ void __launch_bounds__(kThreads) k_xsph(uint32_t n, StepConst kc, Sta
     }
     const double4 xi = s.pos[i];
     double dvx = 0.0, dvy = 0.0, dvz = 0.0;
-    const uint32_t nv = l.nvisit[i];
-    for (uint32_t t = 0; t < nv; ++t) {
-        uint32_t e = l.visit[list_index(i, t, l.capv)];
-        if (e & kEntryBoundary) continue;
-        uint32_t j = e & kEntrySlotMask;
-        double4 xj = s.pos[j];
-        double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
-        double r = sqrt(dx * dx + dy * dy + dz * dz);
-        double wij = cubic_w(r, kc.h, kc.alpha);
-        double4 vj = s.vel[j];
-        double rho_bar = 0.5 * (vi.w + vj.w);
-        double f = kc.mass / rho_bar * wij;
+    for_each_entry(l.visit, i, l.nvisit[i], l.capv, [&](uint32_t e) {
+        if (e & kEntryBoundary) return;
+        const uint32_t j = e & kEntrySlotMask;
+        const double4 xj = s.pos[j];
+        const double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
+        const double r = sqrt(dx * dx + dy * dy + dz * dz);
+        const double wij = kern_w(r, kc);
+        const double4 vj = s.vel[j];
+        const double rho_bar = 0.5 * (vi.w + vj.w);
+        const double f = kc.mass / rho_bar * wij;
         dvx += (vj.x - vi.x) * f;
         dvy += (vj.y - vi.y) * f;
         dvz += (vj.z - vi.z) * f;
-    }
+    });
     vel_out[i] = make_double4(vi.x + dvx * kc.xsph_eps, vi.y + dvy * kc.xsph_eps,
                               vi.z + dvz * kc.xsph_eps, vi.w);
 }
@@ -285,14 +333,12 @@ __global__ void k_in_support(uint32_t n, StepConst kc, StateBufs s, ListBufs l, 
     }
     const double4 xi = s.pos[i];
     uint32_t c = 0;
-    const uint32_t nv = l.nvisit[i];
-    for (uint32_t t = 0; t < nv; ++t) {
-        uint32_t j = l.visit[list_index(i, t, l.capv)] & kEntrySlotMask;
-        double4 xj = s.pos[j];
-        double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
-        double r = sqrt(dx * dx + dy * dy + dz * dz);
-        c += (r / kc.h) < 2.0;
-    }
+    for_each_entry(l.visit, i, l.nvisit[i], l.capv, [&](uint32_t e) {
+        const double4 xj = s.pos[e & kEntrySlotMask];
+        const double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
+        const double r = sqrt(dx * dx + dy * dy + dz * dz);
+        c += div_h(r, kc) < 2.0;
+    });
     out[i] = c;
 }
 

@@ -12,11 +12,13 @@
 //   * a dense cell grid over a fixed key box (ix-major linearisation, so the
 //     linear cell order equals the reference's CellKey order), cell_start,
 //     and the list of occupied cells.
-//   * per-slot neighbour lists (warp-interleaved, see list_index): the
-//     "visit" list holds in-support candidates in the reference's visiting
-//     order; the "lower" list holds, for fluid slots, the fluid neighbours
-//     with a lower original index in ascending original-index order, and,
-//     for boundary slots, all fluid neighbours in ascending original index.
+//   * per-slot neighbour lists (warp-interleaved in groups of four, see
+//     list_index): the "visit" list holds in-support candidates in the
+//     reference's visiting order; the "upper" list is the visit list without
+//     the entries flagged lower; the "lower" list holds, for fluid slots, the
+//     fluid neighbours with a lower original index in ascending original-index
+//     order, and, for boundary slots, all fluid neighbours in ascending
+//     original index.
 #pragma once
 
 #include <cstdint>
@@ -52,6 +54,7 @@ struct GridDesc {
 struct StepConst {
     int dim;
     double h, mass, rho0;      // particles.h, .mass, .rest_density
+    double inv_h;              // RN(1 / h), for the exact division by h
     double alpha;              // cubic_alpha(h, dim)
     double rho_self;           // 0.0 + mass * W(0)
     double visc_alpha, visc_beta, eps_h2;  // eps_h2 = visc.eps * h * h
@@ -78,16 +81,29 @@ struct StateBufs {
 
 struct ListBufs {
     uint32_t* visit;
+    uint32_t* upper;
     uint32_t* lower;
     uint32_t* nvisit;
+    uint32_t* nupper;
     uint32_t* nlower;
     uint32_t* ncand;
-    uint32_t capv, capl;
+    uint32_t capv, capl;  // capacities, multiples of 4 (upper uses capv)
 };
 
-// Warp-interleaved list storage: entry t of slot s.
+// List storage: the 32 slots of a warp share a block of cap * 32 entries; each
+// slot's entries t..t+3 (t a multiple of 4) are 16 contiguous bytes, and the
+// 32 slots' groups are contiguous, so one uint4 load per lane fetches four
+// entries of 32 consecutive slots in one 512-byte transaction.
 __host__ __device__ __forceinline__ size_t list_index(uint32_t s, uint32_t t, uint32_t cap) {
-    return ((size_t)(s >> 5) * cap + t) * 32u + (s & 31u);
+    return ((size_t)(s >> 5) * cap + (t & ~3u)) * 32u + (s & 31u) * 4u + (t & 3u);
+}
+
+// Group g (entries 4g..4g+3) of slot s as a uint4.
+__device__ __forceinline__ uint4 list_group(const uint32_t* list, uint32_t s, uint32_t g,
+                                            uint32_t cap) {
+    const uint4* p = reinterpret_cast<const uint4*>(list) + ((size_t)(s >> 5) * cap) * 8u +
+                     (size_t)g * 32u + (s & 31u);
+    return __ldg(p);
 }
 
 struct DeviceScalars {

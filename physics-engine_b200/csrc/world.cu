@@ -214,11 +214,13 @@ World::World(const WorldParams& prm, const WorldConfig& cfg, int dim, double res
         cell_start_ = alloc<uint32_t>((size_t)g_.ncell + 1);
         occ_ = alloc<uint32_t>(g_.ncell);
         scan_tmp_ = alloc<unsigned char>(scan_temp_bytes(g_.ncell));
-        lists_.capv = cfg_.max_neighbours ? cfg_.max_neighbours : 512u;
-        lists_.capl = cfg_.max_lower ? cfg_.max_lower : lists_.capv;
+        lists_.capv = (cfg_.max_neighbours ? cfg_.max_neighbours : 512u) + 3u & ~3u;
+        lists_.capl = (cfg_.max_lower ? cfg_.max_lower : lists_.capv) + 3u & ~3u;
         lists_.visit = alloc<uint32_t>(npad * lists_.capv);
+        lists_.upper = alloc<uint32_t>(npad * lists_.capv);
         lists_.lower = alloc<uint32_t>(npad * lists_.capl);
         lists_.nvisit = alloc<uint32_t>(N);
+        lists_.nupper = alloc<uint32_t>(N);
         lists_.nlower = alloc<uint32_t>(N);
         lists_.ncand = alloc<uint32_t>(N);
         insup_ = alloc<uint32_t>(N);
@@ -330,6 +332,7 @@ void World::refresh_step_const() {
     StepConst k{};
     k.dim = dim_;
     k.h = h_;
+    k.inv_h = 1.0 / h_;
     k.mass = mass_;
     k.rho0 = rho0_;
     k.alpha = cubic_alpha(h_, dim_);
@@ -401,6 +404,7 @@ void World::ensure_lists() {
     if (!grid_built_) {
         // No grid yet: every neighbour query of the reference returns nothing.
         check(cudaMemsetAsync(lists_.nvisit, 0, sizeof(uint32_t) * n_, st_), "memset");
+        check(cudaMemsetAsync(lists_.nupper, 0, sizeof(uint32_t) * n_, st_), "memset");
         check(cudaMemsetAsync(lists_.nlower, 0, sizeof(uint32_t) * n_, st_), "memset");
         check(cudaMemsetAsync(lists_.ncand, 0, sizeof(uint32_t) * n_, st_), "memset");
     } else {
