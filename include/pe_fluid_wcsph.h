@@ -83,8 +83,9 @@ typedef struct PeWcsphParams {
 /* GPU placement and capacities (no reference counterpart; zeros = defaults). */
 typedef struct PeWcsphConfig {
     int32_t device;               /* CUDA device ordinal; -1 = the current device */
-    uint32_t max_neighbours;      /* per-particle in-support list capacity (0 = 512) */
-    uint32_t max_lower;           /* lower-index list capacity (0 = max_neighbours) */
+    uint32_t max_neighbours;      /* initial capacity of each half of a particle's neighbour
+                                     lists (0 = 256); grows on the first build if short */
+    uint32_t max_lower;           /* reserved, set to 0 */
     double domain_margin;         /* grid domain growth per side, fraction of extent (<0 = 0.25) */
     uint32_t domain_margin_cells; /* minimum growth per side in cells (0 = 4) */
 } PeWcsphConfig;
@@ -201,6 +202,11 @@ int pe_fluid_wcsph_get_neighbour_counts(PeWcsph* w, uint32_t* candidates, uint32
 
 int pe_fluid_wcsph_status(PeWcsph* w, uint32_t* status);
 int pe_fluid_wcsph_clear_status(PeWcsph* w);
+/* Capacity introspection (no reference counterpart): out = {status bits,
+ * largest neighbour-cell union seen, longest list part of the last build,
+ * union stage capacity, list part capacity, occupied cells, dense cells,
+ * list-build CTAs}. */
+int pe_fluid_wcsph_capacity_info(PeWcsph* w, uint64_t out[8]);
 int pe_fluid_wcsph_diagnostics(PeWcsph* w, PeFluidDiagnostics* out);
 /* Per-phase device time, measured with CUDA events on the world's stream:
  * 0 grid build, 1 neighbour lists, 2 density, 3 pressure, 4 forces + kick/drift,

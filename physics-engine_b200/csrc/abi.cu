@@ -684,6 +684,14 @@ int pe_fluid_wcsph_status(PeWcsph* w, uint32_t* status) {
     });
 }
 
+int pe_fluid_wcsph_capacity_info(PeWcsph* w, uint64_t out[8]) {
+    if (!w || !out) return PE_ERR_NULL;
+    return guard([&] {
+        w->world->capacity_info(out);
+        return PE_OK;
+    });
+}
+
 int pe_fluid_wcsph_clear_status(PeWcsph* w) {
     if (!w) return PE_ERR_NULL;
     return guard([&] {

@@ -87,10 +87,14 @@ struct ListBufs {
     uint32_t* nupper;
     uint32_t* nlower;
     uint32_t* ncand;
-    uint32_t capv, capl;  // capacities, multiples of 4 (upper uses capv)
+    uint32_t capv, capl;  // capacities, multiples of 8 (upper uses capv)
+    uint32_t nslots;      // count arrays hold part 0 at [s], part 1 at [nslots + s]
 };
 
-// List storage: the 32 slots of a warp share a block of cap * 32 entries; each
+// List storage: each list of a slot has two parts, entries [0, cap/2) and
+// [cap/2, cap), written independently by the two threads that build it; the
+// list is part 0 followed by part 1. The 32 slots of a warp share a block of
+// cap * 32 entries; each
 // slot's entries t..t+3 (t a multiple of 4) are 16 contiguous bytes, and the
 // 32 slots' groups are contiguous, so one uint4 load per lane fetches four
 // entries of 32 consecutive slots in one 512-byte transaction.
@@ -112,7 +116,7 @@ struct DeviceScalars {
     uint32_t status;
     uint32_t nocc;                  // occupied cells
     uint32_t max_union;             // largest neighbour-cell union seen by the list build
-    uint32_t pad;
+    uint32_t max_part;              // longest list part (untruncated) of the last build
 };
 
 // ----- grid build -----

@@ -187,7 +187,6 @@ World::World(const WorldParams& prm, const WorldConfig& cfg, int dim, double res
 
         // ---- allocations ----
         const size_t N = std::max<uint64_t>(n_, 1);
-        const size_t npad = (N + 31) / 32 * 32;
         auto make_state = [&](StateBufs& s) {
             s.pos = alloc<double4>(N);
             s.vel = alloc<double4>(N);
@@ -214,14 +213,12 @@ World::World(const WorldParams& prm, const WorldConfig& cfg, int dim, double res
         cell_start_ = alloc<uint32_t>((size_t)g_.ncell + 1);
         occ_ = alloc<uint32_t>(g_.ncell);
         scan_tmp_ = alloc<unsigned char>(scan_temp_bytes(g_.ncell));
-        lists_.capv = (cfg_.max_neighbours ? cfg_.max_neighbours : 512u) + 3u & ~3u;
-        lists_.capl = (cfg_.max_lower ? cfg_.max_lower : lists_.capv) + 3u & ~3u;
-        lists_.visit = alloc<uint32_t>(npad * lists_.capv);
-        lists_.upper = alloc<uint32_t>(npad * lists_.capv);
-        lists_.lower = alloc<uint32_t>(npad * lists_.capl);
-        lists_.nvisit = alloc<uint32_t>(N);
-        lists_.nupper = alloc<uint32_t>(N);
-        lists_.nlower = alloc<uint32_t>(N);
+        lists_.nslots = (uint32_t)N;
+        const uint32_t want = cfg_.max_neighbours ? cfg_.max_neighbours : 256u;
+        alloc_lists((want + 7u) & ~7u);
+        lists_.nvisit = alloc<uint32_t>(2 * N);
+        lists_.nupper = alloc<uint32_t>(2 * N);
+        lists_.nlower = alloc<uint32_t>(2 * N);
         lists_.ncand = alloc<uint32_t>(N);
         insup_ = alloc<uint32_t>(N);
         sc_ = alloc<DeviceScalars>(1);
@@ -262,14 +259,33 @@ World::World(const WorldParams& prm, const WorldConfig& cfg, int dim, double res
     } catch (...) {
         for (void* p : allocs_) cudaFree(p);
         allocs_.clear();
+        for (void* p : list_allocs_) cudaFree(p);
+        list_allocs_.clear();
         if (st_) cudaStreamDestroy(st_);
         st_ = nullptr;
         throw;
     }
 }
 
+void World::alloc_lists(uint32_t part_cap) {
+    for (void* p : list_allocs_) cudaFree(p);
+    list_allocs_.clear();
+    lists_.visit = lists_.upper = lists_.lower = nullptr;
+    const size_t npad = ((size_t)lists_.nslots + 31) / 32 * 32;
+    const size_t cap = 2 * (size_t)part_cap;  // two parts per slot
+    for (uint32_t** dst : {&lists_.visit, &lists_.upper, &lists_.lower}) {
+        void* p = nullptr;
+        check(cudaMalloc(&p, npad * cap * sizeof(uint32_t)), "cudaMalloc lists");
+        list_allocs_.push_back(p);
+        *dst = static_cast<uint32_t*>(p);
+    }
+    lists_.capv = lists_.capl = (uint32_t)cap;
+    lists_valid_ = false;
+}
+
 World::~World() {
     if (st_) cudaStreamSynchronize(st_);
+    for (void* p : list_allocs_) cudaFree(p);
     for (auto& r : recs_) {
         cudaEventDestroy(r.a);
         cudaEventDestroy(r.b);
@@ -403,15 +419,46 @@ void World::ensure_lists() {
     if (lists_valid_) return;
     if (!grid_built_) {
         // No grid yet: every neighbour query of the reference returns nothing.
-        check(cudaMemsetAsync(lists_.nvisit, 0, sizeof(uint32_t) * n_, st_), "memset");
-        check(cudaMemsetAsync(lists_.nupper, 0, sizeof(uint32_t) * n_, st_), "memset");
-        check(cudaMemsetAsync(lists_.nlower, 0, sizeof(uint32_t) * n_, st_), "memset");
-        check(cudaMemsetAsync(lists_.ncand, 0, sizeof(uint32_t) * n_, st_), "memset");
+        check(cudaMemsetAsync(lists_.nvisit, 0, sizeof(uint32_t) * 2 * lists_.nslots, st_), "memset");
+        check(cudaMemsetAsync(lists_.nupper, 0, sizeof(uint32_t) * 2 * lists_.nslots, st_), "memset");
+        check(cudaMemsetAsync(lists_.nlower, 0, sizeof(uint32_t) * 2 * lists_.nslots, st_), "memset");
+        check(cudaMemsetAsync(lists_.ncand, 0, sizeof(uint32_t) * lists_.nslots, st_), "memset");
     } else {
-        prof_begin(kLists);
-        launch_nlist(g_, kc_, ucap_, nl_blocks_, occ_, cell_start_, cur_, lists_, sc_, st_);
-        prof_end();
-        launches_ += 1;
+        for (int attempt = 0; attempt < 4; ++attempt) {
+            if (!lists_checked_)
+                check(cudaMemsetAsync(&sc_->max_part, 0, sizeof(uint32_t), st_), "memset");
+            prof_begin(kLists);
+            launch_nlist(g_, kc_, ucap_, nl_blocks_, occ_, cell_start_, cur_, lists_, sc_, st_);
+            prof_end();
+            launches_ += 2;
+            check(cudaGetLastError(), "neighbour lists");
+            if (lists_checked_) break;
+            // First build for these positions: size the lists from the longest
+            // part before any pass consumes them.
+            DeviceScalars hs{};
+            check(cudaMemcpyAsync(&hs, sc_, sizeof(hs), cudaMemcpyDeviceToHost, st_), "lists");
+            check(cudaStreamSynchronize(st_), "lists");
+            const uint32_t part_cap = lists_.capv / 2;
+            const bool overflowed = hs.max_part > part_cap;
+            if (!overflowed && (uint64_t)hs.max_part * 2 <= (uint64_t)part_cap) {
+                lists_checked_ = true;
+                break;
+            }
+            // Keep twice the longest part: lists grow as the fluid compresses
+            // (by 40% in a few steps when a free-surface start collapses), and
+            // the densest part of a list can hold nearly all of its entries (a
+            // particle's lower neighbours sit just below its own index in the
+            // sorted union). Runs poll the length and grow further.
+            uint32_t grow = (2 * hs.max_part + 31u) & ~31u;
+            alloc_lists(grow);
+            if (!overflowed) {
+                lists_valid_ = false;
+                continue;  // rebuild into the larger lists
+            }
+            // this build overflowed and is discarded: clear its status bit
+            uint32_t keep = hs.status & ~kStatusListOverflow;
+            check(cudaMemcpyAsync(&sc_->status, &keep, sizeof(uint32_t), cudaMemcpyHostToDevice, st_), "status");
+        }
     }
     check(cudaGetLastError(), "neighbour lists");
     lists_valid_ = true;
@@ -502,7 +549,7 @@ void World::step(double dt) {
 void World::run(double dt, uint64_t steps) {
     for (uint64_t s = 0; s < steps; ++s) {
         step(dt);
-        if ((s & 63u) == 63u) status();  // lets the list stage grow if needed
+        if ((s & 15u) == 15u) status();  // lets the list storage and stage grow if needed
     }
 }
 
@@ -516,6 +563,13 @@ uint32_t World::status() {
     DeviceScalars hs{};
     check(cudaMemcpyAsync(&hs, sc_, sizeof(hs), cudaMemcpyDeviceToHost, st_), "status");
     check(cudaStreamSynchronize(st_), "status");
+    // Grow the list storage ahead of need: the next list build uses the larger
+    // capacity (the current lists are complete as long as no overflow bit is set).
+    if ((uint64_t)hs.max_part * 4 > (uint64_t)(lists_.capv / 2) * 3) {
+        alloc_lists((2 * hs.max_part + 31u) & ~31u);
+        check(cudaMemsetAsync(&sc_->max_part, 0, sizeof(uint32_t), st_), "memset");
+        lists_checked_ = false;
+    }
     // Grow the shared-memory stage of the list build when the fluid has
     // packed more particles into a neighbourhood than it holds.
     if (hs.max_union > ucap_) {
@@ -526,6 +580,20 @@ uint32_t World::status() {
         }
     }
     return hs.status;
+}
+
+void World::capacity_info(uint64_t* out) {
+    DeviceScalars hs{};
+    check(cudaMemcpyAsync(&hs, sc_, sizeof(hs), cudaMemcpyDeviceToHost, st_), "info");
+    check(cudaStreamSynchronize(st_), "info");
+    out[0] = hs.status;
+    out[1] = hs.max_union;
+    out[2] = hs.max_part;
+    out[3] = ucap_;
+    out[4] = lists_.capv / 2;
+    out[5] = hs.nocc;
+    out[6] = g_.ncell;
+    out[7] = nl_blocks_;
 }
 
 void World::clear_status() {
@@ -559,6 +627,7 @@ void World::set_vec(int which, const double* in) {
         grid_current_ = false;
         rho_current_ = false;
         lists_valid_ = false;
+        lists_checked_ = false;
     }
 }
 

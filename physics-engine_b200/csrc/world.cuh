@@ -27,8 +27,8 @@ struct WorldParams {
 
 struct WorldConfig {
     int device;                 // CUDA device ordinal (-1 = current)
-    uint32_t max_neighbours;    // visit-list capacity per particle (0 = 512)
-    uint32_t max_lower;         // lower-list capacity per particle (0 = max_neighbours)
+    uint32_t max_neighbours;    // initial list-part capacity per particle (0 = 256; grows on demand)
+    uint32_t max_lower;         // reserved
     double domain_margin;       // extra grid domain per side, fraction of extent (<0 = 0.25)
     uint32_t domain_margin_cells;  // minimum extra cells per side (0 = 4)
 };
@@ -80,6 +80,9 @@ class World {
     void get_neighbour_counts(uint32_t* candidates, uint32_t* in_support);
     uint32_t status();
     void clear_status();
+    // status, largest union, longest list part, union stage capacity, list part
+    // capacity, occupied cells, dense cells, list-build CTAs
+    void capacity_info(uint64_t* out);
 
     // Device views (advanced use: zero-copy access from the same process).
     const StateBufs& device_state() const { return cur_; }
@@ -105,6 +108,7 @@ class World {
     void run_xsph();
     void refresh_step_const();
     void configure_lists();
+    void alloc_lists(uint32_t part_cap);
     template <typename T>
     T* alloc(size_t count);
     void gather_orig_vec(const double4* src, double* out);
@@ -135,11 +139,13 @@ class World {
     DeviceScalars* sc_ = nullptr;
     double* xfer_ = nullptr;  // n * 4 doubles of export/import staging
     std::vector<void*> allocs_;
+    std::vector<void*> list_allocs_;
 
     bool grid_built_ = false;    // a grid exists (rebuild_grid ran at least once)
     bool grid_current_ = false;  // grid built from the current positions
     bool rho_current_ = false;   // densities computed from the current grid and positions
     bool lists_valid_ = false;   // neighbour lists match the grid and positions
+    bool lists_checked_ = false; // list capacity verified for the current positions
     uint32_t launches_ = 0;
 
     struct PhaseRec {

@@ -168,6 +168,7 @@ def load_library():
         "pe_fluid_wcsph_get_neighbour_counts": (C.c_int, [vp, vp, vp, u64]),
         "pe_fluid_wcsph_status": (C.c_int, [vp, C.POINTER(u32)]),
         "pe_fluid_wcsph_clear_status": (C.c_int, [vp]),
+        "pe_fluid_wcsph_capacity_info": (C.c_int, [vp, vp]),
         "pe_fluid_wcsph_diagnostics": (C.c_int, [vp, C.POINTER(_Diag)]),
         "pe_fluid_wcsph_kernel_launches": (C.c_int, [vp, C.POINTER(u64), i32]),
         "pe_fluid_wcsph_profile": (C.c_int, [vp, i32]),
@@ -545,6 +546,13 @@ class WcsphWorld:
         s = C.c_uint32()
         _ok(_lib.pe_fluid_wcsph_status(self._w, C.byref(s)), "status")
         return s.value
+
+    def capacity_info(self) -> dict:
+        out = np.zeros(8, np.uint64)
+        _ok(_lib.pe_fluid_wcsph_capacity_info(self._w, _ptr(out)), "capacity_info")
+        keys = ("status", "max_union", "max_part", "union_capacity", "part_capacity",
+                "occupied_cells", "dense_cells", "list_ctas")
+        return {k: int(v) for k, v in zip(keys, out)}
 
     def clear_status(self):
         _ok(_lib.pe_fluid_wcsph_clear_status(self._w), "clear_status")
