@@ -85,6 +85,8 @@ def lib():
             "o_kernel_w": (d, [C.c_int, d, d, C.c_int]),
             "o_grad_w": (None, [C.c_int, dp, d, C.c_int, dp]),
             "o_pow": (d, [d, d]),
+            "o_pi_ij": (d, [d, d, d, d, d, dp, dp, dp, dp, d, d]),
+            "o_tait_pressure": (d, [d, d, d, d]),
             "o_floor_i32": (i32, [d]),
             "o_xoshiro_first": (u64, [u64, i64, vp]),
             "ow_create": (vp, [vp, C.POINTER(OParams)]),
@@ -324,6 +326,14 @@ def grad_w(kernel, rij, h, dim):
 
 def opow(x, y):
     return lib().o_pow(x, y)
+
+
+def pi_ij(alpha, beta, eps, h, c, xi, xj, vi, vj, rho_i, rho_j):
+    return lib().o_pi_ij(alpha, beta, eps, h, c, _d3(xi), _d3(xj), _d3(vi), _d3(vj), rho_i, rho_j)
+
+
+def tait_pressure(rest_density, sound_speed, gamma, density):
+    return lib().o_tait_pressure(rest_density, sound_speed, gamma, density)
 
 
 def floor_i32(x):

@@ -778,6 +778,24 @@ void o_grad_w(int kernel, const double* rij, double h, int dim, double* out) {
     out[0] = g.x; out[1] = g.y; out[2] = g.z;
 }
 double o_pow(double x, double y) { return oracle_pow(x, y); }
+// viscosity.rs:51 pi_ij with explicit parameters
+double o_pi_ij(double alpha, double beta, double eps, double h, double c, const double* xi,
+               const double* xj, const double* vi, const double* vj, double rho_i, double rho_j) {
+    World w;
+    w.prm.visc_alpha = alpha;
+    w.prm.visc_beta = beta;
+    w.prm.visc_eps = eps;
+    return w.pi_ij(h, c, v3(xi[0], xi[1], xi[2]), v3(xj[0], xj[1], xj[2]), v3(vi[0], vi[1], vi[2]),
+                   v3(vj[0], vj[1], vj[2]), rho_i, rho_j);
+}
+// eos.rs:65 TaitEos::pressure
+double o_tait_pressure(double rest_density, double sound_speed, double gamma, double density) {
+    World w;
+    w.prm.eos_rest_density = rest_density;
+    w.prm.eos_sound_speed = sound_speed;
+    w.prm.eos_gamma = gamma;
+    return w.eos_pressure(density);
+}
 int32_t o_floor_i32(double x) { return floor_i32(x); }
 uint64_t o_xoshiro_first(uint64_t seed, long n, uint64_t* out) {
     Xoshiro r = xoshiro_seed(seed);
