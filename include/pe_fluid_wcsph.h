@@ -235,6 +235,37 @@ double pe_fluid_pi_ij(double alpha, double beta, double eps, double h, double so
 /* cfl.rs:36 suggested_dt */
 double pe_fluid_suggested_dt(double h, double sound_speed, double v_max, double a_max,
                              double lambda_v, double lambda_f);
+/* ---- allocation-free density pass (no reference counterpart) ----
+ *
+ * For callers that cannot allocate device memory: applications that give the
+ * library a fixed device budget or route every device allocation through
+ * their own allocator, and real-time loops that must not pay for cudaMalloc's
+ * device-wide synchronisation. It computes what `rebuild_grid` followed by
+ * `compute_density` gives (wcsph.rs:102-154, the same bits as the world API):
+ * rho[i] for every particle, rest_density for boundary samples.
+ *
+ * x [n*3], kind [n], psi [n] (may be NULL), n_out [n*3] (may be NULL) and the
+ * output rho [n] are DEVICE pointers; `stream` is a cudaStream_t (NULL = the
+ * legacy default stream). Nothing is allocated: the working memory is one
+ * fixed array in the library's device image (about 18 MB per device that
+ * loads the library, held until the process exits). Limits: n <=
+ * PE_FLUID_NOALLOC_MAX_PARTICLES and a cell-key bounding box of at most
+ * PE_FLUID_NOALLOC_MAX_CELLS cells (2h-sized cells); beyond either the call
+ * returns PE_ERR_BOUNDS without launching anything else.
+ *
+ * The first call on each device, with that device current, looks up the
+ * array's device address (cudaGetSymbolAddress); make that first call before
+ * any stream capture on the device. The call waits for its stream once (to
+ * read the key bounding box). All calls share the one array, which keeps the
+ * previous call's contents; every call clears what must start at zero. Calls
+ * that overlap on the GPU race on the array: issue them in order on one
+ * stream or otherwise serialise them. */
+#define PE_FLUID_NOALLOC_MAX_PARTICLES 131072u
+#define PE_FLUID_NOALLOC_MAX_CELLS 262144u
+int pe_fluid_density_noalloc(int32_t dim, double rest_density, double mass, double h, uint64_t n,
+                             const double* x, const uint8_t* kind, const double* psi,
+                             const double* n_out, double* rho, void* stream);
+
 /* Library version string. */
 const char* pe_fluid_version(void);
 
