@@ -49,6 +49,8 @@ FORCE_BYTES_PER_FLUID = 104.0
 # Whole step, per fluid / per boundary particle (cell key 28 + sort 8 +
 # density 32 + XSPH 80 + forces 104; boundary 28 + 8 + 3 x 24).
 STEP_BYTES_FLUID, STEP_BYTES_BOUNDARY = 252.0, 108.0
+# Single-precision force pass: read cell-local x, v, rho (28 B), write x, v (24 B).
+FORCE_BYTES_F32 = 52.0
 
 
 def _args():
@@ -59,6 +61,9 @@ def _args():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="dam_break_1m")
     ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--form", choices=("plain", "f32"), default="plain",
+                    help="plain: the f64 step (reference bits); f32: the single-precision "
+                         "form, timed and compared with the f64 step after the same steps")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -199,11 +204,105 @@ def run_reference(args, ws, rank):
     print(json.dumps(line), flush=True)
 
 
+def _state_summary(world, nf_mask, mass, g):
+    """f64 reductions of the fluid state (diagnostics.rs:35-71 quantities)."""
+    import numpy as np
+
+    x, v, rho = world.positions(), world.velocities(), world.densities()
+    x, v, rho = x[nf_mask], v[nf_mask], rho[nf_mask]
+    com = x.mean(axis=0)
+    ke = float((0.5 * mass * (v * v).sum(axis=1)).sum())
+    pe = float((mass * g * x[:, 2]).sum())
+    return rho, com, ke + pe
+
+
+def run_f32(args, ws, rank, local, torch, pe):
+    """Single-precision form next to the f64 step on the same tank: both advance
+    warmup + steps steps; the f32 world is timed, then densities, centre of mass
+    and total energy are compared with the f64 world's."""
+    import numpy as np
+
+    ps, prm, nf = build_scene(pe, args.workload)
+    nb = len(ps) - nf
+    kind = ps.arrays()["kind"]
+    fluid = kind == 0
+    w64 = pe.WcsphWorld(ps, prm, pe.WcsphConfig(device=local))
+    w32 = pe.WcsphWorld(ps, prm, pe.WcsphConfig(device=local, precision=pe.PRECISION_F32))
+    del ps
+    timings = {}
+    for name, w in (("f32", w32), ("f64", w64)):
+        stream = torch.cuda.ExternalStream(w.stream_handle(), device=local)
+        w.run(DT, max(args.warmup, 3))
+        torch.cuda.synchronize()
+        sampler = ClockSampler(local) if name == "f32" else None
+        if sampler:
+            sampler.start()
+        w.set_profiling(True)
+        w.profile(reset=True)
+        w.kernel_launches(reset=True)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record(stream)
+        w.run(DT, args.steps)
+        b.record(stream)
+        b.synchronize()
+        timings[name] = (a.elapsed_time(b), w.profile(reset=True), w.kernel_launches(),
+                         sampler.stop() if sampler else None, w.status())
+        w.set_profiling(False)
+    g = -prm.gravity[2]
+    rho32, com32, e32 = _state_summary(w32, fluid, w32.mass, g)
+    rho64, com64, e64 = _state_summary(w64, fluid, w64.mass, g)
+    rel = np.abs(rho32 - rho64) / rho64
+    ms32, prof32, launches, clocks, status = timings["f32"]
+    ms64 = timings["f64"][0]
+    value = nf * args.steps / (ms32 / 1e3)
+    hbm_peak, peak_kind = _peaks()
+    f_ms, f_n = prof32["forces"]
+    achieved = FORCE_BYTES_F32 * nf * f_n / (f_ms / 1e3) / 1e9 if f_ms > 0 else 0.0
+    line = {
+        "metric": "SPH fluid particle-steps/s @1M (FP32 form)", "value": value, "unit": UNIT,
+        "n_gpus": 1, "steps": args.steps, "warmup": max(args.warmup, 3),
+        "ms_per_step": ms32 / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic", "form": "f32",
+        "config": {"workload": args.workload, "fluid_particles": nf, "boundary_particles": nb,
+                   "dx": DX, "dt": DT, "sound_speed": 20.0, "adapt_sound_speed": False},
+        "gpu_launches": int(launches), "status": int(status),
+        "phases_ms_per_step": {k: v[0] / max(1, args.steps) for k, v in prof32.items()},
+        "f64_ms_per_step": ms64 / args.steps,
+        "speedup_vs_f64_step": ms64 / ms32,
+        "error_vs_f64": {
+            "after_steps": max(args.warmup, 3) + args.steps,
+            "density_rel_max": float(rel.max()), "density_rel_mean": float(rel.mean()),
+            "com_drift_m": float(np.linalg.norm(com32 - com64)),
+            "energy_rel_drift": float((e32 - e64) / abs(e64)),
+        },
+        "roofline": {"bound": "hbm", "kernel": "k_forces_f32 (force + kick + drift)",
+                     "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                     "frac": achieved / hbm_peak, "peak_kind": peak_kind, "traffic": None,
+                     "bytes_per_unit": FORCE_BYTES_F32, "units_per_launch": nf,
+                     "launch_ms": f_ms / max(1, f_n)},
+        "clocks": clocks,
+    }
+    w32.close()
+    w64.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = _args()
     ws, rank, local = _dist()
     if args.impl == "reference":
         run_reference(args, ws, rank)
+        return
+    if args.form == "f32":
+        import torch
+
+        torch.cuda.set_device(local)
+        sys.path.insert(0, os.path.join(ROOT, "physics-engine_b200"))
+        import physics_engine_rs as pe
+
+        run_f32(args, ws, rank, local, torch, pe)
         return
 
     import numpy as np
@@ -263,17 +362,22 @@ def main():
         args.e2e_steps = 0
     x_h = torch.empty((world.n, 3), dtype=torch.float64, pin_memory=True).numpy()
     v_h = torch.empty((world.n, 3), dtype=torch.float64, pin_memory=True).numpy()
-    x_h[:] = world.positions()
-    v_h[:] = world.velocities()
+    world.positions(out=x_h)
+    world.velocities(out=v_h)
+
+    def e2e_step():
+        world.set_positions(x_h)
+        world.set_velocities(v_h)
+        world.step(DT)
+        world.positions(out=x_h)
+        world.velocities(out=v_h)
+
+    e2e_step()  # untimed: the first host round trip re-checks the list capacity
     barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(args.e2e_steps):
-        world.set_positions(x_h)
-        world.set_velocities(v_h)
-        world.step(DT)
-        x_h[:] = world.positions()
-        v_h[:] = world.velocities()
+        e2e_step()
     torch.cuda.synchronize()
     e2e_sec = max(time.perf_counter() - t0, 1e-12)
     if ws > 1:

@@ -88,7 +88,16 @@ typedef struct PeWcsphConfig {
     uint32_t max_lower;           /* reserved, set to 0 */
     double domain_margin;         /* grid domain growth per side, fraction of extent (<0 = 0.25) */
     uint32_t domain_margin_cells; /* minimum growth per side in cells (0 = 4) */
+    int32_t precision;            /* PE_PRECISION_F64 (default, the reference's bits) or
+                                     PE_PRECISION_F32 (single-precision form) */
 } PeWcsphConfig;
+
+#define PE_PRECISION_F64 0
+/* Single-precision form: cell-local float positions and float velocities,
+ * single-precision pair arithmetic with Kahan-compensated density, force and
+ * XSPH sums; the grid, its sort and the sound-speed control stay f64. Not the
+ * reference's bits; see bench_precision.py for its error. */
+#define PE_PRECISION_F32 1
 
 /* Conservation / error reductions (crates/pe-fluid/src/diagnostics.rs:35-102,
  * wcsph.rs:350-369), computed in f64. */

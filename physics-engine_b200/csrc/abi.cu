@@ -150,6 +150,7 @@ pe::WorldConfig to_config(const PeWcsphConfig* c) {
     w.max_lower = c ? c->max_lower : 0;
     w.domain_margin = c ? c->domain_margin : -1.0;
     w.domain_margin_cells = c ? c->domain_margin_cells : 0;
+    w.precision = c ? c->precision : 0;
     if (!c) w.domain_margin = -1.0;
     return w;
 }

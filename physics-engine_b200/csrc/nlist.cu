@@ -48,6 +48,15 @@ __device__ __forceinline__ void emit(uint32_t* list, uint32_t slot, uint32_t t, 
     if (t < cap) list[list_index(slot, t, cap)] = value;
 }
 
+// Base of slot s's entries in a list (entry t at base[(t & ~3) * 32 + (t & 3)]).
+__device__ __forceinline__ uint32_t* slot_base(uint32_t* list, uint32_t s, uint32_t cap) {
+    return list + (size_t)(s >> 5) * cap * 32u + (s & 31u) * 4u;
+}
+
+__device__ __forceinline__ void put(uint32_t* base, uint32_t t, uint32_t value) {
+    base[(t & ~3u) * 32u + (t & 3u)] = value;
+}
+
 template <int NC>
 __device__ __forceinline__ uint32_t slot_of_union(const uint32_t* s_off, const uint32_t* s_cstart,
                                                   uint32_t u) {
@@ -207,6 +216,9 @@ __global__ void __launch_bounds__(kNlThreads) k_nlist_visit(GridDesc g, StepCons
                 const uint32_t mw = __float_as_uint(me.w);
                 const uint32_t myo = mw & kStageOrigMask;
                 uint32_t nv = 0, nu = 0;
+                uint32_t* vb = slot_base(l.visit, kslot, l.capv) ;
+                // no upper list storage in the single-precision form (visit list only)
+                uint32_t* ub = l.upper ? slot_base(l.upper, kslot, l.capv) : nullptr;
                 if (!(mw & kStageBoundary)) {
                     for (uint32_t w = w0; w < w1; ++w) {
                         uint32_t m = 0;
@@ -223,10 +235,10 @@ __global__ void __launch_bounds__(kNlThreads) k_nlist_visit(GridDesc g, StepCons
                             if (!(ow & kStageBoundary) && (ow & kStageOrigMask) < myo) {
                                 e |= kEntryLower;
                             } else {
-                                if (nu < half_cap) emit(l.upper, kslot, base + nu, l.capv, e);
+                                if (ub && nu < half_cap) put(ub, base + nu, e);
                                 ++nu;
                             }
-                            if (nv < half_cap) emit(l.visit, kslot, base + nv, l.capv, e);
+                            if (nv < half_cap) put(vb, base + nv, e);
                             ++nv;
                         }
                     }
@@ -260,7 +272,7 @@ __global__ void __launch_bounds__(kNlThreads) k_nlist_visit(GridDesc g, StepCons
                             if (!(fl & kFlagBoundary) && o < myo) {
                                 e |= kEntryLower;
                             } else {
-                                if (nu < half_cap) emit(l.upper, kslot, nu, l.capv, e);
+                                if (l.upper && nu < half_cap) emit(l.upper, kslot, nu, l.capv, e);
                                 ++nu;
                             }
                             if (nv < half_cap) emit(l.visit, kslot, nv, l.capv, e);
@@ -408,6 +420,7 @@ __global__ void __launch_bounds__(kNlThreads) k_nlist_lower(GridDesc g, StepCons
                 }
                 const uint32_t i_begin = part ? (R >> 1) : 0u, i_end = part ? R : (R >> 1);
                 uint32_t nl = 0;
+                uint32_t* lb = slot_base(l.lower, kslot, l.capl);
                 for (uint32_t i0 = i_begin; i0 < i_end; i0 += 32) {
                     uint32_t m = 0;
 #pragma unroll
@@ -419,7 +432,7 @@ __global__ void __launch_bounds__(kNlThreads) k_nlist_lower(GridDesc g, StepCons
                     while (m) {
                         const uint32_t i = i0 + (__ffs(m) - 1);
                         m &= m - 1u;
-                        if (nl < half_cap) emit(l.lower, kslot, base + nl, l.capl, s_ent[s_sorted[i]]);
+                        if (nl < half_cap) put(lb, base + nl, s_ent[s_sorted[i]]);
                         ++nl;
                     }
                 }
@@ -511,14 +524,16 @@ uint32_t nlist_prepare(int dim, uint32_t ucap) {
 
 void launch_nlist(const GridDesc& g, const StepConst& k, uint32_t ucap, uint32_t nblocks,
                   const uint32_t* occ, const uint32_t* cell_start, const StateBufs& s,
-                  const ListBufs& l, DeviceScalars* sc, cudaStream_t st) {
+                  const ListBufs& l, DeviceScalars* sc, cudaStream_t st, bool visit_only) {
     const size_t sl = nlist_smem_bytes(ucap), sv = visit_smem_bytes(ucap);
     if (g.dim == 3) {
         k_nlist_visit<3><<<nblocks, kNlThreads, sv, st>>>(g, k, ucap, occ, cell_start, s, l, sc);
-        k_nlist_lower<3><<<nblocks, kNlThreads, sl, st>>>(g, k, ucap, occ, cell_start, s, l, sc);
+        if (!visit_only)
+            k_nlist_lower<3><<<nblocks, kNlThreads, sl, st>>>(g, k, ucap, occ, cell_start, s, l, sc);
     } else {
         k_nlist_visit<2><<<nblocks, kNlThreads, sv, st>>>(g, k, ucap, occ, cell_start, s, l, sc);
-        k_nlist_lower<2><<<nblocks, kNlThreads, sl, st>>>(g, k, ucap, occ, cell_start, s, l, sc);
+        if (!visit_only)
+            k_nlist_lower<2><<<nblocks, kNlThreads, sl, st>>>(g, k, ucap, occ, cell_start, s, l, sc);
     }
 }
 

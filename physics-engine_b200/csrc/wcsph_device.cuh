@@ -119,6 +119,37 @@ struct DeviceScalars {
     uint32_t max_part;              // longest list part (untruncated) of the last build
 };
 
+// Single-precision form (sph_f32.cu).
+struct F32Const {
+    int dim;
+    float h, inv_h, alpha, mass, rho0, rho_self, cell;
+    double cell_d;
+    float visc_alpha, visc_beta, eps_h2;
+    double eos_rho0, eos_gamma_d;
+    float inv_eos_rho0, eos_gamma;
+    int gamma7;
+    float gx, gy, gz, xsph_eps;
+    float boundary_eps_h;  // one-sided filter of oriented boundary samples
+    int adapt_sound_speed;
+};
+
+struct F32Bufs {
+    float4* pos;  // cell-local position, w = p / rho^2 (fluid) or psi (boundary)
+    float4* vel;  // velocity, w = rho
+};
+
+void launch_f32_from_f64(uint32_t n, double cell, const StateBufs& s, const F32Bufs& f,
+                         cudaStream_t st);
+void launch_density_f32(uint32_t n, const F32Const& k, const StateBufs& s, const F32Bufs& f,
+                        const ListBufs& l, cudaStream_t st);
+void launch_pressure_f32(uint32_t n, const F32Const& k, const StateBufs& s, const F32Bufs& f,
+                         DeviceScalars* sc, cudaStream_t st);
+void launch_forces_f32(uint32_t n, const F32Const& k, const StateBufs& s, const F32Bufs& f,
+                       const ListBufs& l, const DeviceScalars* sc, float dt, double4* pos_next,
+                       double4* vel_next, float* bf, cudaStream_t st);
+void launch_xsph_f32(uint32_t n, const F32Const& k, const StateBufs& s, const F32Bufs& f,
+                     const ListBufs& l, float4* vel_out, cudaStream_t st);
+
 // ----- grid build -----
 void launch_cell_ids(const GridDesc& g, uint32_t n, const double4* pos_cur, const double4* pos_next,
                      const uint8_t* flags, uint32_t* cellid, int4* key_tmp, uint32_t* count,
@@ -143,7 +174,7 @@ size_t nlist_smem_bytes(uint32_t ucap);
 uint32_t nlist_prepare(int dim, uint32_t ucap);
 void launch_nlist(const GridDesc& g, const StepConst& k, uint32_t ucap, uint32_t nblocks,
                   const uint32_t* occ, const uint32_t* cell_start, const StateBufs& s,
-                  const ListBufs& l, DeviceScalars* sc, cudaStream_t st);
+                  const ListBufs& l, DeviceScalars* sc, cudaStream_t st, bool visit_only = false);
 
 // ----- SPH passes -----
 void launch_density(uint32_t n, const StepConst& k, const StateBufs& s, const ListBufs& l,

@@ -159,6 +159,7 @@ World::World(const WorldParams& prm, const WorldConfig& cfg, int dim, double res
         g_.cell_size = cell;
         g_.dim = dim_;
 
+        f32_ = cfg_.precision == 1;
         refresh_step_const();
 
         // ---- union stage capacity from the largest initial neighbour-cell union ----
@@ -223,6 +224,12 @@ World::World(const WorldParams& prm, const WorldConfig& cfg, int dim, double res
         insup_ = alloc<uint32_t>(N);
         sc_ = alloc<DeviceScalars>(1);
         xfer_ = alloc<double>(N * 4);
+        if (f32_) {
+            fb_.pos = alloc<float4>(N);
+            fb_.vel = alloc<float4>(N);
+            velf_alt_ = alloc<float4>(N);
+            bf32_ = alloc<float>(4 * N);
+        }
 
         // ---- upload in original order (slot = original index) ----
         std::vector<double4> hp(N), hv(N), hn(N);
@@ -274,6 +281,7 @@ void World::alloc_lists(uint32_t part_cap) {
     const size_t npad = ((size_t)lists_.nslots + 31) / 32 * 32;
     const size_t cap = 2 * (size_t)part_cap;  // two parts per slot
     for (uint32_t** dst : {&lists_.visit, &lists_.upper, &lists_.lower}) {
+        if (f32_ && dst != &lists_.visit) continue;  // the f32 form reads the visit list only
         void* p = nullptr;
         check(cudaMalloc(&p, npad * cap * sizeof(uint32_t)), "cudaMalloc lists");
         list_allocs_.push_back(p);
@@ -371,6 +379,39 @@ void World::refresh_step_const() {
     double sup = 2.0 * h_;
     k.r2_filter = std::nextafter((float)(sup * sup * (1.0 + 1e-4)), std::numeric_limits<float>::infinity());
     kc_ = k;
+
+    F32Const f{};
+    f.dim = dim_;
+    f.h = (float)h_;
+    f.inv_h = (float)(1.0 / h_);
+    f.alpha = (float)k.alpha;
+    f.mass = (float)mass_;
+    f.rho0 = (float)rho0_;
+    f.rho_self = (float)k.rho_self;
+    f.cell = (float)(2.0 * h_);
+    f.cell_d = 2.0 * h_;
+    f.visc_alpha = (float)prm_.visc_alpha;
+    f.visc_beta = (float)prm_.visc_beta;
+    f.eps_h2 = (float)k.eps_h2;
+    f.eos_rho0 = prm_.eos_rest_density;
+    f.eos_gamma_d = prm_.eos_gamma;
+    f.inv_eos_rho0 = (float)(1.0 / prm_.eos_rest_density);
+    f.eos_gamma = (float)prm_.eos_gamma;
+    f.gamma7 = prm_.eos_gamma == 7.0;
+    f.gx = (float)prm_.gravity[0];
+    f.gy = (float)prm_.gravity[1];
+    f.gz = (float)prm_.gravity[2];
+    f.xsph_eps = (float)prm_.xsph_epsilon;
+    f.boundary_eps_h = (float)k.boundary_eps_h;
+    f.adapt_sound_speed = prm_.adapt_sound_speed;
+    kf_ = f;
+}
+
+void World::refresh_f32() {
+    if (!f32_) return;
+    launch_f32_from_f64((uint32_t)n_, 2.0 * h_, cur_, fb_, st_);
+    launches_ += 1;
+    check(cudaGetLastError(), "f32 state");
 }
 
 void World::set_params(const WorldParams& p) {
@@ -428,9 +469,9 @@ void World::ensure_lists() {
             if (!lists_checked_)
                 check(cudaMemsetAsync(&sc_->max_part, 0, sizeof(uint32_t), st_), "memset");
             prof_begin(kLists);
-            launch_nlist(g_, kc_, ucap_, nl_blocks_, occ_, cell_start_, cur_, lists_, sc_, st_);
+            launch_nlist(g_, kc_, ucap_, nl_blocks_, occ_, cell_start_, cur_, lists_, sc_, st_, f32_);
             prof_end();
-            launches_ += 2;
+            launches_ += f32_ ? 1 : 2;
             check(cudaGetLastError(), "neighbour lists");
             if (lists_checked_) break;
             // First build for these positions: size the lists from the longest
@@ -440,8 +481,15 @@ void World::ensure_lists() {
             check(cudaStreamSynchronize(st_), "lists");
             const uint32_t part_cap = lists_.capv / 2;
             const bool overflowed = hs.max_part > part_cap;
-            if (!overflowed && (uint64_t)hs.max_part * 2 <= (uint64_t)part_cap) {
+            // The very first sizing wants twice the longest part; later checks
+            // (after the host moved particles) only the 75% rule that runs
+            // poll, so a slowly compressing tank does not reallocate its lists
+            // on every set_positions.
+            const bool fits = lists_sized_ ? (uint64_t)hs.max_part * 4 <= (uint64_t)part_cap * 3
+                                           : (uint64_t)hs.max_part * 2 <= (uint64_t)part_cap;
+            if (!overflowed && fits) {
                 lists_checked_ = true;
+                lists_sized_ = true;
                 break;
             }
             // Keep twice the longest part: lists grow as the fluid compresses
@@ -467,7 +515,8 @@ void World::ensure_lists() {
 void World::run_density() {
     ensure_lists();
     prof_begin(kDensity);
-    launch_density((uint32_t)n_, kc_, cur_, lists_, st_);
+    if (f32_) launch_density_f32((uint32_t)n_, kf_, cur_, fb_, lists_, st_);
+    else launch_density((uint32_t)n_, kc_, cur_, lists_, st_);
     prof_end();
     launches_ += 1;
     check(cudaGetLastError(), "density");
@@ -476,11 +525,16 @@ void World::run_density() {
 void World::run_pressure() {
     prof_begin(kPressure);
     check(cudaMemsetAsync(&sc_->vmax2_bits, 0, sizeof(unsigned long long), st_), "memset");
-    if (kc_.adapt_sound_speed) {
-        launch_vmax((uint32_t)n_, cur_, sc_, st_);
-        launches_ += 1;
+    if (f32_) {
+        launch_pressure_f32((uint32_t)n_, kf_, cur_, fb_, sc_, st_);
+        launches_ += kf_.adapt_sound_speed ? 1 : 0;
+    } else {
+        if (kc_.adapt_sound_speed) {
+            launch_vmax((uint32_t)n_, cur_, sc_, st_);
+            launches_ += 1;
+        }
+        launch_pressure((uint32_t)n_, kc_, cur_, sc_, st_);
     }
-    launch_pressure((uint32_t)n_, kc_, cur_, sc_, st_);
     prof_end();
     launches_ += 1;
     check(cudaGetLastError(), "pressure");
@@ -488,13 +542,23 @@ void World::run_pressure() {
 
 void World::run_forces(bool integrate, double dt) {
     ensure_lists();
-    prof_begin(kForces);
-    launch_forces((uint32_t)n_, kc_, cur_, lists_, sc_, integrate, dt, pos_nx_, vel_nx_, st_);
-    prof_end();
-    prof_begin(kBoundaryForce);
-    launch_boundary_force((uint32_t)n_, kc_, cur_, lists_, st_);
-    prof_end();
-    launches_ += 2;
+    if (f32_) {
+        // the single-precision form always integrates into the next buffers;
+        // without a kick/drift request the step is taken with dt = 0
+        prof_begin(kForces);
+        launch_forces_f32((uint32_t)n_, kf_, cur_, fb_, lists_, sc_, integrate ? (float)dt : 0.f,
+                          pos_nx_, vel_nx_, bf32_, st_);
+        prof_end();
+        launches_ += 2;
+    } else {
+        prof_begin(kForces);
+        launch_forces((uint32_t)n_, kc_, cur_, lists_, sc_, integrate, dt, pos_nx_, vel_nx_, st_);
+        prof_end();
+        prof_begin(kBoundaryForce);
+        launch_boundary_force((uint32_t)n_, kc_, cur_, lists_, st_);
+        prof_end();
+        launches_ += 2;
+    }
     check(cudaGetLastError(), "forces");
 }
 
@@ -502,6 +566,14 @@ void World::run_xsph() {
     if (prm_.xsph_epsilon == 0.0) return;  // wcsph.rs:285
     ensure_lists();
     prof_begin(kXsph);
+    if (f32_) {
+        launch_xsph_f32((uint32_t)n_, kf_, cur_, fb_, lists_, velf_alt_, st_);
+        prof_end();
+        launches_ += 1;
+        check(cudaGetLastError(), "xsph");
+        std::swap(fb_.vel, velf_alt_);
+        return;
+    }
     launch_xsph((uint32_t)n_, kc_, cur_, lists_, vel_nx_, st_);
     prof_end();
     launches_ += 1;
@@ -513,6 +585,7 @@ void World::run_xsph() {
 
 void World::rebuild_grid() {
     build_grid(nullptr, nullptr);
+    refresh_f32();
     grid_current_ = true;
     rho_current_ = false;
 }
@@ -534,11 +607,13 @@ void World::step(double dt) {
     // they are reused.
     if (!(grid_current_ && rho_current_)) {
         build_grid(nullptr, nullptr);
+        refresh_f32();
         run_density();
     }
     run_pressure();               // wcsph.rs:329
     run_forces(true, dt);         // wcsph.rs:330-342 (kick + drift fused)
     build_grid(pos_nx_, vel_nx_); // wcsph.rs:343
+    refresh_f32();
     run_density();                // wcsph.rs:344
     run_xsph();                   // wcsph.rs:345
     t_ += dt;                     // wcsph.rs:346
@@ -622,6 +697,7 @@ void World::set_vec(int which, const double* in) {
     // stores them; they never move), so both kinds are written.
     k_import_vec<<<blocks_for(n, 256), 256, 0, st_>>>(n, slot_of_orig_, xfer_,
                                                       which == 0 ? cur_.pos : cur_.vel, cur_.flags, 0);
+    refresh_f32();
     check(cudaStreamSynchronize(st_), "import");
     if (which == 0) {
         grid_current_ = false;
@@ -647,6 +723,7 @@ void World::set_scalar(int which, const double* in) {
     k_import_w<<<blocks_for(n, 256), 256, 0, st_>>>(n, slot_of_orig_, xfer_,
                                                     which == 0 ? cur_.vel : nullptr, cur_.p);
     k_refresh_pr2<<<blocks_for(n, 256), 256, 0, st_>>>(n, cur_.flags, cur_.p, cur_.pos, cur_.vel);
+    refresh_f32();
     check(cudaStreamSynchronize(st_), "import");
     if (which == 0) rho_current_ = false;
 }

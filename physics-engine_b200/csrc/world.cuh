@@ -31,6 +31,7 @@ struct WorldConfig {
     uint32_t max_lower;         // reserved
     double domain_margin;       // extra grid domain per side, fraction of extent (<0 = 0.25)
     uint32_t domain_margin_cells;  // minimum extra cells per side (0 = 4)
+    int precision;              // 0 = f64 (reference bits), 1 = single-precision form
 };
 
 class CudaError : public std::runtime_error {
@@ -107,6 +108,7 @@ class World {
     void run_forces(bool integrate, double dt);
     void run_xsph();
     void refresh_step_const();
+    void refresh_f32();
     void configure_lists();
     void alloc_lists(uint32_t part_cap);
     template <typename T>
@@ -141,11 +143,19 @@ class World {
     std::vector<void*> allocs_;
     std::vector<void*> list_allocs_;
 
+    // single-precision form
+    bool f32_ = false;
+    F32Const kf_{};
+    F32Bufs fb_{};
+    float4* velf_alt_ = nullptr;
+    float* bf32_ = nullptr;
+
     bool grid_built_ = false;    // a grid exists (rebuild_grid ran at least once)
     bool grid_current_ = false;  // grid built from the current positions
     bool rho_current_ = false;   // densities computed from the current grid and positions
     bool lists_valid_ = false;   // neighbour lists match the grid and positions
     bool lists_checked_ = false; // list capacity verified for the current positions
+    bool lists_sized_ = false;   // the first list sizing has been done
     uint32_t launches_ = 0;
 
     struct PhaseRec {

@@ -81,7 +81,11 @@ class _Config(C.Structure):
         ("max_lower", C.c_uint32),
         ("domain_margin", C.c_double),
         ("domain_margin_cells", C.c_uint32),
+        ("precision", C.c_int32),
     ]
+
+
+PRECISION_F64, PRECISION_F32 = 0, 1
 
 
 class _Profile(C.Structure):
@@ -357,9 +361,10 @@ class WcsphConfig:
     """GPU placement and capacities (no reference counterpart)."""
 
     def __init__(self, device=-1, max_neighbours=0, max_lower=0, domain_margin=-1.0,
-                 domain_margin_cells=0):
+                 domain_margin_cells=0, precision=PRECISION_F64):
         self.device, self.max_neighbours, self.max_lower = device, max_neighbours, max_lower
         self.domain_margin, self.domain_margin_cells = domain_margin, domain_margin_cells
+        self.precision = precision
 
     def _to_c(self):
         c = _Config()
@@ -368,6 +373,7 @@ class WcsphConfig:
         c.max_lower = int(self.max_lower)
         c.domain_margin = float(self.domain_margin)
         c.domain_margin_cells = int(self.domain_margin_cells)
+        c.precision = int(self.precision)
         return c
 
 
@@ -474,8 +480,11 @@ class WcsphWorld:
         _ok(_lib.pe_fluid_wcsph_set_params(self._w, C.byref(p._to_c())), "set_params")
 
     # -- state in original order --
-    def _get3(self, fn, what):
-        out = np.empty((self.n, 3))
+    def _get3(self, fn, what, out=None):
+        if out is None:
+            out = np.empty((self.n, 3))
+        elif out.shape != (self.n, 3) or out.dtype != np.float64 or not out.flags.c_contiguous:
+            raise ValueError(f"{what}: out must be a C-contiguous float64 array of shape ({self.n}, 3)")
         _ok(fn(self._w, _ptr(out), self.n), what)
         return out
 
@@ -484,11 +493,12 @@ class WcsphWorld:
         _ok(fn(self._w, _ptr(out), self.n), what)
         return out
 
-    def positions(self):
-        return self._get3(_lib.pe_fluid_wcsph_get_positions, "get_positions")
+    def positions(self, out=None):
+        """Positions in original order; `out` (n x 3 float64, e.g. pinned) is filled in place."""
+        return self._get3(_lib.pe_fluid_wcsph_get_positions, "get_positions", out)
 
-    def velocities(self):
-        return self._get3(_lib.pe_fluid_wcsph_get_velocities, "get_velocities")
+    def velocities(self, out=None):
+        return self._get3(_lib.pe_fluid_wcsph_get_velocities, "get_velocities", out)
 
     def accelerations(self):
         return self._get3(_lib.pe_fluid_wcsph_get_accelerations, "get_accelerations")
