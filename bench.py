@@ -351,6 +351,7 @@ def main():
     world.set_profiling(False)
     clocks = sampler.stop()
     status = world.status()
+    cap = world.capacity_info()
     if ws > 1:
         t = torch.tensor([ms], device="cuda")
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
@@ -404,6 +405,9 @@ def main():
         "gpu_launches": int(launches),
         "status": int(status),
         "phases_ms_per_step": {k: v[0] / max(1, args.steps) for k, v in prof.items()},
+        "neighbour_lists": {"used_gb": cap["list_groups_used"] * 16 / 1e9,
+                            "pool_gb": cap["list_groups_capacity"] * 16 / 1e9,
+                            "union_stage": cap["union_capacity"], "max_union": cap["max_union"]},
         "roofline": {"bound": "hbm", "kernel": "k_forces (force + kick + drift)",
                      "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                      "frac": achieved / hbm_peak, "peak_kind": peak_kind, "traffic": None,

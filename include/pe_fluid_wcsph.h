@@ -83,8 +83,9 @@ typedef struct PeWcsphParams {
 /* GPU placement and capacities (no reference counterpart; zeros = defaults). */
 typedef struct PeWcsphConfig {
     int32_t device;               /* CUDA device ordinal; -1 = the current device */
-    uint32_t max_neighbours;      /* initial capacity of each half of a particle's neighbour
-                                     lists (0 = 256); grows on the first build if short */
+    uint32_t max_neighbours;      /* first guess of list entries per particle for the
+                                     neighbour-list pool (0 = 256); the first build
+                                     measures the need and resizes the pool */
     uint32_t max_lower;           /* reserved, set to 0 */
     double domain_margin;         /* grid domain growth per side, fraction of extent (<0 = 0.25) */
     uint32_t domain_margin_cells; /* minimum growth per side in cells (0 = 4) */
@@ -212,9 +213,9 @@ int pe_fluid_wcsph_get_neighbour_counts(PeWcsph* w, uint32_t* candidates, uint32
 int pe_fluid_wcsph_status(PeWcsph* w, uint32_t* status);
 int pe_fluid_wcsph_clear_status(PeWcsph* w);
 /* Capacity introspection (no reference counterpart): out = {status bits,
- * largest neighbour-cell union seen, longest list part of the last build,
- * union stage capacity, list part capacity, occupied cells, dense cells,
- * list-build CTAs}. */
+ * largest neighbour-cell union seen, 16-byte list groups the last list build
+ * asked for, union stage capacity, list pool capacity in 16-byte groups,
+ * occupied cells, dense cells, list-build CTAs}. */
 int pe_fluid_wcsph_capacity_info(PeWcsph* w, uint64_t out[8]);
 int pe_fluid_wcsph_diagnostics(PeWcsph* w, PeFluidDiagnostics* out);
 /* Per-phase device time, measured with CUDA events on the world's stream:

@@ -21,10 +21,12 @@
 // all fluid neighbours, both in ascending original index; the order comes
 // from a shared-memory radix sort of the union's fluid entries per cell.
 //
-// Each centre particle is served by two threads in different warps that
-// split its candidates in halves (union words, or sorted positions) and write
-// to the two halves of the particle's list storage; consumers read part 0 and
-// then part 1, which is the full list in order.
+// Both kernels work on chunks of up to 64 centre particles with four threads
+// per particle, each taking a quarter of the candidates (union words, or
+// sorted positions). A first pass keeps the in-support bit masks in shared
+// memory and counts; the chunk's longest lists size one block of the list
+// pool, reserved with one atomic add; a second pass writes each quarter's
+// entries at its offset in the list.
 #include <climits>
 
 #include "pe_math.cuh"
@@ -34,28 +36,17 @@ namespace pe {
 
 namespace {
 
-constexpr int kNlThreads = 128;
-constexpr uint32_t kHalf = kNlThreads / 2;
+constexpr int kNlThreads = 256;
+constexpr uint32_t kChunk = 64;                    // centre particles per chunk
+constexpr uint32_t kWays = kNlThreads / kChunk;    // threads per centre particle
+constexpr uint32_t kWarps = kNlThreads / 32;
 constexpr uint32_t kMaxUnionStage = 8192;
+constexpr uint32_t kStageStep = 256;               // stage capacities are multiples of this
 
 // Staged word w of a union entry: original index (29 bits) | kind flags.
 constexpr uint32_t kStageBoundary = 1u << 31;
 constexpr uint32_t kStageOriented = 1u << 30;
 constexpr uint32_t kStageOrigMask = (1u << 29) - 1u;
-
-__device__ __forceinline__ void emit(uint32_t* list, uint32_t slot, uint32_t t, uint32_t cap,
-                                     uint32_t value) {
-    if (t < cap) list[list_index(slot, t, cap)] = value;
-}
-
-// Base of slot s's entries in a list (entry t at base[(t & ~3) * 32 + (t & 3)]).
-__device__ __forceinline__ uint32_t* slot_base(uint32_t* list, uint32_t s, uint32_t cap) {
-    return list + (size_t)(s >> 5) * cap * 32u + (s & 31u) * 4u;
-}
-
-__device__ __forceinline__ void put(uint32_t* base, uint32_t t, uint32_t value) {
-    base[(t & ~3u) * 32u + (t & 3u)] = value;
-}
 
 template <int NC>
 __device__ __forceinline__ uint32_t slot_of_union(const uint32_t* s_off, const uint32_t* s_cstart,
@@ -75,7 +66,7 @@ __device__ __forceinline__ uint32_t entry_flags(uint32_t w) {
 
 // Block-wide exclusive scan (kNlThreads threads).
 __device__ __forceinline__ void block_exclusive_scan(uint32_t v, uint32_t* ex, uint32_t* total) {
-    __shared__ uint32_t warp_sums[kNlThreads / 32];
+    __shared__ uint32_t warp_sums[kWarps];
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     uint32_t incl = v;
 #pragma unroll
@@ -87,13 +78,19 @@ __device__ __forceinline__ void block_exclusive_scan(uint32_t v, uint32_t* ex, u
     __syncthreads();
     uint32_t before = 0, tot = 0;
 #pragma unroll
-    for (uint32_t w = 0; w < kNlThreads / 32; ++w) {
+    for (uint32_t w = 0; w < kWarps; ++w) {
         if (w < warp) before += warp_sums[w];
         tot += warp_sums[w];
     }
     *ex = before + incl - v;
     *total = tot;
     __syncthreads();
+}
+
+__device__ __forceinline__ uint32_t warp_max(uint32_t v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
 }
 
 struct CellUnion {
@@ -168,9 +165,53 @@ __device__ __forceinline__ bool within(const float4& q, const float4& me, float 
     return dx * dx + dy * dy + dz * dz <= r2f;
 }
 
+__device__ __forceinline__ uint32_t rows_for(uint32_t n) { return (n + 3u) >> 2; }
+
+// Reserved block of one chunk: `rows_a + rows_b` rows of `stride` groups.
+struct ChunkBlock {
+    unsigned long long base;  // group index of row 0, lane 0
+    uint32_t rows_a, rows_b;
+    bool ok;
+};
+
+// Every thread passes its (a, b) list lengths; thread 0 reserves the block for
+// the chunk's longest ones and all threads return it.
+__device__ __forceinline__ ChunkBlock reserve_chunk(const ListBufs& l, DeviceScalars* sc, uint32_t stride,
+                                                    uint32_t na, uint32_t nb, uint32_t (*s_red)[2],
+                                                    ChunkBlock* s_blk, bool* s_overflow) {
+    const uint32_t a = warp_max(na), b = warp_max(nb);
+    if ((threadIdx.x & 31u) == 0) {
+        s_red[threadIdx.x >> 5][0] = a;
+        s_red[threadIdx.x >> 5][1] = b;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t ma = 0, mb = 0;
+#pragma unroll
+        for (uint32_t w = 0; w < kWarps; ++w) {
+            ma = max(ma, s_red[w][0]);
+            mb = max(mb, s_red[w][1]);
+        }
+        ChunkBlock blk;
+        blk.rows_a = rows_for(ma);
+        blk.rows_b = rows_for(mb);
+        const unsigned long long groups = (unsigned long long)(blk.rows_a + blk.rows_b) * stride;
+        blk.base = groups ? atomicAdd(&sc->list_used, groups) : 0ull;
+        // counts, strides and row offsets are stored in 16 bits
+        const bool fits16 = ma < 65536u && mb < 65536u && stride < 65536u && blk.rows_a < 65536u;
+        blk.ok = fits16 && blk.base + groups <= l.pool_groups;
+        if (!blk.ok) *s_overflow = true;
+        *s_blk = blk;
+    }
+    __syncthreads();
+    return *s_blk;
+}
+
 // ----------------------------------------------------------------- visit
-// Shared memory: float4 s_pos[ucap]; uint32 s_ent[ucap].
-template <int DIM>
+// Dynamic shared memory (ucap a multiple of kStageStep): float4 s_pos[ucap];
+// uint32 s_ent[ucap]; uint32 s_mask[(ucap / 32) * kChunk] (word w of chunk
+// lane c at s_mask[w * kChunk + c]).
+template <int DIM, bool UPPER>
 __global__ void __launch_bounds__(kNlThreads) k_nlist_visit(GridDesc g, StepConst k, uint32_t ucap,
                                                             const uint32_t* __restrict__ occ,
                                                             const uint32_t* __restrict__ cell_start,
@@ -180,17 +221,20 @@ __global__ void __launch_bounds__(kNlThreads) k_nlist_visit(GridDesc g, StepCons
     extern __shared__ __align__(16) unsigned char smem[];
     float4* s_pos = reinterpret_cast<float4*>(smem);
     uint32_t* s_ent = reinterpret_cast<uint32_t*>(s_pos + ucap);
+    uint32_t* s_mask = s_ent + ucap;
     __shared__ uint32_t s_cstart[NC];
     __shared__ uint32_t s_off[NC + 1];
+    __shared__ uint32_t s_cv[kWays][kChunk], s_cu[kWays][kChunk];
+    __shared__ uint32_t s_red[kWarps][2];
+    __shared__ ChunkBlock s_blk;
+    __shared__ bool s_overflow;
 
     const float r2f = k.r2_filter;
     const uint32_t nocc = sc->nocc;
     const uint32_t tid = threadIdx.x;
-    const uint32_t part = tid / kHalf;
-    const uint32_t half_cap = l.capv >> 1;
-    const size_t n = l.nslots;
-    bool overflow = false;
-    uint32_t max_union = 0, longest = 0;
+    const uint32_t lane = tid % kChunk, q = tid / kChunk;
+    uint32_t max_union = 0;
+    if (tid == 0) s_overflow = false;
 
     for (uint32_t it = blockIdx.x; it < nocc; it += gridDim.x) {
         const CellUnion cu = cell_union<DIM>(g, occ[it], cell_start, s_cstart, s_off);
@@ -201,105 +245,183 @@ __global__ void __launch_bounds__(kNlThreads) k_nlist_visit(GridDesc g, StepCons
                 const uint32_t slot = slot_of_union<NC>(s_off, s_cstart, u);
                 uint8_t fl;
                 uint32_t o;
-                const float4 q = stage_entry<DIM>(s, slot, cu, &fl, &o);
-                s_pos[u] = q;
-                s_ent[u] = slot | entry_flags(__float_as_uint(q.w));
+                const float4 p = stage_entry<DIM>(s, slot, cu, &fl, &o);
+                s_pos[u] = p;
+                s_ent[u] = slot | entry_flags(__float_as_uint(p.w));
             }
             __syncthreads();
-            const uint32_t W = (U + 31u) >> 5, Wh = (W + 1u) >> 1;
-            const uint32_t w0 = part ? Wh : 0u, w1 = part ? W : Wh;
-            const uint32_t base = part * half_cap;
-            for (uint32_t pi = tid % kHalf; pi < cu.ncenter; pi += kHalf) {
-                const uint32_t kslot = cu.cs + pi;
-                const uint32_t myu = cu.center_off + pi;
-                const float4 me = s_pos[myu];
-                const uint32_t mw = __float_as_uint(me.w);
-                const uint32_t myo = mw & kStageOrigMask;
-                uint32_t nv = 0, nu = 0;
-                uint32_t* vb = slot_base(l.visit, kslot, l.capv) ;
-                // no upper list storage in the single-precision form (visit list only)
-                uint32_t* ub = l.upper ? slot_base(l.upper, kslot, l.capv) : nullptr;
-                if (!(mw & kStageBoundary)) {
-                    for (uint32_t w = w0; w < w1; ++w) {
-                        uint32_t m = 0;
+            const uint32_t W = (U + 31u) >> 5;
+            const uint32_t wb = W * q / kWays, we = W * (q + 1) / kWays;
+            for (uint32_t c0 = 0; c0 < cu.ncenter; c0 += kChunk) {
+                const uint32_t nc = min(kChunk, cu.ncenter - c0);
+                const bool active = lane < nc;
+                const uint32_t myu = cu.center_off + c0 + lane;
+                bool fluidc = false;
+                uint32_t myo = 0;
+                // ---- pass 1: in-support masks of this quarter's words, counts
+                if (active) {
+                    const float4 me = s_pos[myu];
+                    const uint32_t mw = __float_as_uint(me.w);
+                    fluidc = !(mw & kStageBoundary);
+                    myo = mw & kStageOrigMask;
+                    uint32_t cv = 0, cl = 0;
+                    if (fluidc) {
+                        for (uint32_t w = wb; w < we; ++w) {
+                            uint32_t m = 0;
 #pragma unroll
-                        for (int bit = 0; bit < 32; ++bit)
-                            m |= within(s_pos[(w << 5) + bit], me, r2f) ? (1u << bit) : 0u;
-                        if (w == W - 1u && (U & 31u)) m &= (1u << (U & 31u)) - 1u;
-                        if (w == (myu >> 5)) m &= ~(1u << (myu & 31u));
-                        while (m) {
-                            const uint32_t u = (w << 5) + (__ffs(m) - 1);
-                            m &= m - 1u;
-                            const uint32_t ow = __float_as_uint(s_pos[u].w);
-                            uint32_t e = s_ent[u];
-                            if (!(ow & kStageBoundary) && (ow & kStageOrigMask) < myo) {
-                                e |= kEntryLower;
-                            } else {
-                                if (ub && nu < half_cap) put(ub, base + nu, e);
-                                ++nu;
+                            for (int bit = 0; bit < 32; ++bit)
+                                m |= within(s_pos[(w << 5) + bit], me, r2f) ? (1u << bit) : 0u;
+                            if (w == W - 1u && (U & 31u)) m &= (1u << (U & 31u)) - 1u;
+                            if (w == (myu >> 5)) m &= ~(1u << (myu & 31u));
+                            s_mask[w * kChunk + lane] = m;
+                            cv += __popc(m);
+                            if (UPPER) {
+                                uint32_t mm = m;
+                                while (mm) {
+                                    const uint32_t u = (w << 5) + (__ffs(mm) - 1);
+                                    mm &= mm - 1u;
+                                    const uint32_t ow = __float_as_uint(s_pos[u].w);
+                                    cl += (!(ow & kStageBoundary) && (ow & kStageOrigMask) < myo) ? 1u : 0u;
+                                }
                             }
-                            if (nv < half_cap) put(vb, base + nv, e);
-                            ++nv;
+                        }
+                    }
+                    s_cv[q][lane] = cv;
+                    s_cu[q][lane] = cv - cl;
+                }
+                __syncthreads();
+                // ---- list lengths, this quarter's offsets, the chunk's block
+                uint32_t nv = 0, nu = 0, ov = 0, ou = 0;
+                if (active) {
+#pragma unroll
+                    for (uint32_t r = 0; r < kWays; ++r) {
+                        const uint32_t a = s_cv[r][lane], b = s_cu[r][lane];
+                        if (r < q) {
+                            ov += a;
+                            ou += b;
+                        }
+                        nv += a;
+                        nu += b;
+                    }
+                    if (!UPPER) nu = ou = 0;
+                }
+                const ChunkBlock blk = reserve_chunk(l, sc, nc, nv, nu, s_red, &s_blk, &s_overflow);
+                // ---- pass 2: descriptors and entries
+                if (active) {
+                    const uint32_t kslot = cu.cs + c0 + lane;
+                    const uint32_t gv = (uint32_t)blk.base + lane;  // < pool_groups < 2^32 when ok
+                    if (q == 0) {
+                        l.desc[kslot] = blk.ok ? make_uint4(gv, nc | (blk.rows_a << 16), nv | (nu << 16), 0u)
+                                               : make_uint4(0u, 0u, 0u, 0u);
+                        l.ncand[kslot] = fluidc ? U : 0u;
+                    }
+                    if (blk.ok && fluidc) {
+                        const size_t step = 4u * nc;
+                        uint32_t* pv = l.pool + 4 * (size_t)gv;
+                        uint32_t* pu = l.pool + 4 * ((size_t)gv + (size_t)blk.rows_a * nc);
+                        uint32_t tv = ov, tu = ou;
+                        for (uint32_t w = wb; w < we; ++w) {
+                            uint32_t m = s_mask[w * kChunk + lane];
+                            while (m) {
+                                const uint32_t u = (w << 5) + (__ffs(m) - 1);
+                                m &= m - 1u;
+                                uint32_t e = s_ent[u];
+                                if (UPPER) {
+                                    const uint32_t ow = __float_as_uint(s_pos[u].w);
+                                    if (!(ow & kStageBoundary) && (ow & kStageOrigMask) < myo) {
+                                        e |= kEntryLower;
+                                    } else {
+                                        pu[(tu >> 2) * step + (tu & 3u)] = e;
+                                        ++tu;
+                                    }
+                                }
+                                pv[(tv >> 2) * step + (tv & 3u)] = e;
+                                ++tv;
+                            }
                         }
                     }
                 }
-                longest = max(longest, nv);
-                if (nv > half_cap) { overflow = true; nv = half_cap; }
-                if (nu > half_cap) nu = half_cap;
-                l.nvisit[part * n + kslot] = nv;
-                l.nupper[part * n + kslot] = nu;
-                if (part == 0) l.ncand[kslot] = (mw & kStageBoundary) ? 0u : U;
+                __syncthreads();  // masks and counts are reused by the next chunk
             }
         } else {
-            // slow path: a union larger than the stage, straight from global memory
+            // Slow path: a union larger than the stage, straight from global
+            // memory, one thread per centre particle: count, reserve, write.
             if (tid == 0) atomicOr(&sc->status, kStatusSlowUnion);
-            for (uint32_t kslot = cu.cs + tid; kslot < cu.cs + cu.ncenter; kslot += blockDim.x) {
-                uint8_t mfl;
-                uint32_t myo;
-                const float4 me = stage_entry<DIM>(s, kslot, cu, &mfl, &myo);
-                const bool fluid = !(mfl & kFlagBoundary);
-                uint32_t nv = 0, nu = 0;
-                if (fluid) {
-                    for (int q = 0; q < NC; ++q) {
-                        const uint32_t q0 = s_cstart[q], q1 = q0 + (s_off[q + 1] - s_off[q]);
-                        for (uint32_t slot = q0; slot < q1; ++slot) {
-                            if (slot == kslot) continue;
-                            uint8_t fl;
-                            uint32_t o;
-                            const float4 qp = stage_entry<DIM>(s, slot, cu, &fl, &o);
-                            if (!within(qp, me, r2f)) continue;
-                            uint32_t e = slot | entry_flags(__float_as_uint(qp.w));
-                            if (!(fl & kFlagBoundary) && o < myo) {
-                                e |= kEntryLower;
-                            } else {
-                                if (l.upper && nu < half_cap) emit(l.upper, kslot, nu, l.capv, e);
-                                ++nu;
+            for (uint32_t c0 = 0; c0 < cu.ncenter; c0 += kNlThreads) {
+                const uint32_t nc = min((uint32_t)kNlThreads, cu.ncenter - c0);
+                const bool active = tid < nc;
+                const uint32_t kslot = cu.cs + c0 + tid;
+                uint8_t mfl = 0;
+                uint32_t myo = 0;
+                float4 me = make_float4(0.f, 0.f, 0.f, 0.f);
+                uint32_t nv = 0, nl = 0;
+                bool fluidc = false;
+                if (active) {
+                    me = stage_entry<DIM>(s, kslot, cu, &mfl, &myo);
+                    fluidc = !(mfl & kFlagBoundary);
+                    if (fluidc) {
+                        for (int c = 0; c < NC; ++c) {
+                            const uint32_t q0 = s_cstart[c], q1 = q0 + (s_off[c + 1] - s_off[c]);
+                            for (uint32_t slot = q0; slot < q1; ++slot) {
+                                if (slot == kslot) continue;
+                                uint8_t fl;
+                                uint32_t o;
+                                if (!within(stage_entry<DIM>(s, slot, cu, &fl, &o), me, r2f)) continue;
+                                ++nv;
+                                if (!(fl & kFlagBoundary) && o < myo) ++nl;
                             }
-                            if (nv < half_cap) emit(l.visit, kslot, nv, l.capv, e);
-                            ++nv;
                         }
                     }
                 }
-                longest = max(longest, nv);
-                if (nv > half_cap) { overflow = true; nv = half_cap; }
-                if (nu > half_cap) nu = half_cap;
-                l.nvisit[kslot] = nv;
-                l.nupper[kslot] = nu;
-                l.nvisit[n + kslot] = 0;
-                l.nupper[n + kslot] = 0;
-                l.ncand[kslot] = fluid ? U : 0u;
+                const uint32_t nu = UPPER ? nv - nl : 0u;
+                const ChunkBlock blk = reserve_chunk(l, sc, nc, nv, nu, s_red, &s_blk, &s_overflow);
+                if (active) {
+                    const uint32_t gv = (uint32_t)blk.base + tid;
+                    l.desc[kslot] = blk.ok ? make_uint4(gv, nc | (blk.rows_a << 16), nv | (nu << 16), 0u)
+                                           : make_uint4(0u, 0u, 0u, 0u);
+                    l.ncand[kslot] = fluidc ? U : 0u;
+                    if (blk.ok && fluidc) {
+                        const size_t step = 4u * nc;
+                        uint32_t* pv = l.pool + 4 * (size_t)gv;
+                        uint32_t* pu = l.pool + 4 * ((size_t)gv + (size_t)blk.rows_a * nc);
+                        uint32_t tv = 0, tu = 0;
+                        for (int c = 0; c < NC; ++c) {
+                            const uint32_t q0 = s_cstart[c], q1 = q0 + (s_off[c + 1] - s_off[c]);
+                            for (uint32_t slot = q0; slot < q1; ++slot) {
+                                if (slot == kslot) continue;
+                                uint8_t fl;
+                                uint32_t o;
+                                const float4 qp = stage_entry<DIM>(s, slot, cu, &fl, &o);
+                                if (!within(qp, me, r2f)) continue;
+                                uint32_t e = slot | entry_flags(__float_as_uint(qp.w));
+                                if (UPPER) {
+                                    if (!(fl & kFlagBoundary) && o < myo) {
+                                        e |= kEntryLower;
+                                    } else {
+                                        if (tu < nu) pu[(tu >> 2) * step + (tu & 3u)] = e;
+                                        ++tu;
+                                    }
+                                }
+                                if (tv < nv) pv[(tv >> 2) * step + (tv & 3u)] = e;
+                                ++tv;
+                            }
+                        }
+                    }
+                }
+                __syncthreads();
             }
         }
         __syncthreads();  // shared memory is reused by the next cell
     }
-    if (overflow) atomicOr(&sc->status, kStatusListOverflow);
+    if (tid == 0 && s_overflow) atomicOr(&sc->status, kStatusListOverflow);
     if (tid == 0 && max_union) atomicMax(&sc->max_union, max_union);
-    if (longest) atomicMax(&sc->max_part, longest);
 }
 
 // ----------------------------------------------------------------- lower
-// Shared memory: float4 s_pos[ucap]; uint32 s_ent[ucap]; uint16 s_sorted[ucap];
-// uint16 s_tmp[ucap]; uint16 s_cnt[16][kNlThreads].
+// Dynamic shared memory: float4 s_pos[ucap]; uint32 s_ent[ucap] (slot);
+// uint16 s_sorted[ucap]; then a region used first by the radix sort
+// (uint16 s_tmp[ucap], uint16 s_cnt[16 * kNlThreads]) and then by the
+// in-support masks over sorted positions (uint32 s_mask[(ucap / 32) * kChunk]).
 template <int DIM>
 __global__ void __launch_bounds__(kNlThreads) k_nlist_lower(GridDesc g, StepConst k, uint32_t ucap,
                                                             const uint32_t* __restrict__ occ,
@@ -311,20 +433,22 @@ __global__ void __launch_bounds__(kNlThreads) k_nlist_lower(GridDesc g, StepCons
     float4* s_pos = reinterpret_cast<float4*>(smem);
     uint32_t* s_ent = reinterpret_cast<uint32_t*>(s_pos + ucap);
     uint16_t* s_sorted = reinterpret_cast<uint16_t*>(s_ent + ucap);
-    uint16_t* s_tmp = s_sorted + ucap;
+    uint32_t* s_mask = reinterpret_cast<uint32_t*>(s_sorted + ucap);
+    uint16_t* s_tmp = reinterpret_cast<uint16_t*>(s_mask);
     uint16_t* s_cnt = s_tmp + ucap;
     __shared__ uint32_t s_cstart[NC];
     __shared__ uint32_t s_off[NC + 1];
     __shared__ uint32_t s_nf, s_omin, s_omax;
+    __shared__ uint32_t s_cl[kWays][kChunk];
+    __shared__ uint32_t s_red[kWarps][2];
+    __shared__ ChunkBlock s_blk;
+    __shared__ bool s_overflow;
 
     const float r2f = k.r2_filter;
     const uint32_t nocc = sc->nocc;
     const uint32_t tid = threadIdx.x;
-    const uint32_t part = tid / kHalf;
-    const uint32_t half_cap = l.capl >> 1;
-    const size_t n = l.nslots;
-    bool overflow = false;
-    uint32_t longest = 0;
+    const uint32_t lane = tid % kChunk, q = tid / kChunk;
+    if (tid == 0) s_overflow = false;
 
     for (uint32_t it = blockIdx.x; it < nocc; it += gridDim.x) {
         if (tid == 0) {
@@ -372,16 +496,16 @@ __global__ void __launch_bounds__(kNlThreads) k_nlist_lower(GridDesc g, StepCons
                     {
                         uint32_t v[16], sum = 0;
 #pragma unroll
-                        for (int q = 0; q < 16; ++q) {
-                            v[q] = s_cnt[tid * 16 + q];
-                            sum += v[q];
+                        for (int d = 0; d < 16; ++d) {
+                            v[d] = s_cnt[tid * 16 + d];
+                            sum += v[d];
                         }
                         uint32_t ex, tot;
                         block_exclusive_scan(sum, &ex, &tot);
 #pragma unroll
-                        for (int q = 0; q < 16; ++q) {
-                            s_cnt[tid * 16 + q] = (uint16_t)ex;
-                            ex += v[q];
+                        for (int d = 0; d < 16; ++d) {
+                            s_cnt[tid * 16 + d] = (uint16_t)ex;
+                            ex += v[d];
                         }
                     }
                     __syncthreads();
@@ -397,143 +521,217 @@ __global__ void __launch_bounds__(kNlThreads) k_nlist_lower(GridDesc g, StepCons
                 }
                 if (src != s_sorted) {
                     for (uint32_t i = tid; i < nf; i += blockDim.x) s_sorted[i] = src[i];
-                    __syncthreads();
                 }
+                __syncthreads();
             }
-            const uint32_t base = part * half_cap;
-            for (uint32_t pi = tid % kHalf; pi < cu.ncenter; pi += kHalf) {
-                const uint32_t kslot = cu.cs + pi;
-                const float4 me = s_pos[cu.center_off + pi];
-                const uint32_t mw = __float_as_uint(me.w);
-                const uint32_t myo = mw & kStageOrigMask;
-                // R = number of fluid union entries below this particle's index
-                uint32_t R = nf;
-                if (!(mw & kStageBoundary)) {
-                    uint32_t lo = 0, hi = nf;
-                    while (lo < hi) {
-                        const uint32_t mid = (lo + hi) >> 1;
-                        const uint32_t o = __float_as_uint(s_pos[s_sorted[mid]].w) & kStageOrigMask;
-                        if (o < myo) lo = mid + 1;
-                        else hi = mid;
+            for (uint32_t c0 = 0; c0 < cu.ncenter; c0 += kChunk) {
+                const uint32_t nc = min(kChunk, cu.ncenter - c0);
+                const bool active = lane < nc;
+                uint32_t wb = 0, we = 0, R = 0;
+                // ---- pass 1: in-support masks over this quarter's sorted words
+                if (active) {
+                    const float4 me = s_pos[cu.center_off + c0 + lane];
+                    const uint32_t mw = __float_as_uint(me.w);
+                    const uint32_t myo = mw & kStageOrigMask;
+                    // R = fluid union entries below this particle's index (all
+                    // of them for a boundary particle)
+                    R = nf;
+                    if (!(mw & kStageBoundary)) {
+                        uint32_t lo = 0, hi = nf;
+                        while (lo < hi) {
+                            const uint32_t mid = (lo + hi) >> 1;
+                            const uint32_t o = __float_as_uint(s_pos[s_sorted[mid]].w) & kStageOrigMask;
+                            if (o < myo) lo = mid + 1;
+                            else hi = mid;
+                        }
+                        R = lo;
                     }
-                    R = lo;
-                }
-                const uint32_t i_begin = part ? (R >> 1) : 0u, i_end = part ? R : (R >> 1);
-                uint32_t nl = 0;
-                uint32_t* lb = slot_base(l.lower, kslot, l.capl);
-                for (uint32_t i0 = i_begin; i0 < i_end; i0 += 32) {
-                    uint32_t m = 0;
+                    const uint32_t WR = (R + 31u) >> 5;
+                    wb = WR * q / kWays;
+                    we = WR * (q + 1) / kWays;
+                    uint32_t cl = 0;
+                    for (uint32_t w = wb; w < we; ++w) {
+                        uint32_t m = 0;
 #pragma unroll
-                    for (int bit = 0; bit < 32; ++bit) {
-                        const uint32_t i = i0 + bit;
-                        m |= within(s_pos[s_sorted[i < nf ? i : 0u]], me, r2f) ? (1u << bit) : 0u;
+                        for (int bit = 0; bit < 32; ++bit) {
+                            const uint32_t i = (w << 5) + bit;
+                            m |= within(s_pos[s_sorted[i < nf ? i : 0u]], me, r2f) ? (1u << bit) : 0u;
+                        }
+                        if (w == WR - 1u && (R & 31u)) m &= (1u << (R & 31u)) - 1u;
+                        s_mask[w * kChunk + lane] = m;
+                        cl += __popc(m);
                     }
-                    if (i_end - i0 < 32u) m &= (1u << (i_end - i0)) - 1u;
-                    while (m) {
-                        const uint32_t i = i0 + (__ffs(m) - 1);
-                        m &= m - 1u;
-                        if (nl < half_cap) put(lb, base + nl, s_ent[s_sorted[i]]);
-                        ++nl;
+                    s_cl[q][lane] = cl;
+                }
+                __syncthreads();
+                // ---- list length, this quarter's offset, the chunk's block
+                uint32_t nl = 0, ol = 0;
+                if (active) {
+#pragma unroll
+                    for (uint32_t r = 0; r < kWays; ++r) {
+                        const uint32_t a = s_cl[r][lane];
+                        if (r < q) ol += a;
+                        nl += a;
                     }
                 }
-                longest = max(longest, nl);
-                if (nl > half_cap) { overflow = true; nl = half_cap; }
-                l.nlower[part * n + kslot] = nl;
-            }
-        } else {
-            // slow path: ascending original index by repeated selection
-            if (tid == 0) atomicOr(&sc->status, kStatusSlowUnion);
-            for (uint32_t kslot = cu.cs + tid; kslot < cu.cs + cu.ncenter; kslot += blockDim.x) {
-                uint8_t mfl;
-                uint32_t myo;
-                const float4 me = stage_entry<DIM>(s, kslot, cu, &mfl, &myo);
-                const bool fluid = !(mfl & kFlagBoundary);
-                uint32_t nl = 0;
-                long long last = -1;
-                for (;;) {
-                    unsigned long long best = ULLONG_MAX;
-                    uint32_t best_slot = 0;
-                    for (int q = 0; q < NC; ++q) {
-                        const uint32_t q0 = s_cstart[q], q1 = q0 + (s_off[q + 1] - s_off[q]);
-                        for (uint32_t slot = q0; slot < q1; ++slot) {
-                            if (s.flags[slot] & kFlagBoundary) continue;
-                            const uint32_t o = s.orig[slot];
-                            if ((long long)o <= last || (fluid && o >= myo) ||
-                                (unsigned long long)o >= best)
-                                continue;
-                            uint8_t fl;
-                            uint32_t oo;
-                            if (within(stage_entry<DIM>(s, slot, cu, &fl, &oo), me, r2f)) {
-                                best = o;
-                                best_slot = slot;
+                const ChunkBlock blk = reserve_chunk(l, sc, nc, nl, 0u, s_red, &s_blk, &s_overflow);
+                // ---- pass 2: descriptor and entries
+                if (active) {
+                    const uint32_t kslot = cu.cs + c0 + lane;
+                    const uint32_t gl = (uint32_t)blk.base + lane;
+                    if (q == 0) l.ldesc[kslot] = blk.ok ? make_uint2(gl, nl | (nc << 16)) : make_uint2(0u, 0u);
+                    if (blk.ok) {
+                        const size_t step = 4u * nc;
+                        uint32_t* pl = l.pool + 4 * (size_t)gl;
+                        uint32_t tl = ol;
+                        for (uint32_t w = wb; w < we; ++w) {
+                            uint32_t m = s_mask[w * kChunk + lane];
+                            while (m) {
+                                const uint32_t i = (w << 5) + (__ffs(m) - 1);
+                                m &= m - 1u;
+                                pl[(tl >> 2) * step + (tl & 3u)] = s_ent[s_sorted[i]];
+                                ++tl;
                             }
                         }
                     }
-                    if (best == ULLONG_MAX) break;
-                    if (nl < half_cap) emit(l.lower, kslot, nl, l.capl, best_slot);
-                    ++nl;
-                    last = (long long)best;
                 }
-                longest = max(longest, nl);
-                if (nl > half_cap) { overflow = true; nl = half_cap; }
-                l.nlower[kslot] = nl;
-                l.nlower[n + kslot] = 0;
+                __syncthreads();  // masks and counts are reused by the next chunk
+            }
+        } else {
+            // Slow path: ascending original index by repeated selection, one
+            // thread per centre particle: count, reserve, write.
+            if (tid == 0) atomicOr(&sc->status, kStatusSlowUnion);
+            for (uint32_t c0 = 0; c0 < cu.ncenter; c0 += kNlThreads) {
+                const uint32_t nc = min((uint32_t)kNlThreads, cu.ncenter - c0);
+                const bool active = tid < nc;
+                const uint32_t kslot = cu.cs + c0 + tid;
+                uint8_t mfl = 0;
+                uint32_t myo = 0;
+                float4 me = make_float4(0.f, 0.f, 0.f, 0.f);
+                bool fluidc = false;
+                uint32_t nl = 0;
+                if (active) {
+                    me = stage_entry<DIM>(s, kslot, cu, &mfl, &myo);
+                    fluidc = !(mfl & kFlagBoundary);
+                    for (int c = 0; c < NC; ++c) {
+                        const uint32_t q0 = s_cstart[c], q1 = q0 + (s_off[c + 1] - s_off[c]);
+                        for (uint32_t slot = q0; slot < q1; ++slot) {
+                            uint8_t fl;
+                            uint32_t o;
+                            const float4 qp = stage_entry<DIM>(s, slot, cu, &fl, &o);
+                            if ((fl & kFlagBoundary) || (fluidc && o >= myo)) continue;
+                            if (within(qp, me, r2f)) ++nl;
+                        }
+                    }
+                }
+                const ChunkBlock blk = reserve_chunk(l, sc, nc, nl, 0u, s_red, &s_blk, &s_overflow);
+                if (active) {
+                    const uint32_t gl = (uint32_t)blk.base + tid;
+                    l.ldesc[kslot] = blk.ok ? make_uint2(gl, nl | (nc << 16)) : make_uint2(0u, 0u);
+                    if (blk.ok) {
+                        const size_t step = 4u * nc;
+                        uint32_t* pl = l.pool + 4 * (size_t)gl;
+                        uint32_t tl = 0;
+                        long long last = -1;
+                        while (tl < nl) {
+                            unsigned long long best = ULLONG_MAX;
+                            uint32_t best_slot = 0;
+                            for (int c = 0; c < NC; ++c) {
+                                const uint32_t q0 = s_cstart[c], q1 = q0 + (s_off[c + 1] - s_off[c]);
+                                for (uint32_t slot = q0; slot < q1; ++slot) {
+                                    if (s.flags[slot] & kFlagBoundary) continue;
+                                    const uint32_t o = s.orig[slot];
+                                    if ((long long)o <= last || (fluidc && o >= myo) ||
+                                        (unsigned long long)o >= best)
+                                        continue;
+                                    uint8_t fl;
+                                    uint32_t oo;
+                                    if (within(stage_entry<DIM>(s, slot, cu, &fl, &oo), me, r2f)) {
+                                        best = o;
+                                        best_slot = slot;
+                                    }
+                                }
+                            }
+                            if (best == ULLONG_MAX) break;
+                            pl[(tl >> 2) * step + (tl & 3u)] = best_slot;
+                            ++tl;
+                            last = (long long)best;
+                        }
+                    }
+                }
+                __syncthreads();
             }
         }
-        __syncthreads();
+        __syncthreads();  // shared memory is reused by the next cell
     }
-    if (overflow) atomicOr(&sc->status, kStatusListOverflow);
-    if (longest) atomicMax(&sc->max_part, longest);
+    if (tid == 0 && s_overflow) atomicOr(&sc->status, kStatusListOverflow);
 }
 
-size_t visit_smem_bytes(uint32_t ucap) { return (size_t)ucap * (sizeof(float4) + sizeof(uint32_t)); }
+size_t visit_smem_bytes(uint32_t ucap) {
+    return (size_t)ucap * (sizeof(float4) + sizeof(uint32_t)) + (size_t)(ucap / 32) * kChunk * sizeof(uint32_t);
+}
+
+size_t lower_smem_bytes(uint32_t ucap) {
+    const size_t sort = (size_t)ucap * sizeof(uint16_t) + 16 * kNlThreads * sizeof(uint16_t);
+    const size_t mask = (size_t)(ucap / 32) * kChunk * sizeof(uint32_t);
+    return (size_t)ucap * (sizeof(float4) + sizeof(uint32_t) + sizeof(uint16_t)) + (sort > mask ? sort : mask);
+}
 
 }  // namespace
 
 uint32_t nlist_union_capacity(uint32_t max_union) {
-    // The smallest power of two that holds the largest union seen, within the
-    // shared-memory limit; larger unions take the slow path.
-    uint32_t cap = 256;
-    while (cap < max_union && cap < kMaxUnionStage) cap <<= 1;
-    return cap;
+    // The largest union seen plus a quarter, in steps of kStageStep, within
+    // the shared-memory limit; larger unions take the slow path.
+    uint64_t want = (uint64_t)max_union + max_union / 4u;
+    want = (want + kStageStep - 1) / kStageStep * kStageStep;
+    if (want < kStageStep) want = kStageStep;
+    if (want > kMaxUnionStage) want = kMaxUnionStage;
+    return (uint32_t)want;
 }
 
 size_t nlist_smem_bytes(uint32_t ucap) {
-    // the lower kernel's layout, the larger of the two
-    return (size_t)ucap * (sizeof(float4) + sizeof(uint32_t) + 2 * sizeof(uint16_t)) +
-           16 * kNlThreads * sizeof(uint16_t);
+    const size_t a = visit_smem_bytes(ucap), b = lower_smem_bytes(ucap);
+    return a > b ? a : b;
 }
 
 uint32_t nlist_prepare(int dim, uint32_t ucap) {
-    const size_t sl = nlist_smem_bytes(ucap), sv = visit_smem_bytes(ucap);
-    int bl = 0, bv = 0;
+    const int sv = (int)visit_smem_bytes(ucap), sl = (int)lower_smem_bytes(ucap);
+    int bv = 0, bl = 0;
     if (dim == 3) {
-        cudaFuncSetAttribute(k_nlist_lower<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sl);
-        cudaFuncSetAttribute(k_nlist_visit<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sv);
+        cudaFuncSetAttribute(k_nlist_visit<3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sv);
+        cudaFuncSetAttribute(k_nlist_visit<3, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sv);
+        cudaFuncSetAttribute(k_nlist_lower<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, sl);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bv, k_nlist_visit<3, true>, kNlThreads, sv);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bl, k_nlist_lower<3>, kNlThreads, sl);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bv, k_nlist_visit<3>, kNlThreads, sv);
     } else {
-        cudaFuncSetAttribute(k_nlist_lower<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sl);
-        cudaFuncSetAttribute(k_nlist_visit<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sv);
+        cudaFuncSetAttribute(k_nlist_visit<2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sv);
+        cudaFuncSetAttribute(k_nlist_visit<2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sv);
+        cudaFuncSetAttribute(k_nlist_lower<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sl);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bv, k_nlist_visit<2, true>, kNlThreads, sv);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bl, k_nlist_lower<2>, kNlThreads, sl);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bv, k_nlist_visit<2>, kNlThreads, sv);
     }
-    const int b = bl > bv ? bl : bv;
+    const int b = bv > bl ? bv : bl;
     return b > 0 ? (uint32_t)b : 1u;
 }
 
 void launch_nlist(const GridDesc& g, const StepConst& k, uint32_t ucap, uint32_t nblocks,
                   const uint32_t* occ, const uint32_t* cell_start, const StateBufs& s,
                   const ListBufs& l, DeviceScalars* sc, cudaStream_t st, bool visit_only) {
-    const size_t sl = nlist_smem_bytes(ucap), sv = visit_smem_bytes(ucap);
+    const size_t sv = visit_smem_bytes(ucap), sl = lower_smem_bytes(ucap);
     if (g.dim == 3) {
-        k_nlist_visit<3><<<nblocks, kNlThreads, sv, st>>>(g, k, ucap, occ, cell_start, s, l, sc);
-        if (!visit_only)
+        if (visit_only) {
+            k_nlist_visit<3, false><<<nblocks, kNlThreads, sv, st>>>(g, k, ucap, occ, cell_start, s, l, sc);
+        } else {
+            k_nlist_visit<3, true><<<nblocks, kNlThreads, sv, st>>>(g, k, ucap, occ, cell_start, s, l, sc);
             k_nlist_lower<3><<<nblocks, kNlThreads, sl, st>>>(g, k, ucap, occ, cell_start, s, l, sc);
+        }
     } else {
-        k_nlist_visit<2><<<nblocks, kNlThreads, sv, st>>>(g, k, ucap, occ, cell_start, s, l, sc);
-        if (!visit_only)
+        if (visit_only) {
+            k_nlist_visit<2, false><<<nblocks, kNlThreads, sv, st>>>(g, k, ucap, occ, cell_start, s, l, sc);
+        } else {
+            k_nlist_visit<2, true><<<nblocks, kNlThreads, sv, st>>>(g, k, ucap, occ, cell_start, s, l, sc);
             k_nlist_lower<2><<<nblocks, kNlThreads, sl, st>>>(g, k, ucap, occ, cell_start, s, l, sc);
+        }
     }
 }
 

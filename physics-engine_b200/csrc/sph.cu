@@ -33,23 +33,13 @@ constexpr int kThreads = 128;
 
 inline uint32_t blocks_for(uint64_t n, uint32_t t) { return (uint32_t)((n + t - 1) / t); }
 
-// Calls f(entry) over the whole list of slot s — part 0 then part 1 — as one
-// loop over the concatenation (entry t of the list is physical entry t for
-// t < n0, else cap/2 + t - n0), with the loads of the next two entries issued
-// before the current one is processed.
+// Calls f(entry) over a slot's list in order, with the loads of the next two
+// entries issued before the current one is processed.
 template <class F>
-__device__ __forceinline__ void for_each_entry(const uint32_t* __restrict__ list,
-                                               const uint32_t* __restrict__ count, uint32_t nslots,
-                                               uint32_t s, uint32_t cap, F&& f) {
-    const uint32_t n0 = count[s];
-    const uint32_t n = n0 + count[(size_t)nslots + s];
+__device__ __forceinline__ void for_each_entry(const ListRef r, F&& f) {
+    const uint32_t n = r.n;
     if (n == 0) return;
-    const uint32_t skip = (cap >> 1) - n0;
-    const size_t block = (size_t)(s >> 5) * cap * 32u + (s & 31u) * 4u;
-    auto at = [&](uint32_t t) {
-        const uint32_t p = t < n0 ? t : t + skip;
-        return __ldg(list + block + (size_t)(p & ~3u) * 32u + (p & 3u));
-    };
+    auto at = [&](uint32_t t) { return __ldg(r.p + (size_t)(t >> 2) * r.step + (t & 3u)); };
     uint32_t e0 = at(0), e1 = n > 1 ? at(1) : 0u;
     for (uint32_t t = 0; t < n; ++t) {
         const uint32_t e = e0;
@@ -69,7 +59,7 @@ __global__ void __launch_bounds__(kThreads) k_density(uint32_t n, StepConst k, S
     }
     const double4 xi = s.pos[i];
     double rho = k.rho_self;  // 0.0 + mass * W(0)
-    for_each_entry(l.visit, l.nvisit, l.nslots, i, l.capv, [&](uint32_t e) {
+    for_each_entry(list_ref(l, i, kListVisit), [&](uint32_t e) {
         const uint32_t j = e & kEntrySlotMask;
         const double4 xj = s.pos[j];
         const double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
@@ -195,11 +185,11 @@ __global__ void __launch_bounds__(kThreads) k_forces(uint32_t n, StepConst kc, S
     const double4 vk = s.vel[k];
     double ax = 0.0, ay = 0.0, az = 0.0;
     // fluid i < k, ascending original index
-    for_each_entry(l.lower, l.nlower, l.nslots, k, l.capl, [&](uint32_t j) {
+    for_each_entry(list_ref(l, k, kListLower), [&](uint32_t j) {
         fluid_pair(kc, nac, xk, vk, s.pos[j], s.vel[j], ax, ay, az);
     });
     // fluid j > k and boundary j, visiting order
-    for_each_entry(l.upper, l.nupper, l.nslots, k, l.capv, [&](uint32_t e) {
+    for_each_entry(list_ref(l, k, kListUpper), [&](uint32_t e) {
         const uint32_t j = e & kEntrySlotMask;
         if (e & kEntryBoundary) {
             boundary_pair(kc, xk, s.pos[j], (e & kEntryOriented) != 0u, s.nout, j, ax, ay, az);
@@ -237,7 +227,7 @@ __global__ void __launch_bounds__(kThreads) k_boundary_force(uint32_t n, StepCon
     const double mpsi = -(kc.rho0 * xb.w);
     const double mneg = -kc.mass;
     double fx = 0.0, fy = 0.0, fz = 0.0;
-    for_each_entry(l.lower, l.nlower, l.nslots, b, l.capl, [&](uint32_t i) {
+    for_each_entry(list_ref(l, b, kListLower), [&](uint32_t i) {
         double4 xi = s.pos[i];
         double rx = xb.x - xi.x, ry = xb.y - xi.y, rz = xb.z - xi.z;
         double r2 = rx * rx + ry * ry + rz * rz;
@@ -266,7 +256,7 @@ __global__ void __launch_bounds__(kThreads) k_xsph(uint32_t n, StepConst kc, Sta
     }
     const double4 xi = s.pos[i];
     double dvx = 0.0, dvy = 0.0, dvz = 0.0;
-    for_each_entry(l.visit, l.nvisit, l.nslots, i, l.capv, [&](uint32_t e) {
+    for_each_entry(list_ref(l, i, kListVisit), [&](uint32_t e) {
         if (e & kEntryBoundary) return;
         const uint32_t j = e & kEntrySlotMask;
         const double4 xj = s.pos[j];
@@ -293,7 +283,7 @@ __global__ void k_in_support(uint32_t n, StepConst kc, StateBufs s, ListBufs l, 
     }
     const double4 xi = s.pos[i];
     uint32_t c = 0;
-    for_each_entry(l.visit, l.nvisit, l.nslots, i, l.capv, [&](uint32_t e) {
+    for_each_entry(list_ref(l, i, kListVisit), [&](uint32_t e) {
         const double4 xj = s.pos[e & kEntrySlotMask];
         const double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
         const double r = sqrt(dx * dx + dy * dy + dz * dz);

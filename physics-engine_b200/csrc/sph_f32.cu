@@ -73,14 +73,8 @@ __device__ __forceinline__ bool sees_fluid_f32(const F32Const& k, const double4&
 
 template <class F>
 __device__ __forceinline__ void for_each_visit(const ListBufs& l, uint32_t s, F&& f) {
-    const uint32_t n0 = l.nvisit[s];
-    const uint32_t n = n0 + l.nvisit[(size_t)l.nslots + s];
-    const uint32_t skip = (l.capv >> 1) - n0;
-    const size_t block = (size_t)(s >> 5) * l.capv * 32u + (s & 31u) * 4u;
-    for (uint32_t t = 0; t < n; ++t) {
-        const uint32_t p = t < n0 ? t : t + skip;
-        f(__ldg(l.visit + block + (size_t)(p & ~3u) * 32u + (p & 3u)));
-    }
+    const ListRef r = list_ref(l, s, kListVisit);
+    for (uint32_t t = 0; t < r.n; ++t) f(__ldg(r.p + (size_t)(t >> 2) * r.step + (t & 3u)));
 }
 
 __global__ void __launch_bounds__(kThreads) k_density_f32(uint32_t n, F32Const k, StateBufs s,

@@ -12,8 +12,8 @@
 //   * a dense cell grid over a fixed key box (ix-major linearisation, so the
 //     linear cell order equals the reference's CellKey order), cell_start,
 //     and the list of occupied cells.
-//   * per-slot neighbour lists (warp-interleaved in groups of four, see
-//     list_index): the "visit" list holds in-support candidates in the
+//   * per-slot neighbour lists in one pool, reserved per chunk of a cell's
+//     slots with exact capacities (see ListBufs): the "visit" list holds in-support candidates in the
 //     reference's visiting order; the "upper" list is the visit list without
 //     the entries flagged lower; the "lower" list holds, for fluid slots, the
 //     fluid neighbours with a lower original index in ascending original-index
@@ -80,34 +80,48 @@ struct StateBufs {
 };
 
 struct ListBufs {
-    uint32_t* visit;
-    uint32_t* upper;
-    uint32_t* lower;
-    uint32_t* nvisit;
-    uint32_t* nupper;
-    uint32_t* nlower;
-    uint32_t* ncand;
-    uint32_t capv, capl;  // capacities, multiples of 8 (upper uses capv)
-    uint32_t nslots;      // count arrays hold part 0 at [s], part 1 at [nslots + s]
+    uint32_t* pool;                   // list entries, allocated in 16-byte groups
+    uint4* desc;                      // per slot: visit and upper lists, see list_ref
+    uint2* ldesc;                     // per slot: lower list, see list_ref
+    uint32_t* ncand;                  // candidates examined per slot (fluid: union size)
+    unsigned long long pool_groups;   // capacity of pool in 16-byte groups (< 2^32)
+    uint32_t nslots;
 };
 
-// List storage: each list of a slot has two parts, entries [0, cap/2) and
-// [cap/2, cap), written independently by the two threads that build it; the
-// list is part 0 followed by part 1. The 32 slots of a warp share a block of
-// cap * 32 entries; each
-// slot's entries t..t+3 (t a multiple of 4) are 16 contiguous bytes, and the
-// 32 slots' groups are contiguous, so one uint4 load per lane fetches four
-// entries of 32 consecutive slots in one 512-byte transaction.
-__host__ __device__ __forceinline__ size_t list_index(uint32_t s, uint32_t t, uint32_t cap) {
-    return ((size_t)(s >> 5) * cap + (t & ~3u)) * 32u + (s & 31u) * 4u + (t & 3u);
-}
+// List storage. The list build reserves, for each chunk of consecutive slots
+// of one cell, a block of rows of `stride` 16-byte groups, where stride is the
+// chunk's slot count and the number of rows covers the chunk's longest list
+// (rounded up to 4 entries). Entries t..t+3 of a slot's list are one group,
+// and the chunk's slots' groups of a row are contiguous, so the lanes of a
+// warp reading entry t of consecutive slots read consecutive 16-byte groups.
+//   desc[s]  = (group of row 0 of the visit list (chunk base + lane),
+//               stride | first row of the upper list << 16,
+//               visit count | upper count << 16, 0)
+//   ldesc[s] = (group of row 0 of the lower list, lower count | stride << 16)
+enum ListKind : int { kListVisit = 0, kListUpper = 1, kListLower = 2 };
 
-// Group g (entries 4g..4g+3) of slot s as a uint4.
-__device__ __forceinline__ uint4 list_group(const uint32_t* list, uint32_t s, uint32_t g,
-                                            uint32_t cap) {
-    const uint4* p = reinterpret_cast<const uint4*>(list) + ((size_t)(s >> 5) * cap) * 8u +
-                     (size_t)g * 32u + (s & 31u);
-    return __ldg(p);
+struct ListRef {
+    const uint32_t* p;  // entry t at p[(t >> 2) * step + (t & 3)]
+    uint32_t step;      // 4 * stride (u32 units between rows)
+    uint32_t n;
+};
+
+__device__ __forceinline__ ListRef list_ref(const ListBufs& l, uint32_t s, int kind) {
+    ListRef r;
+    if (kind == kListLower) {
+        const uint2 d = __ldg(l.ldesc + s);
+        r.p = l.pool + 4 * (size_t)d.x;
+        r.step = 4 * (d.y >> 16);
+        r.n = d.y & 0xffffu;
+        return r;
+    }
+    const uint4 d = __ldg(l.desc + s);
+    const uint32_t stride = d.y & 0xffffu;
+    const uint32_t row = kind == kListUpper ? d.y >> 16 : 0u;
+    r.p = l.pool + 4 * ((size_t)d.x + (size_t)row * stride);
+    r.step = 4 * stride;
+    r.n = kind == kListUpper ? d.z >> 16 : d.z & 0xffffu;
+    return r;
 }
 
 struct DeviceScalars {
@@ -116,7 +130,8 @@ struct DeviceScalars {
     uint32_t status;
     uint32_t nocc;                  // occupied cells
     uint32_t max_union;             // largest neighbour-cell union seen by the list build
-    uint32_t max_part;              // longest list part (untruncated) of the last build
+    uint32_t pad_;
+    unsigned long long list_used;   // 16-byte groups the last list build asked for
 };
 
 // Single-precision form (sph_f32.cu).

@@ -215,11 +215,12 @@ World::World(const WorldParams& prm, const WorldConfig& cfg, int dim, double res
         occ_ = alloc<uint32_t>(g_.ncell);
         scan_tmp_ = alloc<unsigned char>(scan_temp_bytes(g_.ncell));
         lists_.nslots = (uint32_t)N;
-        const uint32_t want = cfg_.max_neighbours ? cfg_.max_neighbours : 256u;
-        alloc_lists((want + 7u) & ~7u);
-        lists_.nvisit = alloc<uint32_t>(2 * N);
-        lists_.nupper = alloc<uint32_t>(2 * N);
-        lists_.nlower = alloc<uint32_t>(2 * N);
+        // first guess of the list pool: max_neighbours entries per slot (the
+        // first build measures the need and resizes)
+        const uint64_t want = cfg_.max_neighbours ? cfg_.max_neighbours : 256u;
+        alloc_lists((unsigned long long)N * ((want + 3u) / 4u));
+        lists_.desc = alloc<uint4>(N);
+        lists_.ldesc = alloc<uint2>(N);
         lists_.ncand = alloc<uint32_t>(N);
         insup_ = alloc<uint32_t>(N);
         sc_ = alloc<DeviceScalars>(1);
@@ -274,20 +275,18 @@ World::World(const WorldParams& prm, const WorldConfig& cfg, int dim, double res
     }
 }
 
-void World::alloc_lists(uint32_t part_cap) {
+void World::alloc_lists(unsigned long long groups) {
     for (void* p : list_allocs_) cudaFree(p);
     list_allocs_.clear();
-    lists_.visit = lists_.upper = lists_.lower = nullptr;
-    const size_t npad = ((size_t)lists_.nslots + 31) / 32 * 32;
-    const size_t cap = 2 * (size_t)part_cap;  // two parts per slot
-    for (uint32_t** dst : {&lists_.visit, &lists_.upper, &lists_.lower}) {
-        if (f32_ && dst != &lists_.visit) continue;  // the f32 form reads the visit list only
-        void* p = nullptr;
-        check(cudaMalloc(&p, npad * cap * sizeof(uint32_t)), "cudaMalloc lists");
-        list_allocs_.push_back(p);
-        *dst = static_cast<uint32_t*>(p);
-    }
-    lists_.capv = lists_.capl = (uint32_t)cap;
+    lists_.pool = nullptr;
+    lists_.pool_groups = 0;
+    // group indices are 32-bit: at most 2^32 - 1 groups (64 GB) of entries
+    groups = std::min<unsigned long long>(std::max<unsigned long long>(groups, 1024ull), 0xffffffffull);
+    void* p = nullptr;
+    check(cudaMalloc(&p, groups * 16ull), "cudaMalloc lists");
+    list_allocs_.push_back(p);
+    lists_.pool = static_cast<uint32_t*>(p);
+    lists_.pool_groups = groups;
     lists_valid_ = false;
 }
 
@@ -460,52 +459,46 @@ void World::ensure_lists() {
     if (lists_valid_) return;
     if (!grid_built_) {
         // No grid yet: every neighbour query of the reference returns nothing.
-        check(cudaMemsetAsync(lists_.nvisit, 0, sizeof(uint32_t) * 2 * lists_.nslots, st_), "memset");
-        check(cudaMemsetAsync(lists_.nupper, 0, sizeof(uint32_t) * 2 * lists_.nslots, st_), "memset");
-        check(cudaMemsetAsync(lists_.nlower, 0, sizeof(uint32_t) * 2 * lists_.nslots, st_), "memset");
+        check(cudaMemsetAsync(lists_.desc, 0, sizeof(uint4) * lists_.nslots, st_), "memset");
+        check(cudaMemsetAsync(lists_.ldesc, 0, sizeof(uint2) * lists_.nslots, st_), "memset");
         check(cudaMemsetAsync(lists_.ncand, 0, sizeof(uint32_t) * lists_.nslots, st_), "memset");
     } else {
         for (int attempt = 0; attempt < 4; ++attempt) {
-            if (!lists_checked_)
-                check(cudaMemsetAsync(&sc_->max_part, 0, sizeof(uint32_t), st_), "memset");
+            check(cudaMemsetAsync(&sc_->list_used, 0, sizeof(unsigned long long), st_), "memset");
             prof_begin(kLists);
             launch_nlist(g_, kc_, ucap_, nl_blocks_, occ_, cell_start_, cur_, lists_, sc_, st_, f32_);
             prof_end();
-            launches_ += f32_ ? 1 : 2;
+            launches_ += 1;
             check(cudaGetLastError(), "neighbour lists");
             if (lists_checked_) break;
-            // First build for these positions: size the lists from the longest
-            // part before any pass consumes them.
+            // First build for these positions: size the pool from what the
+            // build asked for before any pass consumes the lists.
             DeviceScalars hs{};
             check(cudaMemcpyAsync(&hs, sc_, sizeof(hs), cudaMemcpyDeviceToHost, st_), "lists");
             check(cudaStreamSynchronize(st_), "lists");
-            const uint32_t part_cap = lists_.capv / 2;
-            const bool overflowed = hs.max_part > part_cap;
-            // The very first sizing wants twice the longest part; later checks
-            // (after the host moved particles) only the 75% rule that runs
-            // poll, so a slowly compressing tank does not reallocate its lists
-            // on every set_positions.
-            const bool fits = lists_sized_ ? (uint64_t)hs.max_part * 4 <= (uint64_t)part_cap * 3
-                                           : (uint64_t)hs.max_part * 2 <= (uint64_t)part_cap;
+            const unsigned long long need = hs.list_used, have = lists_.pool_groups;
+            const bool overflowed = need > have || (hs.status & kStatusListOverflow);
+            // The very first sizing keeps twice the need (lists grow by ~40%
+            // in a few steps when a free-surface start collapses); later
+            // checks (after the host moved particles) use the 75% rule that
+            // runs poll, so a slowly compressing tank does not reallocate on
+            // every set_positions.
+            const bool fits = lists_sized_ ? need * 4 <= have * 3 : need * 2 <= have;
             if (!overflowed && fits) {
                 lists_checked_ = true;
                 lists_sized_ = true;
                 break;
             }
-            // Keep twice the longest part: lists grow as the fluid compresses
-            // (by 40% in a few steps when a free-surface start collapses), and
-            // the densest part of a list can hold nearly all of its entries (a
-            // particle's lower neighbours sit just below its own index in the
-            // sorted union). Runs poll the length and grow further.
-            uint32_t grow = (2 * hs.max_part + 31u) & ~31u;
-            alloc_lists(grow);
-            if (!overflowed) {
-                lists_valid_ = false;
-                continue;  // rebuild into the larger lists
+            if (overflowed && have >= 0xffffffffull)
+                throw std::length_error("neighbour lists exceed the 64 GB pool limit");
+            alloc_lists(2 * need);
+            if (overflowed) {
+                // this build is discarded: clear its status bit
+                const uint32_t keep = hs.status & ~kStatusListOverflow;
+                check(cudaMemcpyAsync(&sc_->status, &keep, sizeof(uint32_t), cudaMemcpyHostToDevice, st_),
+                      "status");
             }
-            // this build overflowed and is discarded: clear its status bit
-            uint32_t keep = hs.status & ~kStatusListOverflow;
-            check(cudaMemcpyAsync(&sc_->status, &keep, sizeof(uint32_t), cudaMemcpyHostToDevice, st_), "status");
+            // rebuild into the new pool
         }
     }
     check(cudaGetLastError(), "neighbour lists");
@@ -640,9 +633,8 @@ uint32_t World::status() {
     check(cudaStreamSynchronize(st_), "status");
     // Grow the list storage ahead of need: the next list build uses the larger
     // capacity (the current lists are complete as long as no overflow bit is set).
-    if ((uint64_t)hs.max_part * 4 > (uint64_t)(lists_.capv / 2) * 3) {
-        alloc_lists((2 * hs.max_part + 31u) & ~31u);
-        check(cudaMemsetAsync(&sc_->max_part, 0, sizeof(uint32_t), st_), "memset");
+    if (hs.list_used * 4 > lists_.pool_groups * 3 && lists_.pool_groups < 0xffffffffull) {
+        alloc_lists(2 * hs.list_used);
         lists_checked_ = false;
     }
     // Grow the shared-memory stage of the list build when the fluid has
@@ -663,9 +655,9 @@ void World::capacity_info(uint64_t* out) {
     check(cudaStreamSynchronize(st_), "info");
     out[0] = hs.status;
     out[1] = hs.max_union;
-    out[2] = hs.max_part;
+    out[2] = hs.list_used;
     out[3] = ucap_;
-    out[4] = lists_.capv / 2;
+    out[4] = lists_.pool_groups;
     out[5] = hs.nocc;
     out[6] = g_.ncell;
     out[7] = nl_blocks_;

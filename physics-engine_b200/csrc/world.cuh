@@ -110,7 +110,7 @@ class World {
     void refresh_step_const();
     void refresh_f32();
     void configure_lists();
-    void alloc_lists(uint32_t part_cap);
+    void alloc_lists(unsigned long long groups);
     template <typename T>
     T* alloc(size_t count);
     void gather_orig_vec(const double4* src, double* out);

@@ -560,7 +560,7 @@ class WcsphWorld:
     def capacity_info(self) -> dict:
         out = np.zeros(8, np.uint64)
         _ok(_lib.pe_fluid_wcsph_capacity_info(self._w, _ptr(out)), "capacity_info")
-        keys = ("status", "max_union", "max_part", "union_capacity", "part_capacity",
+        keys = ("status", "max_union", "list_groups_used", "union_capacity", "list_groups_capacity",
                 "occupied_cells", "dense_cells", "list_ctas")
         return {k: int(v) for k, v in zip(keys, out)}
 
