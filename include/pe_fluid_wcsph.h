@@ -91,6 +91,9 @@ typedef struct PeWcsphConfig {
     uint32_t domain_margin_cells; /* minimum growth per side in cells (0 = 4) */
     int32_t precision;            /* PE_PRECISION_F64 (default, the reference's bits) or
                                      PE_PRECISION_F32 (single-precision form) */
+    int32_t use_graph;            /* nonzero: pe_fluid_wcsph_run replays a captured CUDA
+                                     graph of six steps once the step is steady (no
+                                     host synchronisation inside); same results */
 } PeWcsphConfig;
 
 #define PE_PRECISION_F64 0
@@ -142,6 +145,10 @@ int pe_fluid_recomputed_akinci_psi(PeParticles* p, int32_t kernel);
  * in 3-D), each U(-amplitude, amplitude), added to the position. */
 int pe_fluid_particles_jitter_fluid(PeParticles* p, uint64_t seed, double amplitude);
 /* Copy out SoA arrays (any pointer may be NULL); n must equal the length. */
+/* count draws lo + (hi - lo) * u, u = (next >> 11) * 2^-53, in sequence from the
+ * project's Xoshiro256** seeded with seed (the generator of the jitter,
+ * rng.rs:14-72); used to draw seeded scene parameters. */
+int pe_fluid_rng_uniform(uint64_t seed, double lo, double hi, uint64_t count, double* out);
 int pe_fluid_particles_export(const PeParticles* p, double* x, double* v, uint8_t* kind, double* psi,
                               double* n_out, uint64_t n);
 /* mass_from_spacing (particles.rs:166), mass_calibrated_to_rest (particles.rs:178). */
@@ -163,7 +170,29 @@ int pe_fluid_wcsph_create_from_arrays(const PeWcsphParams* params, int32_t dim, 
                                       double mass, double h, uint64_t n, const double* x,
                                       const double* v, const uint8_t* kind, const double* psi,
                                       const double* n_out, const PeWcsphConfig* cfg, PeWcsph** out);
+/* Batched form (no reference counterpart; replaces a loop of WcsphWorld::step
+ * over independent tanks): n_tanks tanks with the same material and physics,
+ * particles stored tank-major, tank t owning particles [tank_offsets[t],
+ * tank_offsets[t + 1]) (tank_offsets has n_tanks + 1 entries, 0 ... n, no tank
+ * empty). Every tank keeps its own grid domain and persisted sound speed and
+ * evolves exactly as a world created from its particles alone; one step call
+ * advances all tanks. n_tanks = 1 with tank_offsets NULL is
+ * pe_fluid_wcsph_create_from_arrays. */
+int pe_fluid_wcsph_create_batch(const PeWcsphParams* params, int32_t dim, double rest_density,
+                                double mass, double h, uint64_t n, const double* x, const double* v,
+                                const uint8_t* kind, const double* psi, const double* n_out,
+                                uint32_t n_tanks, const uint64_t* tank_offsets,
+                                const PeWcsphConfig* cfg, PeWcsph** out);
 void pe_fluid_wcsph_destroy(PeWcsph* w);
+int pe_fluid_wcsph_tanks(PeWcsph* w, uint32_t* n_tanks);
+/* The persisted sound speed of every tank (n_tanks must equal the world's). */
+int pe_fluid_wcsph_get_sound_speeds(PeWcsph* w, double* out, uint32_t n_tanks);
+/* Launch-shape autotuner (no reference counterpart): times the candidate block
+ * sizes of the density, force and XSPH passes (64, 128, 256) and list-build CTAs
+ * per SM on the current state without advancing it, and keeps the fastest.
+ * out (may be NULL) = {density, forces, xsph block sizes, list CTAs per SM}. */
+int pe_fluid_wcsph_autotune(PeWcsph* w, uint32_t out[4]);
+int pe_fluid_wcsph_shapes(PeWcsph* w, uint32_t out[4]);
 
 /* WcsphWorld::step (wcsph.rs:326). Synchronous; returns PE_ERR_BOUNDS if the
  * step raised PE_STATUS_DOMAIN or PE_STATUS_NEIGHBOUR_OVERFLOW. */

@@ -151,6 +151,7 @@ pe::WorldConfig to_config(const PeWcsphConfig* c) {
     w.domain_margin = c ? c->domain_margin : -1.0;
     w.domain_margin_cells = c ? c->domain_margin_cells : 0;
     w.precision = c ? c->precision : 0;
+    w.use_graph = c ? c->use_graph : 0;
     if (!c) w.domain_margin = -1.0;
     return w;
 }
@@ -375,6 +376,14 @@ int pe_fluid_particles_jitter_fluid(PeParticles* p, uint64_t seed, double amplit
     return PE_OK;
 }
 
+int pe_fluid_rng_uniform(uint64_t seed, double lo, double hi, uint64_t count, double* out) {
+    if (count && !out) return PE_ERR_NULL;
+    if (!(std::isfinite(lo) && std::isfinite(hi))) return PE_ERR_ARG;
+    Xoshiro256ss r(seed);
+    for (uint64_t i = 0; i < count; ++i) out[i] = r.uniform(lo, hi);
+    return PE_OK;
+}
+
 int pe_fluid_particles_export(const PeParticles* p, double* x, double* v, uint8_t* kind, double* psi,
                               double* n_out, uint64_t n) {
     if (!p) return PE_ERR_NULL;
@@ -438,7 +447,25 @@ int pe_fluid_wcsph_create_from_arrays(const PeWcsphParams* params, int32_t dim, 
                                       double mass, double h, uint64_t n, const double* x,
                                       const double* v, const uint8_t* kind, const double* psi,
                                       const double* n_out, const PeWcsphConfig* cfg, PeWcsph** out) {
+    return pe_fluid_wcsph_create_batch(params, dim, rest_density, mass, h, n, x, v, kind, psi, n_out,
+                                       1, nullptr, cfg, out);
+}
+
+int pe_fluid_wcsph_create_batch(const PeWcsphParams* params, int32_t dim, double rest_density,
+                                double mass, double h, uint64_t n, const double* x, const double* v,
+                                const uint8_t* kind, const double* psi, const double* n_out,
+                                uint32_t n_tanks, const uint64_t* tank_offsets,
+                                const PeWcsphConfig* cfg, PeWcsph** out) {
     if (!out) return PE_ERR_NULL;
+    *out = nullptr;
+    if (n_tanks == 0) return PE_ERR_ARG;
+    if (n_tanks > 65535u) return PE_ERR_BOUNDS;
+    if (n_tanks > 1 && !tank_offsets) return PE_ERR_NULL;
+    if (tank_offsets) {
+        if (tank_offsets[0] != 0 || tank_offsets[n_tanks] != n) return PE_ERR_ARG;
+        for (uint32_t t = 0; t < n_tanks; ++t)
+            if (tank_offsets[t + 1] <= tank_offsets[t]) return PE_ERR_ARG;
+    }
     *out = nullptr;
     int rc = check_params(params);
     if (rc != PE_OK) return rc;
@@ -463,7 +490,7 @@ int pe_fluid_wcsph_create_from_arrays(const PeWcsphParams* params, int32_t dim, 
         }
         pe::WorldConfig wc = to_config(cfg);
         auto* w = new pe::World(to_world(*params), wc, dim, rest_density, mass, h, n, x, v, kind, ps,
-                                n_out);
+                                n_out, tank_offsets, n_tanks);
         *out = new PeWcsph{w};
         return PE_OK;
     });
@@ -546,6 +573,45 @@ int pe_fluid_wcsph_get_sound_speed(PeWcsph* w, double* c) {
         *c = w->world->sound_speed();
         return PE_OK;
     });
+}
+
+int pe_fluid_wcsph_tanks(PeWcsph* w, uint32_t* n_tanks) {
+    if (!w || !n_tanks) return PE_ERR_NULL;
+    *n_tanks = w->world->tanks();
+    return PE_OK;
+}
+
+int pe_fluid_wcsph_get_sound_speeds(PeWcsph* w, double* out, uint32_t n_tanks) {
+    if (!w || !out) return PE_ERR_NULL;
+    if (n_tanks != w->world->tanks()) return PE_ERR_BOUNDS;
+    return guard([&] {
+        w->world->get_sound_speeds(out);
+        return PE_OK;
+    });
+}
+
+int pe_fluid_wcsph_autotune(PeWcsph* w, uint32_t out[4]) {
+    if (!w) return PE_ERR_NULL;
+    return guard([&] {
+        const pe::World::Shapes r = w->world->autotune();
+        if (out) {
+            out[0] = r.density;
+            out[1] = r.forces;
+            out[2] = r.xsph;
+            out[3] = r.list_ctas_per_sm;
+        }
+        return status_code(w->world->status());
+    });
+}
+
+int pe_fluid_wcsph_shapes(PeWcsph* w, uint32_t out[4]) {
+    if (!w || !out) return PE_ERR_NULL;
+    const pe::World::Shapes r = w->world->shapes();
+    out[0] = r.density;
+    out[1] = r.forces;
+    out[2] = r.xsph;
+    out[3] = r.list_ctas_per_sm;
+    return PE_OK;
 }
 
 int pe_fluid_wcsph_get_params(PeWcsph* w, PeWcsphParams* out) {

@@ -22,7 +22,7 @@ constexpr uint32_t kScanTile = kScanThreads * kScanItems;
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
 
-__global__ void k_cell_ids(GridDesc g, uint32_t n, const double4* __restrict__ pos_cur,
+__global__ void k_cell_ids(GridDesc g, Tanks tk, uint32_t n, const double4* __restrict__ pos_cur,
                            const double4* __restrict__ pos_next, const uint8_t* __restrict__ flags,
                            uint32_t* __restrict__ cellid, int4* __restrict__ key_tmp,
                            uint32_t* __restrict__ count, DeviceScalars* sc) {
@@ -39,14 +39,27 @@ __global__ void k_cell_ids(GridDesc g, uint32_t n, const double4* __restrict__ p
         if (!isfinite(p.x) || !isfinite(p.y) || (g.dim == 3 && !isfinite(p.z)))
             atomicOr(&sc->status, kStatusNonFinite);
         key_tmp[s] = make_int4(ix, iy, iz, 0);
-        long long dx = (long long)ix - g.kx0, dy = (long long)iy - g.ky0, dz = (long long)iz - g.kz0;
-        if (dx < 0 || dy < 0 || dz < 0 || dx >= g.nx || dy >= g.ny || dz >= g.nz) {
-            atomicOr(&sc->status, kStatusDomain);
-            dx = dx < 0 ? 0 : (dx >= g.nx ? g.nx - 1 : dx);
-            dy = dy < 0 ? 0 : (dy >= g.ny ? g.ny - 1 : dy);
-            dz = dz < 0 ? 0 : (dz >= g.nz ? g.nz - 1 : dz);
+        // the box of this slot's tank (slots keep their tank across re-sorts)
+        TankDesc td;
+        if (tk.desc) {
+            td = tk.desc[tk.slot_tank[s]];
+        } else {
+            td.kx0 = g.kx0;
+            td.ky0 = g.ky0;
+            td.kz0 = g.kz0;
+            td.nx = g.nx;
+            td.ny = g.ny;
+            td.nz = g.nz;
+            td.cell_base = 0;
         }
-        c = (uint32_t)((dx * g.ny + dy) * g.nz + dz);
+        long long dx = (long long)ix - td.kx0, dy = (long long)iy - td.ky0, dz = (long long)iz - td.kz0;
+        if (dx < 0 || dy < 0 || dz < 0 || dx >= td.nx || dy >= td.ny || dz >= td.nz) {
+            atomicOr(&sc->status, kStatusDomain);
+            dx = dx < 0 ? 0 : (dx >= td.nx ? td.nx - 1 : dx);
+            dy = dy < 0 ? 0 : (dy >= td.ny ? td.ny - 1 : dy);
+            dz = dz < 0 ? 0 : (dz >= td.nz ? td.nz - 1 : dz);
+        }
+        c = td.cell_base + (uint32_t)((dx * td.ny + dy) * td.nz + dz);
         cellid[s] = c;
     }
     unsigned mask = __ballot_sync(0xffffffffu, active);
@@ -251,11 +264,11 @@ inline uint32_t blocks_for(uint64_t n, uint32_t t) { return (uint32_t)((n + t - 
 
 }  // namespace
 
-void launch_cell_ids(const GridDesc& g, uint32_t n, const double4* pos_cur, const double4* pos_next,
-                     const uint8_t* flags, uint32_t* cellid, int4* key_tmp, uint32_t* count,
-                     DeviceScalars* sc, cudaStream_t st) {
+void launch_cell_ids(const GridDesc& g, const Tanks& tk, uint32_t n, const double4* pos_cur,
+                     const double4* pos_next, const uint8_t* flags, uint32_t* cellid, int4* key_tmp,
+                     uint32_t* count, DeviceScalars* sc, cudaStream_t st) {
     if (n == 0) return;
-    k_cell_ids<<<blocks_for(n, 256), 256, 0, st>>>(g, n, pos_cur, pos_next, flags, cellid, key_tmp,
+    k_cell_ids<<<blocks_for(n, 256), 256, 0, st>>>(g, tk, n, pos_cur, pos_next, flags, cellid, key_tmp,
                                                   count, sc);
 }
 

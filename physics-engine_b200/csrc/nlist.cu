@@ -98,17 +98,20 @@ struct CellUnion {
     double ox, oy, oz;
 };
 
-// Ranges of the NC neighbour cells of dense cell c, in visiting order.
+// Ranges of the NC neighbour cells of global dense cell c, in visiting order;
+// neighbours are taken inside the box of c's tank.
 template <int DIM>
-__device__ __forceinline__ CellUnion cell_union(const GridDesc& g, uint32_t c,
+__device__ __forceinline__ CellUnion cell_union(const GridDesc& g, const Tanks& tk, uint32_t c,
                                                 const uint32_t* __restrict__ cell_start,
                                                 uint32_t* s_cstart, uint32_t* s_off) {
     constexpr int NC = DIM == 3 ? 27 : 9;
     constexpr int CENTER = DIM == 3 ? 13 : 4;
     const uint32_t tid = threadIdx.x;
-    const int cz = (int)(c % (uint32_t)g.nz);
-    const int cy = (int)((c / (uint32_t)g.nz) % (uint32_t)g.ny);
-    const int cx = (int)(c / ((uint32_t)g.nz * (uint32_t)g.ny));
+    const TankDesc td = tk.desc[tk.cell_tank[c]];
+    const uint32_t lc = c - td.cell_base;
+    const int cz = (int)(lc % (uint32_t)td.nz);
+    const int cy = (int)((lc / (uint32_t)td.nz) % (uint32_t)td.ny);
+    const int cx = (int)(lc / ((uint32_t)td.nz * (uint32_t)td.ny));
     if (tid < 32) {
         uint32_t st = 0, cnt = 0;
         if ((int)tid < NC) {
@@ -116,8 +119,9 @@ __device__ __forceinline__ CellUnion cell_union(const GridDesc& g, uint32_t c,
             int dy = DIM == 3 ? ((int)tid / 3) % 3 - 1 : (int)tid / 3 - 1;
             int dx = (int)tid % 3 - 1;
             int qx = cx + dx, qy = cy + dy, qz = cz + dz;
-            if (qx >= 0 && qy >= 0 && qz >= 0 && qx < g.nx && qy < g.ny && qz < g.nz) {
-                uint32_t nc = ((uint32_t)qx * (uint32_t)g.ny + (uint32_t)qy) * (uint32_t)g.nz + (uint32_t)qz;
+            if (qx >= 0 && qy >= 0 && qz >= 0 && qx < td.nx && qy < td.ny && qz < td.nz) {
+                uint32_t nc = td.cell_base +
+                              ((uint32_t)qx * (uint32_t)td.ny + (uint32_t)qy) * (uint32_t)td.nz + (uint32_t)qz;
                 st = cell_start[nc];
                 cnt = cell_start[nc + 1] - st;
             }
@@ -140,9 +144,9 @@ __device__ __forceinline__ CellUnion cell_union(const GridDesc& g, uint32_t c,
     cu.cs = s_cstart[CENTER];
     cu.ncenter = s_off[CENTER + 1] - s_off[CENTER];
     cu.center_off = s_off[CENTER];
-    cu.ox = (double)(g.kx0 + cx) * g.cell_size;
-    cu.oy = (double)(g.ky0 + cy) * g.cell_size;
-    cu.oz = DIM == 3 ? (double)(g.kz0 + cz) * g.cell_size : 0.0;
+    cu.ox = (double)(td.kx0 + cx) * g.cell_size;
+    cu.oy = (double)(td.ky0 + cy) * g.cell_size;
+    cu.oz = DIM == 3 ? (double)(td.kz0 + cz) * g.cell_size : 0.0;
     return cu;
 }
 
@@ -212,7 +216,7 @@ __device__ __forceinline__ ChunkBlock reserve_chunk(const ListBufs& l, DeviceSca
 // uint32 s_ent[ucap]; uint32 s_mask[(ucap / 32) * kChunk] (word w of chunk
 // lane c at s_mask[w * kChunk + c]).
 template <int DIM, bool UPPER>
-__global__ void __launch_bounds__(kNlThreads) k_nlist_visit(GridDesc g, StepConst k, uint32_t ucap,
+__global__ void __launch_bounds__(kNlThreads) k_nlist_visit(GridDesc g, Tanks tk, StepConst k, uint32_t ucap,
                                                             const uint32_t* __restrict__ occ,
                                                             const uint32_t* __restrict__ cell_start,
                                                             StateBufs s, ListBufs l,
@@ -237,7 +241,7 @@ __global__ void __launch_bounds__(kNlThreads) k_nlist_visit(GridDesc g, StepCons
     if (tid == 0) s_overflow = false;
 
     for (uint32_t it = blockIdx.x; it < nocc; it += gridDim.x) {
-        const CellUnion cu = cell_union<DIM>(g, occ[it], cell_start, s_cstart, s_off);
+        const CellUnion cu = cell_union<DIM>(g, tk, occ[it], cell_start, s_cstart, s_off);
         const uint32_t U = cu.U;
         max_union = max(max_union, U);
         if (U <= ucap) {
@@ -423,7 +427,7 @@ __global__ void __launch_bounds__(kNlThreads) k_nlist_visit(GridDesc g, StepCons
 // (uint16 s_tmp[ucap], uint16 s_cnt[16 * kNlThreads]) and then by the
 // in-support masks over sorted positions (uint32 s_mask[(ucap / 32) * kChunk]).
 template <int DIM>
-__global__ void __launch_bounds__(kNlThreads) k_nlist_lower(GridDesc g, StepConst k, uint32_t ucap,
+__global__ void __launch_bounds__(kNlThreads) k_nlist_lower(GridDesc g, Tanks tk, StepConst k, uint32_t ucap,
                                                             const uint32_t* __restrict__ occ,
                                                             const uint32_t* __restrict__ cell_start,
                                                             StateBufs s, ListBufs l,
@@ -456,7 +460,7 @@ __global__ void __launch_bounds__(kNlThreads) k_nlist_lower(GridDesc g, StepCons
             s_omin = 0xffffffffu;
             s_omax = 0u;
         }
-        const CellUnion cu = cell_union<DIM>(g, occ[it], cell_start, s_cstart, s_off);
+        const CellUnion cu = cell_union<DIM>(g, tk, occ[it], cell_start, s_cstart, s_off);
         const uint32_t U = cu.U;
         if (U <= ucap) {
             for (uint32_t u = tid; u < U; u += blockDim.x) {
@@ -714,23 +718,24 @@ uint32_t nlist_prepare(int dim, uint32_t ucap) {
     return b > 0 ? (uint32_t)b : 1u;
 }
 
-void launch_nlist(const GridDesc& g, const StepConst& k, uint32_t ucap, uint32_t nblocks,
-                  const uint32_t* occ, const uint32_t* cell_start, const StateBufs& s,
-                  const ListBufs& l, DeviceScalars* sc, cudaStream_t st, bool visit_only) {
+void launch_nlist(const GridDesc& g, const Tanks& tk, const StepConst& k, uint32_t ucap,
+                  uint32_t nblocks, const uint32_t* occ, const uint32_t* cell_start,
+                  const StateBufs& s, const ListBufs& l, DeviceScalars* sc, cudaStream_t st,
+                  bool visit_only) {
     const size_t sv = visit_smem_bytes(ucap), sl = lower_smem_bytes(ucap);
     if (g.dim == 3) {
         if (visit_only) {
-            k_nlist_visit<3, false><<<nblocks, kNlThreads, sv, st>>>(g, k, ucap, occ, cell_start, s, l, sc);
+            k_nlist_visit<3, false><<<nblocks, kNlThreads, sv, st>>>(g, tk, k, ucap, occ, cell_start, s, l, sc);
         } else {
-            k_nlist_visit<3, true><<<nblocks, kNlThreads, sv, st>>>(g, k, ucap, occ, cell_start, s, l, sc);
-            k_nlist_lower<3><<<nblocks, kNlThreads, sl, st>>>(g, k, ucap, occ, cell_start, s, l, sc);
+            k_nlist_visit<3, true><<<nblocks, kNlThreads, sv, st>>>(g, tk, k, ucap, occ, cell_start, s, l, sc);
+            k_nlist_lower<3><<<nblocks, kNlThreads, sl, st>>>(g, tk, k, ucap, occ, cell_start, s, l, sc);
         }
     } else {
         if (visit_only) {
-            k_nlist_visit<2, false><<<nblocks, kNlThreads, sv, st>>>(g, k, ucap, occ, cell_start, s, l, sc);
+            k_nlist_visit<2, false><<<nblocks, kNlThreads, sv, st>>>(g, tk, k, ucap, occ, cell_start, s, l, sc);
         } else {
-            k_nlist_visit<2, true><<<nblocks, kNlThreads, sv, st>>>(g, k, ucap, occ, cell_start, s, l, sc);
-            k_nlist_lower<2><<<nblocks, kNlThreads, sl, st>>>(g, k, ucap, occ, cell_start, s, l, sc);
+            k_nlist_visit<2, true><<<nblocks, kNlThreads, sv, st>>>(g, tk, k, ucap, occ, cell_start, s, l, sc);
+            k_nlist_lower<2><<<nblocks, kNlThreads, sl, st>>>(g, tk, k, ucap, occ, cell_start, s, l, sc);
         }
     }
 }

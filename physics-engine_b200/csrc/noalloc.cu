@@ -255,7 +255,7 @@ extern "C" int pe_fluid_density_noalloc(int32_t dim, double rest_density, double
     if (cudaMemsetAsync(count, 0, sizeof(uint32_t) * g.ncell, st) != cudaSuccess ||
         cudaMemsetAsync(fill, 0, sizeof(uint32_t) * g.ncell, st) != cudaSuccess)
         return PE_ERR_DEVICE;
-    launch_cell_ids(g, nn, reinterpret_cast<const double4*>(scratch + kOffPos), nullptr,
+    launch_cell_ids(g, Tanks{}, nn, reinterpret_cast<const double4*>(scratch + kOffPos), nullptr,
                     scratch + kOffFlags, cellid, key, count, sc, st);
     launch_scan_cells(g.ncell, count, start, occ, sc, scratch + kOffScan, st);
     launch_place(nn, cellid, start, fill, reinterpret_cast<const uint32_t*>(scratch + kOffOrig),

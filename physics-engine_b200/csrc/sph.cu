@@ -49,7 +49,7 @@ __device__ __forceinline__ void for_each_entry(const ListRef r, F&& f) {
     }
 }
 
-__global__ void __launch_bounds__(kThreads) k_density(uint32_t n, StepConst k, StateBufs s,
+__global__ void __launch_bounds__(kMaxPassThreads) k_density(uint32_t n, StepConst k, StateBufs s,
                                                       ListBufs l) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -77,38 +77,52 @@ __global__ void __launch_bounds__(kThreads) k_density(uint32_t n, StepConst k, S
     s.pos[i].w = s.p[i] / (rho * rho);
 }
 
-__global__ void k_vmax(uint32_t n, StateBufs s, DeviceScalars* sc) {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+// max |v|^2 of each tank's fluid (viscosity.rs:89-100), as u64 bits: a warp
+// whose lanes all belong to one tank reduces first, a warp across a tank
+// boundary lets each lane add its own value.
+__global__ void k_vmax(uint32_t n, Tanks tk, StateBufs s) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     double m = 0.0;
-    if (i < n && !(s.flags[i] & kFlagBoundary)) {
-        double4 v = s.vel[i];
-        double q = v.x * v.x + v.y * v.y + v.z * v.z;
-        if (q > m) m = q;  // viscosity.rs:91-96 (NaN never exceeds m)
+    uint32_t t = 0xffffffffu;
+    if (i < n) {
+        t = tk.slot_tank[i];
+        if (!(s.flags[i] & kFlagBoundary)) {
+            double4 v = s.vel[i];
+            double q = v.x * v.x + v.y * v.y + v.z * v.z;
+            if (q > m) m = q;  // viscosity.rs:91-96 (NaN never exceeds m)
+        }
     }
     unsigned long long b = __double_as_longlong(m);
+    const uint32_t t0 = __shfl_sync(0xffffffffu, t, 0);
+    if (i >= n) t = t0;  // idle lanes carry lane 0's tank and a zero
+    if (__all_sync(0xffffffffu, t == t0)) {
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        unsigned long long x = __shfl_xor_sync(0xffffffffu, b, o);
-        b = x > b ? x : b;
+        for (int o = 16; o > 0; o >>= 1) {
+            unsigned long long x = __shfl_xor_sync(0xffffffffu, b, o);
+            b = x > b ? x : b;
+        }
+        // Non-negative doubles order like their bit patterns.
+        if ((threadIdx.x & 31u) == 0 && b != 0ull && t0 != 0xffffffffu) atomicMax(&tk.vmax2[t0], b);
+    } else if (b != 0ull && i < n) {
+        atomicMax(&tk.vmax2[t], b);
     }
-    // Non-negative doubles order like their bit patterns.
-    if ((threadIdx.x & 31u) == 0 && b != 0ull) atomicMax(&sc->vmax2_bits, b);
 }
 
-__global__ void k_pressure(uint32_t n, StepConst k, StateBufs s, DeviceScalars* sc) {
+__global__ void k_pressure(uint32_t n, StepConst k, Tanks tk, StateBufs s) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    // compute_pressure (wcsph.rs:158-169): c = max(c, 10 * v_max), persisted.
-    // Every thread derives the same c; re-reading an already-updated c gives
-    // the same value (the update is idempotent), so the write is race-free in
-    // effect.
-    double c = sc->sound_speed;
+    if (i >= n) return;
+    // compute_pressure (wcsph.rs:158-169): c = max(c, 10 * v_max), persisted
+    // per tank. Every thread of a tank derives the same c; re-reading an
+    // already-updated c gives the same value (the update is idempotent), so
+    // the write by the tank's first slot is race-free in effect.
+    const uint32_t t = tk.slot_tank[i];
+    double c = tk.c[t];
     if (k.adapt_sound_speed) {
-        double vmax = sqrt(__longlong_as_double((long long)sc->vmax2_bits));
+        double vmax = sqrt(__longlong_as_double((long long)tk.vmax2[t]));
         double min_c = 10.0 * fmax(vmax, 0.0);
         c = c < min_c ? min_c : c;
     }
-    if (i == 0) sc->sound_speed = c;
-    if (i >= n) return;
+    if (i == tk.desc[t].slot_begin) tk.c[t] = c;
     if (s.flags[i] & kFlagBoundary) {
         s.p[i] = 0.0;
         return;
@@ -172,14 +186,14 @@ __device__ __forceinline__ void boundary_pair(const StepConst& kc, double4 xk, d
 }
 
 template <bool INTEGRATE, int DIM>
-__global__ void __launch_bounds__(kThreads) k_forces(uint32_t n, StepConst kc, StateBufs s,
-                                                     ListBufs l, const DeviceScalars* sc,
-                                                     double dt, double4* __restrict__ pos_next,
-                                                     double4* __restrict__ vel_next) {
+__global__ void __launch_bounds__(kMaxPassThreads) k_forces(uint32_t n, StepConst kc, Tanks tk,
+                                                            StateBufs s, ListBufs l, double dt,
+                                                            double4* __restrict__ pos_next,
+                                                            double4* __restrict__ vel_next) {
     uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     if (s.flags[k] & kFlagBoundary) return;
-    const double c0 = sc->sound_speed;
+    const double c0 = tk.c[tk.slot_tank[k]];
     const double nac = -kc.visc_alpha * c0;  // (-alpha) * c_bar, viscosity.rs:72
     const double4 xk = s.pos[k];
     const double4 vk = s.vel[k];
@@ -245,7 +259,7 @@ __global__ void __launch_bounds__(kThreads) k_boundary_force(uint32_t n, StepCon
     s.bf[b] = make_double4(fx, fy, fz, 0.0);
 }
 
-__global__ void __launch_bounds__(kThreads) k_xsph(uint32_t n, StepConst kc, StateBufs s,
+__global__ void __launch_bounds__(kMaxPassThreads) k_xsph(uint32_t n, StepConst kc, StateBufs s,
                                                    ListBufs l, double4* __restrict__ vel_out) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -294,31 +308,31 @@ __global__ void k_in_support(uint32_t n, StepConst kc, StateBufs s, ListBufs l, 
 
 }  // namespace
 
-void launch_density(uint32_t n, const StepConst& k, const StateBufs& s, const ListBufs& l,
-                    cudaStream_t st) {
-    if (n) k_density<<<blocks_for(n, kThreads), kThreads, 0, st>>>(n, k, s, l);
+void launch_density(uint32_t n, uint32_t threads, const StepConst& k, const StateBufs& s,
+                    const ListBufs& l, cudaStream_t st) {
+    if (n) k_density<<<blocks_for(n, threads), threads, 0, st>>>(n, k, s, l);
 }
 
-void launch_vmax(uint32_t n, const StateBufs& s, DeviceScalars* sc, cudaStream_t st) {
-    if (n) k_vmax<<<blocks_for(n, 256), 256, 0, st>>>(n, s, sc);
+void launch_vmax(uint32_t n, const Tanks& tk, const StateBufs& s, cudaStream_t st) {
+    if (n) k_vmax<<<blocks_for(n, 256), 256, 0, st>>>(n, tk, s);
 }
 
-void launch_pressure(uint32_t n, const StepConst& k, const StateBufs& s, DeviceScalars* sc,
+void launch_pressure(uint32_t n, const StepConst& k, const Tanks& tk, const StateBufs& s,
                      cudaStream_t st) {
-    k_pressure<<<blocks_for(n ? n : 1, 256), 256, 0, st>>>(n, k, s, sc);
+    if (n) k_pressure<<<blocks_for(n, 256), 256, 0, st>>>(n, k, tk, s);
 }
 
-void launch_forces(uint32_t n, const StepConst& k, const StateBufs& s, const ListBufs& l,
-                   const DeviceScalars* sc, bool integrate, double dt, double4* pos_next,
-                   double4* vel_next, cudaStream_t st) {
+void launch_forces(uint32_t n, uint32_t threads, const StepConst& k, const Tanks& tk,
+                   const StateBufs& s, const ListBufs& l, bool integrate, double dt,
+                   double4* pos_next, double4* vel_next, cudaStream_t st) {
     if (!n) return;
-    uint32_t b = blocks_for(n, kThreads);
+    const uint32_t b = blocks_for(n, threads);
     if (k.dim == 3) {
-        if (integrate) k_forces<true, 3><<<b, kThreads, 0, st>>>(n, k, s, l, sc, dt, pos_next, vel_next);
-        else k_forces<false, 3><<<b, kThreads, 0, st>>>(n, k, s, l, sc, dt, pos_next, vel_next);
+        if (integrate) k_forces<true, 3><<<b, threads, 0, st>>>(n, k, tk, s, l, dt, pos_next, vel_next);
+        else k_forces<false, 3><<<b, threads, 0, st>>>(n, k, tk, s, l, dt, pos_next, vel_next);
     } else {
-        if (integrate) k_forces<true, 2><<<b, kThreads, 0, st>>>(n, k, s, l, sc, dt, pos_next, vel_next);
-        else k_forces<false, 2><<<b, kThreads, 0, st>>>(n, k, s, l, sc, dt, pos_next, vel_next);
+        if (integrate) k_forces<true, 2><<<b, threads, 0, st>>>(n, k, tk, s, l, dt, pos_next, vel_next);
+        else k_forces<false, 2><<<b, threads, 0, st>>>(n, k, tk, s, l, dt, pos_next, vel_next);
     }
 }
 
@@ -327,9 +341,9 @@ void launch_boundary_force(uint32_t n, const StepConst& k, const StateBufs& s, c
     if (n) k_boundary_force<<<blocks_for(n, kThreads), kThreads, 0, st>>>(n, k, s, l);
 }
 
-void launch_xsph(uint32_t n, const StepConst& k, const StateBufs& s, const ListBufs& l,
-                 double4* vel_out, cudaStream_t st) {
-    if (n) k_xsph<<<blocks_for(n, kThreads), kThreads, 0, st>>>(n, k, s, l, vel_out);
+void launch_xsph(uint32_t n, uint32_t threads, const StepConst& k, const StateBufs& s,
+                 const ListBufs& l, double4* vel_out, cudaStream_t st) {
+    if (n) k_xsph<<<blocks_for(n, threads), threads, 0, st>>>(n, k, s, l, vel_out);
 }
 
 void launch_in_support_counts(uint32_t n, const StepConst& k, const StateBufs& s,

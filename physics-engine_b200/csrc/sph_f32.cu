@@ -18,7 +18,6 @@ namespace pe {
 
 namespace {
 
-constexpr int kThreads = 128;
 
 inline uint32_t blocks_for(uint64_t n, uint32_t t) { return (uint32_t)((n + t - 1) / t); }
 
@@ -77,7 +76,7 @@ __device__ __forceinline__ void for_each_visit(const ListBufs& l, uint32_t s, F&
     for (uint32_t t = 0; t < r.n; ++t) f(__ldg(r.p + (size_t)(t >> 2) * r.step + (t & 3u)));
 }
 
-__global__ void __launch_bounds__(kThreads) k_density_f32(uint32_t n, F32Const k, StateBufs s,
+__global__ void __launch_bounds__(kMaxPassThreads) k_density_f32(uint32_t n, F32Const k, StateBufs s,
                                                           F32Bufs f, ListBufs l) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -103,33 +102,45 @@ __global__ void __launch_bounds__(kThreads) k_density_f32(uint32_t n, F32Const k
     s.vel[i].w = (double)r;
 }
 
-__global__ void k_vmax_f32(uint32_t n, StateBufs s, F32Bufs f, DeviceScalars* sc) {
+__global__ void k_vmax_f32(uint32_t n, Tanks tk, StateBufs s, F32Bufs f) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     double m = 0.0;
-    if (i < n && !(s.flags[i] & kFlagBoundary)) {
-        const float4 v = f.vel[i];
-        const double q = (double)v.x * v.x + (double)v.y * v.y + (double)v.z * v.z;
-        if (q > m) m = q;
+    uint32_t t = 0xffffffffu;
+    if (i < n) {
+        t = tk.slot_tank[i];
+        if (!(s.flags[i] & kFlagBoundary)) {
+            const float4 v = f.vel[i];
+            const double q = (double)v.x * v.x + (double)v.y * v.y + (double)v.z * v.z;
+            if (q > m) m = q;
+        }
     }
     unsigned long long b = __double_as_longlong(m);
+    const uint32_t t0 = __shfl_sync(0xffffffffu, t, 0);
+    if (i >= n) t = t0;
+    if (__all_sync(0xffffffffu, t == t0)) {
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        const unsigned long long x = __shfl_xor_sync(0xffffffffu, b, o);
-        b = x > b ? x : b;
+        for (int o = 16; o > 0; o >>= 1) {
+            const unsigned long long x = __shfl_xor_sync(0xffffffffu, b, o);
+            b = x > b ? x : b;
+        }
+        if ((threadIdx.x & 31u) == 0 && b != 0ull && t0 != 0xffffffffu) atomicMax(&tk.vmax2[t0], b);
+    } else if (b != 0ull && i < n) {
+        atomicMax(&tk.vmax2[t], b);
     }
-    if ((threadIdx.x & 31u) == 0 && b != 0ull) atomicMax(&sc->vmax2_bits, b);
 }
 
-__global__ void k_pressure_f32(uint32_t n, F32Const k, StateBufs s, F32Bufs f, DeviceScalars* sc) {
+__global__ void k_pressure_f32(uint32_t n, F32Const k, Tanks tk, StateBufs s, F32Bufs f) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    double c = sc->sound_speed;  // f64 control of the sound speed (wcsph.rs:158-169)
+    if (i >= n) return;
+    // f64 control of each tank's sound speed (wcsph.rs:158-169)
+    const uint32_t t = tk.slot_tank[i];
+    double c = tk.c[t];
     if (k.adapt_sound_speed) {
-        const double vmax = sqrt(__longlong_as_double((long long)sc->vmax2_bits));
+        const double vmax = sqrt(__longlong_as_double((long long)tk.vmax2[t]));
         const double min_c = 10.0 * fmax(vmax, 0.0);
         c = c < min_c ? min_c : c;
     }
-    if (i == 0) sc->sound_speed = c;
-    if (i >= n) return;
+    if (i == tk.desc[t].slot_begin) tk.c[t] = c;
     if (s.flags[i] & kFlagBoundary) {
         s.p[i] = 0.0;
         return;
@@ -150,14 +161,14 @@ __global__ void k_pressure_f32(uint32_t n, F32Const k, StateBufs s, F32Bufs f, D
 }
 
 template <int DIM>
-__global__ void __launch_bounds__(kThreads) k_forces_f32(uint32_t n, F32Const k, StateBufs s, F32Bufs f,
-                                                         ListBufs l, const DeviceScalars* sc,
-                                                         float dt, double4* __restrict__ pos_next,
-                                                         double4* __restrict__ vel_next,
-                                                         float* __restrict__ bf) {
+__global__ void __launch_bounds__(kMaxPassThreads) k_forces_f32(uint32_t n, F32Const k, Tanks tk,
+                                                                StateBufs s, F32Bufs f, ListBufs l,
+                                                                float dt, double4* __restrict__ pos_next,
+                                                                double4* __restrict__ vel_next,
+                                                                float* __restrict__ bf) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n || (s.flags[i] & kFlagBoundary)) return;
-    const float c0 = (float)sc->sound_speed;
+    const float c0 = (float)tk.c[tk.slot_tank[i]];
     const float nac = -k.visc_alpha * c0;
     const float4 pi = f.pos[i];
     const float4 vi = f.vel[i];
@@ -214,7 +225,7 @@ __global__ void __launch_bounds__(kThreads) k_forces_f32(uint32_t n, F32Const k,
     vel_next[i] = make_double4(vx, vy, vz, vi.w);
 }
 
-__global__ void __launch_bounds__(kThreads) k_xsph_f32(uint32_t n, F32Const k, StateBufs s, F32Bufs f,
+__global__ void __launch_bounds__(kMaxPassThreads) k_xsph_f32(uint32_t n, F32Const k, StateBufs s, F32Bufs f,
                                                        ListBufs l, float4* __restrict__ vel_out) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -271,32 +282,34 @@ void launch_f32_from_f64(uint32_t n, double cell, const StateBufs& s, const F32B
     if (n) k_f32_from_f64<<<blocks_for(n, 256), 256, 0, st>>>(n, cell, s, f);
 }
 
-void launch_density_f32(uint32_t n, const F32Const& k, const StateBufs& s, const F32Bufs& f,
-                        const ListBufs& l, cudaStream_t st) {
-    if (n) k_density_f32<<<blocks_for(n, kThreads), kThreads, 0, st>>>(n, k, s, f, l);
+void launch_density_f32(uint32_t n, uint32_t threads, const F32Const& k, const StateBufs& s,
+                        const F32Bufs& f, const ListBufs& l, cudaStream_t st) {
+    if (n) k_density_f32<<<blocks_for(n, threads), threads, 0, st>>>(n, k, s, f, l);
 }
 
-void launch_pressure_f32(uint32_t n, const F32Const& k, const StateBufs& s, const F32Bufs& f,
-                         DeviceScalars* sc, cudaStream_t st) {
-    if (k.adapt_sound_speed && n) k_vmax_f32<<<blocks_for(n, 256), 256, 0, st>>>(n, s, f, sc);
-    k_pressure_f32<<<blocks_for(n ? n : 1, 256), 256, 0, st>>>(n, k, s, f, sc);
+void launch_pressure_f32(uint32_t n, const F32Const& k, const Tanks& tk, const StateBufs& s,
+                         const F32Bufs& f, cudaStream_t st) {
+    if (!n) return;
+    if (k.adapt_sound_speed) k_vmax_f32<<<blocks_for(n, 256), 256, 0, st>>>(n, tk, s, f);
+    k_pressure_f32<<<blocks_for(n, 256), 256, 0, st>>>(n, k, tk, s, f);
 }
 
-void launch_forces_f32(uint32_t n, const F32Const& k, const StateBufs& s, const F32Bufs& f,
-                       const ListBufs& l, const DeviceScalars* sc, float dt, double4* pos_next,
-                       double4* vel_next, float* bf, cudaStream_t st) {
+void launch_forces_f32(uint32_t n, uint32_t threads, const F32Const& k, const Tanks& tk,
+                       const StateBufs& s, const F32Bufs& f, const ListBufs& l, float dt,
+                       double4* pos_next, double4* vel_next, float* bf, cudaStream_t st) {
     if (!n) return;
     if (bf) cudaMemsetAsync(bf, 0, sizeof(float) * 4 * (size_t)n, st);
+    const uint32_t b = blocks_for(n, threads);
     if (k.dim == 3)
-        k_forces_f32<3><<<blocks_for(n, kThreads), kThreads, 0, st>>>(n, k, s, f, l, sc, dt, pos_next, vel_next, bf);
+        k_forces_f32<3><<<b, threads, 0, st>>>(n, k, tk, s, f, l, dt, pos_next, vel_next, bf);
     else
-        k_forces_f32<2><<<blocks_for(n, kThreads), kThreads, 0, st>>>(n, k, s, f, l, sc, dt, pos_next, vel_next, bf);
+        k_forces_f32<2><<<b, threads, 0, st>>>(n, k, tk, s, f, l, dt, pos_next, vel_next, bf);
     if (bf) k_bf_to_f64<<<blocks_for(n, 256), 256, 0, st>>>(n, bf, s);
 }
 
-void launch_xsph_f32(uint32_t n, const F32Const& k, const StateBufs& s, const F32Bufs& f,
-                     const ListBufs& l, float4* vel_out, cudaStream_t st) {
-    if (n) k_xsph_f32<<<blocks_for(n, kThreads), kThreads, 0, st>>>(n, k, s, f, l, vel_out);
+void launch_xsph_f32(uint32_t n, uint32_t threads, const F32Const& k, const StateBufs& s,
+                     const F32Bufs& f, const ListBufs& l, float4* vel_out, cudaStream_t st) {
+    if (n) k_xsph_f32<<<blocks_for(n, threads), threads, 0, st>>>(n, k, s, f, l, vel_out);
 }
 
 }  // namespace pe

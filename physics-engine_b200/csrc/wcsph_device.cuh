@@ -51,6 +51,27 @@ struct GridDesc {
     int dim;
 };
 
+// Tanks: independent worlds stepped together. Particles are stored tank-major
+// (original index = tank's first index + index within the tank); each tank has
+// its own dense key box, and the boxes are laid end to end in one cell-id
+// space, so the counting sort keeps every tank's particles in the tank's own
+// slot range. A single world is one tank.
+struct TankDesc {
+    int32_t kx0, ky0, kz0;  // key of the tank's dense cell (0,0,0)
+    int32_t nx, ny, nz;     // dense extents
+    uint32_t cell_base;     // first global cell id of the tank
+    uint32_t slot_begin;    // first slot (and original index) of the tank
+};
+
+struct Tanks {
+    const TankDesc* desc;          // [count]; null selects the single box of GridDesc
+    const uint16_t* slot_tank;     // [n] tank of each slot
+    const uint16_t* cell_tank;     // [ncell] tank of each dense cell
+    double* c;                     // [count] persisted sound speed (wcsph.rs:168)
+    unsigned long long* vmax2;     // [count] max |v|^2 of the tank's fluid as u64 bits
+    uint32_t count;
+};
+
 struct StepConst {
     int dim;
     double h, mass, rho0;      // particles.h, .mass, .rest_density
@@ -125,13 +146,18 @@ __device__ __forceinline__ ListRef list_ref(const ListBufs& l, uint32_t s, int k
 }
 
 struct DeviceScalars {
-    unsigned long long vmax2_bits;  // max |v|^2 of fluid as u64 bits
-    double sound_speed;             // persisted c (wcsph.rs:168)
     uint32_t status;
     uint32_t nocc;                  // occupied cells
     uint32_t max_union;             // largest neighbour-cell union seen by the list build
     uint32_t pad_;
     unsigned long long list_used;   // 16-byte groups the last list build asked for
+};
+
+// Block size of the per-particle passes: a launch parameter, chosen by the
+// world's autotuner among 64, 128 and 256.
+constexpr int kMaxPassThreads = 256;
+struct PassShape {
+    uint32_t density = 128, forces = 128, xsph = 128;
 };
 
 // Single-precision form (sph_f32.cu).
@@ -155,20 +181,20 @@ struct F32Bufs {
 
 void launch_f32_from_f64(uint32_t n, double cell, const StateBufs& s, const F32Bufs& f,
                          cudaStream_t st);
-void launch_density_f32(uint32_t n, const F32Const& k, const StateBufs& s, const F32Bufs& f,
-                        const ListBufs& l, cudaStream_t st);
-void launch_pressure_f32(uint32_t n, const F32Const& k, const StateBufs& s, const F32Bufs& f,
-                         DeviceScalars* sc, cudaStream_t st);
-void launch_forces_f32(uint32_t n, const F32Const& k, const StateBufs& s, const F32Bufs& f,
-                       const ListBufs& l, const DeviceScalars* sc, float dt, double4* pos_next,
-                       double4* vel_next, float* bf, cudaStream_t st);
-void launch_xsph_f32(uint32_t n, const F32Const& k, const StateBufs& s, const F32Bufs& f,
-                     const ListBufs& l, float4* vel_out, cudaStream_t st);
+void launch_density_f32(uint32_t n, uint32_t threads, const F32Const& k, const StateBufs& s,
+                        const F32Bufs& f, const ListBufs& l, cudaStream_t st);
+void launch_pressure_f32(uint32_t n, const F32Const& k, const Tanks& tk, const StateBufs& s,
+                         const F32Bufs& f, cudaStream_t st);
+void launch_forces_f32(uint32_t n, uint32_t threads, const F32Const& k, const Tanks& tk,
+                       const StateBufs& s, const F32Bufs& f, const ListBufs& l, float dt,
+                       double4* pos_next, double4* vel_next, float* bf, cudaStream_t st);
+void launch_xsph_f32(uint32_t n, uint32_t threads, const F32Const& k, const StateBufs& s,
+                     const F32Bufs& f, const ListBufs& l, float4* vel_out, cudaStream_t st);
 
 // ----- grid build -----
-void launch_cell_ids(const GridDesc& g, uint32_t n, const double4* pos_cur, const double4* pos_next,
-                     const uint8_t* flags, uint32_t* cellid, int4* key_tmp, uint32_t* count,
-                     DeviceScalars* sc, cudaStream_t st);
+void launch_cell_ids(const GridDesc& g, const Tanks& tk, uint32_t n, const double4* pos_cur,
+                     const double4* pos_next, const uint8_t* flags, uint32_t* cellid, int4* key_tmp,
+                     uint32_t* count, DeviceScalars* sc, cudaStream_t st);
 size_t scan_temp_bytes(uint32_t ncell);
 void launch_scan_cells(uint32_t ncell, const uint32_t* count, uint32_t* cell_start, uint32_t* occ,
                        DeviceScalars* sc, void* temp, cudaStream_t st);
@@ -187,23 +213,24 @@ size_t nlist_smem_bytes(uint32_t ucap);
 // Sets the dynamic shared-memory limit of the list kernel for this stage size
 // and returns how many of its CTAs fit on one SM.
 uint32_t nlist_prepare(int dim, uint32_t ucap);
-void launch_nlist(const GridDesc& g, const StepConst& k, uint32_t ucap, uint32_t nblocks,
-                  const uint32_t* occ, const uint32_t* cell_start, const StateBufs& s,
-                  const ListBufs& l, DeviceScalars* sc, cudaStream_t st, bool visit_only = false);
+void launch_nlist(const GridDesc& g, const Tanks& tk, const StepConst& k, uint32_t ucap,
+                  uint32_t nblocks, const uint32_t* occ, const uint32_t* cell_start,
+                  const StateBufs& s, const ListBufs& l, DeviceScalars* sc, cudaStream_t st,
+                  bool visit_only = false);
 
 // ----- SPH passes -----
-void launch_density(uint32_t n, const StepConst& k, const StateBufs& s, const ListBufs& l,
-                    cudaStream_t st);
-void launch_vmax(uint32_t n, const StateBufs& s, DeviceScalars* sc, cudaStream_t st);
-void launch_pressure(uint32_t n, const StepConst& k, const StateBufs& s, DeviceScalars* sc,
+void launch_density(uint32_t n, uint32_t threads, const StepConst& k, const StateBufs& s,
+                    const ListBufs& l, cudaStream_t st);
+void launch_vmax(uint32_t n, const Tanks& tk, const StateBufs& s, cudaStream_t st);
+void launch_pressure(uint32_t n, const StepConst& k, const Tanks& tk, const StateBufs& s,
                      cudaStream_t st);
-void launch_forces(uint32_t n, const StepConst& k, const StateBufs& s, const ListBufs& l,
-                   const DeviceScalars* sc, bool integrate, double dt, double4* pos_next,
-                   double4* vel_next, cudaStream_t st);
+void launch_forces(uint32_t n, uint32_t threads, const StepConst& k, const Tanks& tk,
+                   const StateBufs& s, const ListBufs& l, bool integrate, double dt,
+                   double4* pos_next, double4* vel_next, cudaStream_t st);
 void launch_boundary_force(uint32_t n, const StepConst& k, const StateBufs& s, const ListBufs& l,
                            cudaStream_t st);
-void launch_xsph(uint32_t n, const StepConst& k, const StateBufs& s, const ListBufs& l,
-                 double4* vel_out, cudaStream_t st);
+void launch_xsph(uint32_t n, uint32_t threads, const StepConst& k, const StateBufs& s,
+                 const ListBufs& l, double4* vel_out, cudaStream_t st);
 
 // ----- exports / diagnostics -----
 void launch_occupied_export(const GridDesc& g, const uint32_t* occ, const DeviceScalars* sc,

@@ -113,48 +113,77 @@ T* World::alloc(size_t count) {
 
 World::World(const WorldParams& prm, const WorldConfig& cfg, int dim, double rest_density,
              double mass, double h, uint64_t n, const double* x, const double* v,
-             const uint8_t* kind, const double* psi, const double* n_out)
+             const uint8_t* kind, const double* psi, const double* n_out,
+             const uint64_t* tank_offsets, uint32_t n_tanks)
     : dim_(dim), rho0_(rest_density), mass_(mass), h_(h), n_(n), prm_(prm), cfg_(cfg) {
     if (cfg_.device >= 0) check(cudaSetDevice(cfg_.device), "cudaSetDevice");
     check(cudaGetDevice(&device_), "cudaGetDevice");
+    // ---- tanks: contiguous particle ranges ----
+    std::vector<uint64_t> toff;
+    if (tank_offsets && n_tanks >= 1) {
+        if (n_tanks > 65535u) throw std::length_error("too many tanks");
+        toff.assign(tank_offsets, tank_offsets + n_tanks + 1);
+        if (toff.front() != 0 || toff.back() != n_) throw std::invalid_argument("tank offsets");
+        for (uint32_t t = 0; t < n_tanks; ++t)
+            if (toff[t + 1] <= toff[t]) throw std::invalid_argument("empty or unordered tank");
+    } else {
+        n_tanks = 1;
+        toff = {0, n_};
+    }
+    n_tanks_ = n_tanks;
     check(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking), "cudaStreamCreate");
     try {
-        // ---- grid domain from the initial keys (grid.rs:62 key_of) ----
+        // ---- each tank's grid domain from its initial keys (grid.rs:62 key_of) ----
         const double cell = 2.0 * h_;  // support_radius(CubicSpline, h), kernels.rs:32
         const double inv = 1.0 / cell;
-        long long lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
-        for (uint64_t i = 0; i < n_; ++i) {
-            long long k3[3] = {floor_i32(x[3 * i] * inv), floor_i32(x[3 * i + 1] * inv),
-                               dim_ == 2 ? 0 : floor_i32(x[3 * i + 2] * inv)};
+        const double frac = cfg_.domain_margin < 0.0 ? 0.25 : cfg_.domain_margin;
+        const long long minc = cfg_.domain_margin_cells ? cfg_.domain_margin_cells : 4;
+        tank_host_.resize(n_tanks_);
+        uint64_t total_cells = 0;
+        for (uint32_t t = 0; t < n_tanks_; ++t) {
+            long long lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+            for (uint64_t i = toff[t]; i < toff[t + 1]; ++i) {
+                long long k3[3] = {floor_i32(x[3 * i] * inv), floor_i32(x[3 * i + 1] * inv),
+                                   dim_ == 2 ? 0 : floor_i32(x[3 * i + 2] * inv)};
+                for (int a = 0; a < 3; ++a) {
+                    if (i == toff[t] || k3[a] < lo[a]) lo[a] = k3[a];
+                    if (i == toff[t] || k3[a] > hi[a]) hi[a] = k3[a];
+                }
+            }
+            long long ext[3];
             for (int a = 0; a < 3; ++a) {
-                if (i == 0 || k3[a] < lo[a]) lo[a] = k3[a];
-                if (i == 0 || k3[a] > hi[a]) hi[a] = k3[a];
+                if (dim_ == 2 && a == 2) {
+                    lo[a] = hi[a] = 0;
+                    ext[a] = 1;
+                    continue;
+                }
+                long long span = hi[a] - lo[a] + 1;
+                long long m = std::max<long long>(minc, (long long)std::ceil(frac * (double)span));
+                lo[a] = std::max<long long>(lo[a] - m, -2147483647LL);
+                hi[a] = std::min<long long>(hi[a] + m, 2147483646LL);
+                ext[a] = hi[a] - lo[a] + 1;
             }
+            const double ncell = (double)ext[0] * (double)ext[1] * (double)ext[2];
+            if (ncell > (double)(1u << 28)) throw std::length_error("grid domain too large");
+            TankDesc& td = tank_host_[t];
+            td.kx0 = (int32_t)lo[0];
+            td.ky0 = (int32_t)lo[1];
+            td.kz0 = (int32_t)lo[2];
+            td.nx = (int32_t)ext[0];
+            td.ny = (int32_t)ext[1];
+            td.nz = (int32_t)ext[2];
+            td.cell_base = (uint32_t)total_cells;
+            td.slot_begin = (uint32_t)toff[t];
+            total_cells += (uint64_t)ncell;
+            if (total_cells > (1ull << 31)) throw std::length_error("grid domain too large");
         }
-        double frac = cfg_.domain_margin < 0.0 ? 0.25 : cfg_.domain_margin;
-        long long minc = cfg_.domain_margin_cells ? cfg_.domain_margin_cells : 4;
-        long long ext[3];
-        for (int a = 0; a < 3; ++a) {
-            if (dim_ == 2 && a == 2) {
-                lo[a] = hi[a] = 0;
-                ext[a] = 1;
-                continue;
-            }
-            long long span = hi[a] - lo[a] + 1;
-            long long m = std::max<long long>(minc, (long long)std::ceil(frac * (double)span));
-            lo[a] = std::max<long long>(lo[a] - m, -2147483647LL);
-            hi[a] = std::min<long long>(hi[a] + m, 2147483646LL);
-            ext[a] = hi[a] - lo[a] + 1;
-        }
-        double ncell = (double)ext[0] * (double)ext[1] * (double)ext[2];
-        if (ncell > (double)(1u << 28)) throw std::length_error("grid domain too large");
-        g_.kx0 = (int32_t)lo[0];
-        g_.ky0 = (int32_t)lo[1];
-        g_.kz0 = (int32_t)lo[2];
-        g_.nx = (int32_t)ext[0];
-        g_.ny = (int32_t)ext[1];
-        g_.nz = (int32_t)ext[2];
-        g_.ncell = (uint32_t)ncell;
+        g_.kx0 = tank_host_[0].kx0;
+        g_.ky0 = tank_host_[0].ky0;
+        g_.kz0 = tank_host_[0].kz0;
+        g_.nx = tank_host_[0].nx;
+        g_.ny = tank_host_[0].ny;
+        g_.nz = tank_host_[0].nz;
+        g_.ncell = (uint32_t)total_cells;
         g_.inv_cell = inv;
         g_.cell_size = cell;
         g_.dim = dim_;
@@ -164,26 +193,35 @@ World::World(const WorldParams& prm, const WorldConfig& cfg, int dim, double res
 
         // ---- union stage capacity from the largest initial neighbour-cell union ----
         std::vector<uint32_t> cnt(g_.ncell, 0);
-        for (uint64_t i = 0; i < n_; ++i) {
-            long long kx = floor_i32(x[3 * i] * inv) - g_.kx0, ky = floor_i32(x[3 * i + 1] * inv) - g_.ky0;
-            long long kz = dim_ == 2 ? 0 : floor_i32(x[3 * i + 2] * inv) - g_.kz0;
-            ++cnt[(uint32_t)((kx * g_.ny + ky) * g_.nz + kz)];
-        }
+        std::vector<uint16_t> cell_tank(g_.ncell, 0);
         uint32_t max_union = 1;
-        for (int cx = 0; cx < g_.nx; ++cx)
-            for (int cy = 0; cy < g_.ny; ++cy)
-                for (int cz = 0; cz < g_.nz; ++cz) {
-                    if (!cnt[((size_t)cx * g_.ny + cy) * g_.nz + cz]) continue;
-                    uint32_t u = 0;
-                    for (int dx = -1; dx <= 1; ++dx)
-                        for (int dy = -1; dy <= 1; ++dy)
-                            for (int dz = (dim_ == 2 ? 0 : -1); dz <= (dim_ == 2 ? 0 : 1); ++dz) {
-                                int qx = cx + dx, qy = cy + dy, qz = cz + dz;
-                                if (qx < 0 || qy < 0 || qz < 0 || qx >= g_.nx || qy >= g_.ny || qz >= g_.nz) continue;
-                                u += cnt[((size_t)qx * g_.ny + qy) * g_.nz + qz];
-                            }
-                    max_union = std::max(max_union, u);
-                }
+        for (uint32_t t = 0; t < n_tanks_; ++t) {
+            const TankDesc& td = tank_host_[t];
+            const size_t cells_t = (size_t)td.nx * td.ny * td.nz;
+            std::fill(cell_tank.begin() + td.cell_base, cell_tank.begin() + td.cell_base + cells_t,
+                      (uint16_t)t);
+            uint32_t* c = cnt.data() + td.cell_base;
+            std::vector<uint32_t> occupied;
+            for (uint64_t i = toff[t]; i < toff[t + 1]; ++i) {
+                long long kx = floor_i32(x[3 * i] * inv) - td.kx0, ky = floor_i32(x[3 * i + 1] * inv) - td.ky0;
+                long long kz = dim_ == 2 ? 0 : floor_i32(x[3 * i + 2] * inv) - td.kz0;
+                const uint32_t lc = (uint32_t)((kx * td.ny + ky) * td.nz + kz);
+                if (c[lc]++ == 0) occupied.push_back(lc);
+            }
+            for (uint32_t lc : occupied) {
+                const int cz = (int)(lc % (uint32_t)td.nz), cy = (int)((lc / (uint32_t)td.nz) % (uint32_t)td.ny);
+                const int cx = (int)(lc / ((uint32_t)td.nz * (uint32_t)td.ny));
+                uint32_t u = 0;
+                for (int dx = -1; dx <= 1; ++dx)
+                    for (int dy = -1; dy <= 1; ++dy)
+                        for (int dz = (dim_ == 2 ? 0 : -1); dz <= (dim_ == 2 ? 0 : 1); ++dz) {
+                            int qx = cx + dx, qy = cy + dy, qz = cz + dz;
+                            if (qx < 0 || qy < 0 || qz < 0 || qx >= td.nx || qy >= td.ny || qz >= td.nz) continue;
+                            u += c[((size_t)qx * td.ny + qy) * td.nz + qz];
+                        }
+                max_union = std::max(max_union, u);
+            }
+        }
         ucap_ = nlist_union_capacity(max_union);
 
         // ---- allocations ----
@@ -224,6 +262,31 @@ World::World(const WorldParams& prm, const WorldConfig& cfg, int dim, double res
         lists_.ncand = alloc<uint32_t>(N);
         insup_ = alloc<uint32_t>(N);
         sc_ = alloc<DeviceScalars>(1);
+        {
+            TankDesc* d_desc = alloc<TankDesc>(n_tanks_);
+            uint16_t* d_slot_tank = alloc<uint16_t>(N);
+            uint16_t* d_cell_tank = alloc<uint16_t>(g_.ncell);
+            tanks_.c = alloc<double>(n_tanks_);
+            tanks_.vmax2 = alloc<unsigned long long>(n_tanks_);
+            std::vector<uint16_t> slot_tank(N, 0);
+            for (uint32_t t = 0; t < n_tanks_; ++t)
+                std::fill(slot_tank.begin() + toff[t], slot_tank.begin() + toff[t + 1], (uint16_t)t);
+            std::vector<double> c0(n_tanks_, prm_.eos_sound_speed);
+            check(cudaMemcpyAsync(d_desc, tank_host_.data(), sizeof(TankDesc) * n_tanks_,
+                                  cudaMemcpyHostToDevice, st_), "upload");
+            check(cudaMemcpyAsync(d_slot_tank, slot_tank.data(), sizeof(uint16_t) * N,
+                                  cudaMemcpyHostToDevice, st_), "upload");
+            check(cudaMemcpyAsync(d_cell_tank, cell_tank.data(), sizeof(uint16_t) * g_.ncell,
+                                  cudaMemcpyHostToDevice, st_), "upload");
+            check(cudaMemcpyAsync(tanks_.c, c0.data(), sizeof(double) * n_tanks_, cudaMemcpyHostToDevice, st_),
+                  "upload");
+            // the host vectors must outlive the copies
+            check(cudaStreamSynchronize(st_), "upload");
+            tanks_.desc = d_desc;
+            tanks_.slot_tank = d_slot_tank;
+            tanks_.cell_tank = d_cell_tank;
+            tanks_.count = n_tanks_;
+        }
         xfer_ = alloc<double>(N * 4);
         if (f32_) {
             fb_.pos = alloc<float4>(N);
@@ -255,7 +318,6 @@ World::World(const WorldParams& prm, const WorldConfig& cfg, int dim, double res
         check(cudaMemcpyAsync(cur_.orig, ho.data(), N * sizeof(uint32_t), cudaMemcpyHostToDevice, st_), "upload");
         check(cudaMemcpyAsync(slot_of_orig_, ho.data(), N * sizeof(uint32_t), cudaMemcpyHostToDevice, st_), "upload");
         DeviceScalars hs{};
-        hs.sound_speed = prm_.eos_sound_speed;
         check(cudaMemcpyAsync(sc_, &hs, sizeof(hs), cudaMemcpyHostToDevice, st_), "upload");
 
         // ---- launch geometry of the list build: a persistent grid ----
@@ -288,10 +350,12 @@ void World::alloc_lists(unsigned long long groups) {
     lists_.pool = static_cast<uint32_t*>(p);
     lists_.pool_groups = groups;
     lists_valid_ = false;
+    invalidate_graph();
 }
 
 World::~World() {
     if (st_) cudaStreamSynchronize(st_);
+    release_graph();
     for (void* p : list_allocs_) cudaFree(p);
     for (auto& r : recs_) {
         cudaEventDestroy(r.a);
@@ -404,6 +468,7 @@ void World::refresh_step_const() {
     f.boundary_eps_h = (float)k.boundary_eps_h;
     f.adapt_sound_speed = prm_.adapt_sound_speed;
     kf_ = f;
+    invalidate_graph();
 }
 
 void World::refresh_f32() {
@@ -422,15 +487,22 @@ void World::set_params(const WorldParams& p) {
 
 double World::sound_speed() {
     double c = 0.0;
-    check(cudaMemcpyAsync(&c, &sc_->sound_speed, sizeof(double), cudaMemcpyDeviceToHost, st_), "get c");
+    check(cudaMemcpyAsync(&c, tanks_.c, sizeof(double), cudaMemcpyDeviceToHost, st_), "get c");
     check(cudaStreamSynchronize(st_), "get c");
     prm_.eos_sound_speed = c;
     return c;
 }
 
+void World::get_sound_speeds(double* out) {
+    check(cudaMemcpyAsync(out, tanks_.c, sizeof(double) * n_tanks_, cudaMemcpyDeviceToHost, st_), "get c");
+    check(cudaStreamSynchronize(st_), "get c");
+}
+
 void World::set_sound_speed(double c) {
     prm_.eos_sound_speed = c;
-    check(cudaMemcpyAsync(&sc_->sound_speed, &c, sizeof(double), cudaMemcpyHostToDevice, st_), "set c");
+    std::vector<double> all(n_tanks_, c);
+    check(cudaMemcpyAsync(tanks_.c, all.data(), sizeof(double) * n_tanks_, cudaMemcpyHostToDevice, st_),
+          "set c");
     check(cudaStreamSynchronize(st_), "set c");
 }
 
@@ -441,7 +513,7 @@ void World::build_grid(const double4* pos_next, const double4* vel_next) {
     prof_begin(kGrid);
     check(cudaMemsetAsync(count_, 0, sizeof(uint32_t) * g_.ncell, st_), "memset");
     check(cudaMemsetAsync(fill_, 0, sizeof(uint32_t) * g_.ncell, st_), "memset");
-    launch_cell_ids(g_, n, cur_.pos, pos_next, cur_.flags, cellid_, key_tmp_, count_, sc_, st_);
+    launch_cell_ids(g_, tanks_, n, cur_.pos, pos_next, cur_.flags, cellid_, key_tmp_, count_, sc_, st_);
     launch_scan_cells(g_.ncell, count_, cell_start_, occ_, sc_, scan_tmp_, st_);
     launch_place(n, cellid_, cell_start_, fill_, cur_.orig, tmp_old_, tmp_orig_, st_);
     launch_cellsort(std::min<uint32_t>(g_.ncell, n ? n : 1), occ_, sc_, cell_start_, tmp_old_, tmp_orig_,
@@ -466,7 +538,7 @@ void World::ensure_lists() {
         for (int attempt = 0; attempt < 4; ++attempt) {
             check(cudaMemsetAsync(&sc_->list_used, 0, sizeof(unsigned long long), st_), "memset");
             prof_begin(kLists);
-            launch_nlist(g_, kc_, ucap_, nl_blocks_, occ_, cell_start_, cur_, lists_, sc_, st_, f32_);
+            launch_nlist(g_, tanks_, kc_, ucap_, nl_blocks_, occ_, cell_start_, cur_, lists_, sc_, st_, f32_);
             prof_end();
             launches_ += 1;
             check(cudaGetLastError(), "neighbour lists");
@@ -508,8 +580,8 @@ void World::ensure_lists() {
 void World::run_density() {
     ensure_lists();
     prof_begin(kDensity);
-    if (f32_) launch_density_f32((uint32_t)n_, kf_, cur_, fb_, lists_, st_);
-    else launch_density((uint32_t)n_, kc_, cur_, lists_, st_);
+    if (f32_) launch_density_f32((uint32_t)n_, shape_.density, kf_, cur_, fb_, lists_, st_);
+    else launch_density((uint32_t)n_, shape_.density, kc_, cur_, lists_, st_);
     prof_end();
     launches_ += 1;
     check(cudaGetLastError(), "density");
@@ -517,16 +589,17 @@ void World::run_density() {
 
 void World::run_pressure() {
     prof_begin(kPressure);
-    check(cudaMemsetAsync(&sc_->vmax2_bits, 0, sizeof(unsigned long long), st_), "memset");
+    if (prm_.adapt_sound_speed)
+        check(cudaMemsetAsync(tanks_.vmax2, 0, sizeof(unsigned long long) * n_tanks_, st_), "memset");
     if (f32_) {
-        launch_pressure_f32((uint32_t)n_, kf_, cur_, fb_, sc_, st_);
+        launch_pressure_f32((uint32_t)n_, kf_, tanks_, cur_, fb_, st_);
         launches_ += kf_.adapt_sound_speed ? 1 : 0;
     } else {
         if (kc_.adapt_sound_speed) {
-            launch_vmax((uint32_t)n_, cur_, sc_, st_);
+            launch_vmax((uint32_t)n_, tanks_, cur_, st_);
             launches_ += 1;
         }
-        launch_pressure((uint32_t)n_, kc_, cur_, sc_, st_);
+        launch_pressure((uint32_t)n_, kc_, tanks_, cur_, st_);
     }
     prof_end();
     launches_ += 1;
@@ -539,13 +612,14 @@ void World::run_forces(bool integrate, double dt) {
         // the single-precision form always integrates into the next buffers;
         // without a kick/drift request the step is taken with dt = 0
         prof_begin(kForces);
-        launch_forces_f32((uint32_t)n_, kf_, cur_, fb_, lists_, sc_, integrate ? (float)dt : 0.f,
-                          pos_nx_, vel_nx_, bf32_, st_);
+        launch_forces_f32((uint32_t)n_, shape_.forces, kf_, tanks_, cur_, fb_, lists_,
+                          integrate ? (float)dt : 0.f, pos_nx_, vel_nx_, bf32_, st_);
         prof_end();
         launches_ += 2;
     } else {
         prof_begin(kForces);
-        launch_forces((uint32_t)n_, kc_, cur_, lists_, sc_, integrate, dt, pos_nx_, vel_nx_, st_);
+        launch_forces((uint32_t)n_, shape_.forces, kc_, tanks_, cur_, lists_, integrate, dt, pos_nx_,
+                      vel_nx_, st_);
         prof_end();
         prof_begin(kBoundaryForce);
         launch_boundary_force((uint32_t)n_, kc_, cur_, lists_, st_);
@@ -560,14 +634,14 @@ void World::run_xsph() {
     ensure_lists();
     prof_begin(kXsph);
     if (f32_) {
-        launch_xsph_f32((uint32_t)n_, kf_, cur_, fb_, lists_, velf_alt_, st_);
+        launch_xsph_f32((uint32_t)n_, shape_.xsph, kf_, cur_, fb_, lists_, velf_alt_, st_);
         prof_end();
         launches_ += 1;
         check(cudaGetLastError(), "xsph");
         std::swap(fb_.vel, velf_alt_);
         return;
     }
-    launch_xsph((uint32_t)n_, kc_, cur_, lists_, vel_nx_, st_);
+    launch_xsph((uint32_t)n_, shape_.xsph, kc_, cur_, lists_, vel_nx_, st_);
     prof_end();
     launches_ += 1;
     check(cudaGetLastError(), "xsph");
@@ -615,16 +689,185 @@ void World::step(double dt) {
 }
 
 void World::run(double dt, uint64_t steps) {
-    for (uint64_t s = 0; s < steps; ++s) {
+    uint64_t s = 0, last_poll = 0;
+    while (s < steps) {
+        if (cfg_.use_graph && steps - s >= kGraphSteps && graph_capturable()) {
+            if (!graph_exec_ || graph_dt_ != dt || graph_epoch_ != epoch_) capture_graph(dt);
+            if (graph_exec_) {
+                check(cudaGraphLaunch(graph_exec_, st_), "graph launch");
+                s += kGraphSteps;
+                for (uint32_t k = 0; k < kGraphSteps; ++k) t_ += dt;  // wcsph.rs:346, once per step
+                launches_ += graph_launches_;
+                if (s - last_poll >= 16) {
+                    status();
+                    last_poll = s;
+                }
+                continue;
+            }
+        }
         step(dt);
-        if ((s & 15u) == 15u) status();  // lets the list storage and stage grow if needed
+        ++s;
+        if (s - last_poll >= 16) {
+            status();  // lets the list storage and stage grow if needed
+            last_poll = s;
+        }
     }
+}
+
+// A step can be captured when it issues no host synchronisation: the grid and
+// densities are current (no initial rebuild), the list capacity has been
+// checked for these positions, and no phase events are being recorded.
+bool World::graph_capturable() const {
+    return grid_current_ && rho_current_ && lists_checked_ && lists_sized_ && !profiling_ && n_ > 0;
+}
+
+void World::release_graph() {
+    if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
+    graph_exec_ = nullptr;
+}
+
+// Captures kGraphSteps steps into one graph. Capturing records the launches
+// without running them, so every host-side effect of the captured steps
+// (buffer rotations, time, launch count) is undone afterwards and replayed
+// per graph launch; the rotations return to their start after kGraphSteps
+// steps, which is checked here.
+bool World::capture_graph(double dt) {
+    release_graph();
+    const StateBufs cur0 = cur_, alt0 = alt_;
+    double4* const vel_nx0 = vel_nx_;
+    const F32Bufs fb0 = fb_;
+    float4* const velf_alt0 = velf_alt_;
+    const double t0 = t_;
+    const uint32_t l0 = launches_;
+    cudaGraph_t graph = nullptr;
+    bool ok = cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+    if (ok) {
+        try {
+            for (uint32_t k = 0; k < kGraphSteps; ++k) step(dt);
+        } catch (const std::exception&) {
+            ok = false;
+        }
+        ok = cudaStreamEndCapture(st_, &graph) == cudaSuccess && ok;
+    }
+    const bool same = std::memcmp(&cur_, &cur0, sizeof(cur0)) == 0 &&
+                      std::memcmp(&alt_, &alt0, sizeof(alt0)) == 0 && vel_nx_ == vel_nx0 &&
+                      std::memcmp(&fb_, &fb0, sizeof(fb0)) == 0 && velf_alt_ == velf_alt0;
+    graph_launches_ = launches_ - l0;
+    cur_ = cur0;
+    alt_ = alt0;
+    vel_nx_ = vel_nx0;
+    fb_ = fb0;
+    velf_alt_ = velf_alt0;
+    t_ = t0;
+    launches_ = l0;
+    cudaGetLastError();  // clear the (non-sticky) error a failed capture leaves
+    if (ok && same && graph) {
+        if (cudaGraphInstantiate(&graph_exec_, graph, 0) != cudaSuccess) {
+            graph_exec_ = nullptr;
+            cudaGetLastError();
+        }
+    }
+    if (graph) cudaGraphDestroy(graph);
+    graph_dt_ = dt;
+    graph_epoch_ = epoch_;
+    return graph_exec_ != nullptr;
 }
 
 void World::configure_lists() {
     uint32_t per_sm = nlist_prepare(dim_, ucap_);
     check(cudaGetLastError(), "nlist prepare");
-    nl_blocks_ = sms_ * std::max<uint32_t>(per_sm, 1u) * 4u;
+    const uint32_t mult = list_ctas_per_sm_ ? list_ctas_per_sm_ : std::max<uint32_t>(per_sm, 1u) * 4u;
+    nl_blocks_ = sms_ * mult;
+    invalidate_graph();
+}
+
+World::Shapes World::shapes() const {
+    Shapes r;
+    r.density = shape_.density;
+    r.forces = shape_.forces;
+    r.xsph = shape_.xsph;
+    r.list_ctas_per_sm = nl_blocks_ / std::max<uint32_t>(sms_, 1u);
+    return r;
+}
+
+// Times each candidate launch shape on the current state with CUDA events and
+// keeps the fastest. Every timed pass is idempotent here: the list build and
+// the density pass recompute the same values, the force pass writes only the
+// next-state scratch buffers, and XSPH (f64) writes the scratch velocity
+// buffer without the swap that would commit it. Results do not depend on the
+// shapes (each particle's sums run in the same order in every shape).
+World::Shapes World::autotune() {
+    if (!n_) return shapes();
+    if (!grid_current_) {
+        build_grid(nullptr, nullptr);
+        refresh_f32();
+        grid_current_ = true;
+        rho_current_ = false;
+    }
+    ensure_lists();
+    const bool prof = profiling_;
+    profiling_ = false;
+    cudaEvent_t a = take_event(), b = take_event();
+    auto time_it = [&](auto&& launch) {
+        launch();  // warm
+        check(cudaEventRecord(a, st_), "autotune");
+        for (int r = 0; r < 3; ++r) launch();
+        check(cudaEventRecord(b, st_), "autotune");
+        check(cudaEventSynchronize(b), "autotune");
+        float ms = 0.f;
+        check(cudaEventElapsedTime(&ms, a, b), "autotune");
+        return ms;
+    };
+    const uint32_t cand[3] = {64, 128, 256};
+    const uint32_t n = (uint32_t)n_;
+    auto pick = [&](uint32_t& field, auto&& launch) {
+        float best = 0.f;
+        uint32_t best_t = 0;
+        for (uint32_t t : cand) {
+            field = t;
+            const float ms = time_it(launch);
+            if (best_t == 0 || ms < best) {
+                best = ms;
+                best_t = t;
+            }
+        }
+        field = best_t;
+    };
+    pick(shape_.density, [&] {
+        if (f32_) launch_density_f32(n, shape_.density, kf_, cur_, fb_, lists_, st_);
+        else launch_density(n, shape_.density, kc_, cur_, lists_, st_);
+    });
+    pick(shape_.forces, [&] {
+        if (f32_) launch_forces_f32(n, shape_.forces, kf_, tanks_, cur_, fb_, lists_, 0.f, pos_nx_, vel_nx_, nullptr, st_);
+        else launch_forces(n, shape_.forces, kc_, tanks_, cur_, lists_, true, 0.0, pos_nx_, vel_nx_, st_);
+    });
+    if (!f32_ && prm_.xsph_epsilon != 0.0)
+        pick(shape_.xsph, [&] { launch_xsph(n, shape_.xsph, kc_, cur_, lists_, vel_nx_, st_); });
+    // list-build CTAs per SM: multiples of the resident count
+    {
+        const uint32_t per_sm = std::max<uint32_t>(nlist_prepare(dim_, ucap_), 1u);
+        float best = 0.f;
+        uint32_t best_m = 0;
+        for (uint32_t m : {1u, 2u, 4u, 8u}) {
+            nl_blocks_ = sms_ * per_sm * m;
+            const float ms = time_it([&] {
+                check(cudaMemsetAsync(&sc_->list_used, 0, sizeof(unsigned long long), st_), "memset");
+                launch_nlist(g_, tanks_, kc_, ucap_, nl_blocks_, occ_, cell_start_, cur_, lists_, sc_, st_, f32_);
+            });
+            if (best_m == 0 || ms < best) {
+                best = ms;
+                best_m = per_sm * m;
+            }
+        }
+        list_ctas_per_sm_ = best_m;
+        nl_blocks_ = sms_ * best_m;
+    }
+    check(cudaGetLastError(), "autotune");
+    event_pool_.push_back(a);
+    event_pool_.push_back(b);
+    profiling_ = prof;
+    invalidate_graph();
+    return shapes();
 }
 
 uint32_t World::status() {

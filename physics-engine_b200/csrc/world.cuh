@@ -32,6 +32,7 @@ struct WorldConfig {
     double domain_margin;       // extra grid domain per side, fraction of extent (<0 = 0.25)
     uint32_t domain_margin_cells;  // minimum extra cells per side (0 = 4)
     int precision;              // 0 = f64 (reference bits), 1 = single-precision form
+    int use_graph;              // run() replays captured CUDA graphs of the step
 };
 
 class CudaError : public std::runtime_error {
@@ -41,9 +42,12 @@ class CudaError : public std::runtime_error {
 
 class World {
    public:
+    // tank_offsets (n_tanks + 1 entries, from 0 to n) splits the particles into
+    // independent tanks stepped together; null means one tank.
     World(const WorldParams& prm, const WorldConfig& cfg, int dim, double rest_density, double mass,
           double h, uint64_t n, const double* x, const double* v, const uint8_t* kind,
-          const double* psi, const double* n_out);
+          const double* psi, const double* n_out, const uint64_t* tank_offsets = nullptr,
+          uint32_t n_tanks = 1);
     ~World();
     World(const World&) = delete;
     World& operator=(const World&) = delete;
@@ -62,8 +66,10 @@ class World {
     int dim() const { return dim_; }
     double time() const { return t_; }
     void set_time(double t) { t_ = t; }
-    double sound_speed();
-    void set_sound_speed(double c);
+    double sound_speed();             // tank 0
+    void set_sound_speed(double c);   // every tank
+    uint32_t tanks() const { return n_tanks_; }
+    void get_sound_speeds(double* out);  // one per tank
     const WorldParams& params() const { return prm_; }
     void set_params(const WorldParams& p);
     double mass() const { return mass_; }
@@ -81,8 +87,8 @@ class World {
     void get_neighbour_counts(uint32_t* candidates, uint32_t* in_support);
     uint32_t status();
     void clear_status();
-    // status, largest union, longest list part, union stage capacity, list part
-    // capacity, occupied cells, dense cells, list-build CTAs
+    // status, largest union, list groups the last build asked for, union stage
+    // capacity, list pool groups, occupied cells, dense cells, list-build CTAs
     void capacity_info(uint64_t* out);
 
     // Device views (advanced use: zero-copy access from the same process).
@@ -99,6 +105,15 @@ class World {
     // last reset; synchronises the stream.
     void profile_read(double* ms, uint64_t* count, bool reset);
 
+    // Launch shapes picked by autotune(): block sizes of the density, force and
+    // XSPH passes and the list-build CTAs per SM. Timing repeats idempotent
+    // passes on the current state, so the simulation does not advance.
+    struct Shapes {
+        uint32_t density, forces, xsph, list_ctas_per_sm;
+    };
+    Shapes shapes() const;
+    Shapes autotune();
+
    private:
     void check(cudaError_t e, const char* what);
     void build_grid(const double4* pos_next, const double4* vel_next);
@@ -111,6 +126,10 @@ class World {
     void refresh_f32();
     void configure_lists();
     void alloc_lists(unsigned long long groups);
+    void invalidate_graph() { ++epoch_; }
+    bool graph_capturable() const;
+    bool capture_graph(double dt);
+    void release_graph();
     template <typename T>
     T* alloc(size_t count);
     void gather_orig_vec(const double4* src, double* out);
@@ -125,6 +144,11 @@ class World {
     cudaStream_t st_ = nullptr;
 
     GridDesc g_{};
+    uint32_t n_tanks_ = 1;
+    Tanks tanks_{};
+    std::vector<TankDesc> tank_host_;
+    PassShape shape_{};
+    uint32_t list_ctas_per_sm_ = 0;  // 0: four times the resident count
     StepConst kc_{};
     uint32_t ucap_ = 0, nl_blocks_ = 0, sms_ = 148;
 
@@ -157,6 +181,14 @@ class World {
     bool lists_checked_ = false; // list capacity verified for the current positions
     bool lists_sized_ = false;   // the first list sizing has been done
     uint32_t launches_ = 0;
+
+    // CUDA graph of kGraphSteps steps (the step's buffer rotations return to
+    // their start after six steps)
+    static constexpr uint32_t kGraphSteps = 6;
+    cudaGraphExec_t graph_exec_ = nullptr;
+    double graph_dt_ = 0.0;
+    uint64_t epoch_ = 1, graph_epoch_ = 0;
+    uint32_t graph_launches_ = 0;
 
     struct PhaseRec {
         int phase;

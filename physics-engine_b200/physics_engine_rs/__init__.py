@@ -82,6 +82,7 @@ class _Config(C.Structure):
         ("domain_margin", C.c_double),
         ("domain_margin_cells", C.c_uint32),
         ("precision", C.c_int32),
+        ("use_graph", C.c_int32),
     ]
 
 
@@ -143,6 +144,13 @@ def load_library():
         "pe_fluid_wcsph_create": (C.c_int, [vp, P, C.POINTER(_Config), C.POINTER(vp)]),
         "pe_fluid_wcsph_create_from_arrays": (C.c_int, [P, i32, d, d, d, u64, vp, vp, vp, vp, vp,
                                                         C.POINTER(_Config), C.POINTER(vp)]),
+        "pe_fluid_wcsph_create_batch": (C.c_int, [P, i32, d, d, d, u64, vp, vp, vp, vp, vp, u32, vp,
+                                                  C.POINTER(_Config), C.POINTER(vp)]),
+        "pe_fluid_wcsph_tanks": (C.c_int, [vp, C.POINTER(u32)]),
+        "pe_fluid_wcsph_get_sound_speeds": (C.c_int, [vp, vp, u32]),
+        "pe_fluid_wcsph_autotune": (C.c_int, [vp, vp]),
+        "pe_fluid_wcsph_shapes": (C.c_int, [vp, vp]),
+        "pe_fluid_rng_uniform": (C.c_int, [u64, d, d, u64, vp]),
         "pe_fluid_wcsph_destroy": (None, [vp]),
         "pe_fluid_wcsph_step": (C.c_int, [vp, d]),
         "pe_fluid_wcsph_run": (C.c_int, [vp, d, u64]),
@@ -361,10 +369,11 @@ class WcsphConfig:
     """GPU placement and capacities (no reference counterpart)."""
 
     def __init__(self, device=-1, max_neighbours=0, max_lower=0, domain_margin=-1.0,
-                 domain_margin_cells=0, precision=PRECISION_F64):
+                 domain_margin_cells=0, precision=PRECISION_F64, use_graph=False):
         self.device, self.max_neighbours, self.max_lower = device, max_neighbours, max_lower
         self.domain_margin, self.domain_margin_cells = domain_margin, domain_margin_cells
         self.precision = precision
+        self.use_graph = use_graph
 
     def _to_c(self):
         c = _Config()
@@ -374,6 +383,7 @@ class WcsphConfig:
         c.domain_margin = float(self.domain_margin)
         c.domain_margin_cells = int(self.domain_margin_cells)
         c.precision = int(self.precision)
+        c.use_graph = 1 if self.use_graph else 0
         return c
 
 
@@ -415,6 +425,62 @@ class WcsphWorld:
         self._w = hnd
         self.n, self.dim, self.mass, self.h, self.rest_density = n, int(dim), float(mass), float(h), float(rest_density)
         return self
+
+    @classmethod
+    def from_tanks(cls, params: WcsphParams, tanks, config: WcsphConfig | None = None):
+        """Batched form: independent tanks (a list of `Particles` with the same
+        dim, rest density, mass and h) stepped together by one world. State
+        arrays are the tanks' arrays concatenated in order; `tank_offsets`
+        gives each tank's range."""
+        L = load_library()
+        tanks = list(tanks)
+        if not tanks:
+            raise ValueError("no tanks")
+        p0 = tanks[0]
+        for t in tanks:
+            if (t.dim, t.rest_density, t.mass, t.h) != (p0.dim, p0.rest_density, p0.mass, p0.h):
+                raise ValueError("tanks must share dim, rest density, mass and h")
+        arrs = [t.arrays() for t in tanks]
+        counts = np.array([a["x"].shape[0] for a in arrs], np.uint64)
+        offsets = np.zeros(len(tanks) + 1, np.uint64)
+        offsets[1:] = np.cumsum(counts)
+        cat = {k: np.ascontiguousarray(np.concatenate([a[k] for a in arrs])) for k in arrs[0]}
+        n = int(offsets[-1])
+        self = cls.__new__(cls)
+        self._w = None
+        hnd = C.c_void_p()
+        cfg = config._to_c() if config is not None else None
+        _ok(L.pe_fluid_wcsph_create_batch(
+            C.byref(params._to_c()), int(p0.dim), float(p0.rest_density), float(p0.mass), float(p0.h), n,
+            _ptr(cat["x"]), _ptr(cat["v"]), _ptr(cat["kind"]), _ptr(cat["psi"]), _ptr(cat["n_out"]),
+            len(tanks), _ptr(offsets), C.byref(cfg) if cfg is not None else None, C.byref(hnd)),
+            "create_batch")
+        self._w = hnd
+        self.n, self.dim, self.mass, self.h, self.rest_density = n, p0.dim, p0.mass, p0.h, p0.rest_density
+        self.tank_offsets = offsets
+        return self
+
+    def tanks(self) -> int:
+        t = C.c_uint32()
+        _ok(_lib.pe_fluid_wcsph_tanks(self._w, C.byref(t)), "tanks")
+        return t.value
+
+    def sound_speeds(self):
+        out = np.zeros(self.tanks())
+        _ok(_lib.pe_fluid_wcsph_get_sound_speeds(self._w, _ptr(out), out.size), "get_sound_speeds")
+        return out
+
+    def autotune(self) -> dict:
+        """Pick the passes' block sizes and the list-build CTAs per SM by timing
+        them on the current state (the simulation does not advance)."""
+        out = np.zeros(4, np.uint32)
+        _ok(_lib.pe_fluid_wcsph_autotune(self._w, _ptr(out)), "autotune")
+        return dict(zip(("density", "forces", "xsph", "list_ctas_per_sm"), (int(v) for v in out)))
+
+    def shapes(self) -> dict:
+        out = np.zeros(4, np.uint32)
+        _ok(_lib.pe_fluid_wcsph_shapes(self._w, _ptr(out)), "shapes")
+        return dict(zip(("density", "forces", "xsph", "list_ctas_per_sm"), (int(v) for v in out)))
 
     def close(self):
         if getattr(self, "_w", None) and _lib is not None:

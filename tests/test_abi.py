@@ -160,3 +160,30 @@ def test_world_creation_fails_loudly_without_a_device():
     with pytest.raises(pe.PeError) as e:
         pe.WcsphWorld(p, pe.WcsphParams.water(1000.0, 20.0, (0, 0, -9.81)))
     assert e.value.code == pe.PE_ERR_DEVICE
+
+
+def test_batch_scene_rules():
+    """The seeded batch spec: budgets and extents in range, compact blocks within budget."""
+    from physics_engine_rs import scenes
+
+    spec = scenes.batch_spec(16, seed=3)
+    assert spec == scenes.batch_spec(16, seed=3)
+    for s in spec:
+        assert 2048 <= s["budget"] <= 65536
+        assert all(0.3 <= L <= 1.2 for L in s["box"])
+        nx, ny, nz = s["block"]
+        assert nx * ny * nz <= s["budget"]
+        assert max(s["block"]) <= 2 * min(s["block"])
+        for n, L in zip(s["block"], s["box"]):
+            assert 0.01 * n <= L - 0.01 + 1e-12  # last lattice point keeps a dx gap
+
+
+def test_rng_uniform_is_the_jitter_generator():
+    """Draws come from the same Xoshiro256** stream the jitter uses (seeded alike)."""
+    from physics_engine_rs import scenes
+
+    u = scenes.rng_uniform(0x5EED5EED, -1e-4, 1e-4, 3)
+    p = pe.Particles(3, 1000.0, 1e-3, 0.02)
+    p.push_fluid((0.0, 0.0, 0.0))
+    p.jitter_fluid(0x5EED5EED, 1e-4)
+    assert np.array_equal(p.arrays()["x"][0], u)

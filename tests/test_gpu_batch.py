@@ -1,0 +1,90 @@
+"""Batched form: independent tanks stepped by one world, through the C ABI.
+
+Each tank of a batch must evolve bit for bit as a world created from that
+tank's particles alone (same grid, same list orders, its own persisted sound
+speed), and the CUDA-graph replay and the autotuned launch shapes must not
+change a bit.
+"""
+import numpy as np
+import pytest
+
+import physics_engine_rs as pe
+from helpers import assert_bits_equal, dam_break_params_pe
+from physics_engine_rs import scenes
+
+pytestmark = pytest.mark.gpu
+
+DT = 1e-4
+
+
+def _small_batch(n_tanks=4, seed=11):
+    # budgets 600..3000 particles in 0.2..0.4 m tanks
+    return scenes.batch_dam_break(n_tanks, seed, 600, 3000, 0.2, 0.4)
+
+
+def _state(w):
+    return w.positions(), w.velocities(), w.densities(), w.pressures(), w.accelerations()
+
+
+def _run_separately(tanks, prm, steps, cfg=None):
+    out = []
+    for p in tanks:
+        w = pe.WcsphWorld(p, prm, cfg)
+        w.run(DT, steps)
+        out.append((_state(w), w.sound_speed))
+        w.close()
+    return out
+
+
+@pytest.mark.parametrize("adapt,steps", [(False, 12), (True, 5)])
+def test_batch_matches_tanks_run_alone(adapt, steps):
+    tanks, _ = _small_batch()
+    prm = dam_break_params_pe(adapt_sound_speed=adapt)
+    alone = _run_separately(tanks, prm, steps)
+    b = pe.WcsphWorld.from_tanks(prm, tanks)
+    assert b.tanks() == len(tanks)
+    b.run(DT, steps)
+    xs, vs, rhos, ps, accs = _state(b)
+    cs = b.sound_speeds()
+    off = b.tank_offsets
+    for t, ((x, v, rho, p, a), c) in enumerate(alone):
+        sl = slice(int(off[t]), int(off[t + 1]))
+        assert_bits_equal(xs[sl], x, f"tank {t} x")
+        assert_bits_equal(vs[sl], v, f"tank {t} v")
+        assert_bits_equal(rhos[sl], rho, f"tank {t} rho")
+        assert_bits_equal(ps[sl], p, f"tank {t} p")
+        assert_bits_equal(accs[sl], a, f"tank {t} a")
+        assert_bits_equal([cs[t]], [c], f"tank {t} c")
+    b.close()
+
+
+def test_graph_replay_and_autotune_keep_bits():
+    tanks, _ = _small_batch(3, seed=5)
+    prm = dam_break_params_pe()
+    eager = pe.WcsphWorld.from_tanks(prm, tanks)
+    eager.run(DT, 20)
+    graph = pe.WcsphWorld.from_tanks(prm, tanks, pe.WcsphConfig(use_graph=True))
+    graph.run(DT, 2)
+    shapes = graph.autotune()
+    assert shapes["density"] in (64, 128, 256) and shapes["list_ctas_per_sm"] >= 1
+    graph.run(DT, 18)  # three graph replays of six steps
+    assert graph.t == eager.t
+    for a, b_, what in zip(_state(eager), _state(graph), ("x", "v", "rho", "p", "a")):
+        assert_bits_equal(b_, a, what)
+    eager.close()
+    graph.close()
+
+
+def test_batch_f32_runs_close_to_f64():
+    tanks, _ = _small_batch(3, seed=7)
+    prm = dam_break_params_pe()
+    w64 = pe.WcsphWorld.from_tanks(prm, tanks)
+    w32 = pe.WcsphWorld.from_tanks(prm, tanks, pe.WcsphConfig(precision=pe.PRECISION_F32, use_graph=True))
+    w64.run(DT, 12)
+    w32.run(DT, 12)
+    fluid = np.concatenate([t.arrays()["kind"] for t in tanks]) == 0
+    r64, r32 = w64.densities()[fluid], w32.densities()[fluid]
+    # tolerance of the single-precision form after 12 steps
+    assert np.max(np.abs(r32 - r64) / r64) < 2e-4
+    w64.close()
+    w32.close()
