@@ -14,6 +14,8 @@ namespace {
 
 inline uint32_t blocks_for(uint64_t n, uint32_t t) { return (uint32_t)((n + t - 1) / t); }
 
+constexpr unsigned long long kMaxListGroups = 0xffffffffull;  // 32-bit group indices
+
 // out[orig * 3 + c] = src[slot_of_orig[orig]].{x,y,z}
 __global__ void k_export_vec(uint32_t n, const uint32_t* __restrict__ slot_of_orig,
                              const double4* __restrict__ src, double* __restrict__ out) {
@@ -343,7 +345,7 @@ void World::alloc_lists(unsigned long long groups) {
     lists_.pool = nullptr;
     lists_.pool_groups = 0;
     // group indices are 32-bit: at most 2^32 - 1 groups (64 GB) of entries
-    groups = std::min<unsigned long long>(std::max<unsigned long long>(groups, 1024ull), 0xffffffffull);
+    groups = std::min<unsigned long long>(std::max<unsigned long long>(groups, 1024ull), kMaxListGroups);
     void* p = nullptr;
     check(cudaMalloc(&p, groups * 16ull), "cudaMalloc lists");
     list_allocs_.push_back(p);
@@ -535,7 +537,9 @@ void World::ensure_lists() {
         check(cudaMemsetAsync(lists_.ldesc, 0, sizeof(uint2) * lists_.nslots, st_), "memset");
         check(cudaMemsetAsync(lists_.ncand, 0, sizeof(uint32_t) * lists_.nslots, st_), "memset");
     } else {
-        for (int attempt = 0; attempt < 4; ++attempt) {
+        // Every pass of this loop builds into the current pool, so the loop
+        // always ends with lists built in the pool they describe.
+        for (int attempt = 0;; ++attempt) {
             check(cudaMemsetAsync(&sc_->list_used, 0, sizeof(unsigned long long), st_), "memset");
             prof_begin(kLists);
             launch_nlist(g_, tanks_, kc_, ucap_, nl_blocks_, occ_, cell_start_, cur_, lists_, sc_, st_, f32_);
@@ -550,18 +554,20 @@ void World::ensure_lists() {
             check(cudaStreamSynchronize(st_), "lists");
             const unsigned long long need = hs.list_used, have = lists_.pool_groups;
             const bool overflowed = need > have || (hs.status & kStatusListOverflow);
+            const bool at_max = have >= kMaxListGroups;
             // The very first sizing keeps twice the need (lists grow by ~40%
             // in a few steps when a free-surface start collapses); later
             // checks (after the host moved particles) use the 75% rule that
             // runs poll, so a slowly compressing tank does not reallocate on
-            // every set_positions.
-            const bool fits = lists_sized_ ? need * 4 <= have * 3 : need * 2 <= have;
-            if (!overflowed && fits) {
+            // every set_positions. A pool at its maximum only has to hold the need.
+            const bool fits = at_max ? need <= have
+                                     : (lists_sized_ ? need * 4 <= have * 3 : need * 2 <= have);
+            if (!overflowed && (fits || attempt >= 3)) {
                 lists_checked_ = true;
                 lists_sized_ = true;
                 break;
             }
-            if (overflowed && have >= 0xffffffffull)
+            if (overflowed && (at_max || attempt >= 3))
                 throw std::length_error("neighbour lists exceed the 64 GB pool limit");
             alloc_lists(2 * need);
             if (overflowed) {
@@ -876,7 +882,7 @@ uint32_t World::status() {
     check(cudaStreamSynchronize(st_), "status");
     // Grow the list storage ahead of need: the next list build uses the larger
     // capacity (the current lists are complete as long as no overflow bit is set).
-    if (hs.list_used * 4 > lists_.pool_groups * 3 && lists_.pool_groups < 0xffffffffull) {
+    if (hs.list_used * 4 > lists_.pool_groups * 3 && lists_.pool_groups < kMaxListGroups) {
         alloc_lists(2 * hs.list_used);
         lists_checked_ = false;
     }
