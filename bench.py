@@ -92,6 +92,18 @@ def _dist():
     return ws, rank, local
 
 
+def max_over_ranks(x: float, torch) -> float:
+    """The maximum of x over all ranks (device timings are reported as the
+    slowest rank's); x itself on one rank."""
+    dist = torch.distributed
+    if not dist.is_available() or not dist.is_initialized() or dist.get_world_size() == 1:
+        return x
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], device=dev, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def build_scene(pe, workload):
     (nx, ny, nz), box = WORKLOADS[workload]
     mass = pe.mass_from_spacing(1000.0, DX, 3)
@@ -338,10 +350,7 @@ def run_batched(args, ws, rank, local, torch, pe):
     launches = w.kernel_launches()
     status = w.status()
     cap = w.capacity_info()
-    if ws > 1:
-        tt = torch.tensor([ms], device="cuda")
-        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        ms = float(tt.item())
+    ms = max_over_ranks(ms, torch)
     value = ws * nf * args.steps / (ms / 1e3)
     w.close()
     del w
@@ -461,10 +470,7 @@ def main():
     clocks = sampler.stop()
     status = world.status()
     cap = world.capacity_info()
-    if ws > 1:
-        t = torch.tensor([ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, torch)
     value = ws * nf * args.steps / (ms / 1e3)
 
     # ---- end-to-end through the public API with host buffers ----
@@ -490,10 +496,7 @@ def main():
         e2e_step()
     torch.cuda.synchronize()
     e2e_sec = max(time.perf_counter() - t0, 1e-12)
-    if ws > 1:
-        t = torch.tensor([e2e_sec], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_sec = float(t.item())
+    e2e_sec = max_over_ranks(e2e_sec, torch)
     e2e = ws * nf * args.e2e_steps / e2e_sec
     io_bytes = 2 * world.n * 24
 
