@@ -1,0 +1,59 @@
+/* Learned surrogate of the WCSPH step (no reference counterpart).
+ *
+ * A two-hop message-passing network over the particles' neighbour graph
+ * predicts each fluid particle's acceleration and density rate; BF16 weights
+ * on the tensor cores with fp32 accumulation, trained on the GPU on rollouts
+ * of the plain step. The plain step judges it every k steps and replaces it
+ * when the density error exceeds a bound (pe_fluid_wcsph_run_learned).
+ * Return codes are those of pe_fluid_wcsph.h. */
+#ifndef PE_FLUID_SURROGATE_H
+#define PE_FLUID_SURROGATE_H
+
+#include <stdint.h>
+
+#include "pe_fluid_wcsph.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+#pragma GCC visibility push(default)
+
+typedef struct PeSurrogate PeSurrogate;
+
+/* Network with He-initialised weights from seed; edges join particles closer
+ * than r_msg_over_h * h. */
+int pe_surrogate_create(uint64_t seed, double r_msg_over_h, PeSurrogate** out);
+void pe_surrogate_destroy(PeSurrogate* s);
+
+/* Parameters: linear layers in network order, W is K x N row-major (inputs x
+ * outputs), b has N entries (zeros for the bias-free layers). */
+int pe_surrogate_num_params(PeSurrogate* s, int32_t* n);
+int pe_surrogate_param_info(PeSurrogate* s, int32_t i, char* name, int32_t name_cap, int32_t* K, int32_t* N,
+                            int32_t* has_bias);
+int pe_surrogate_get_param(PeSurrogate* s, int32_t i, float* W, float* b);
+int pe_surrogate_set_param(PeSurrogate* s, int32_t i, const float* W, const float* b);
+/* Gradient of the last pe_surrogate_train_step's loss, same layout. */
+int pe_surrogate_get_grad(PeSurrogate* s, int32_t i, float* W, float* b);
+
+/* An explicit graph: n nodes (features f, n x 8), E edges sorted by
+ * destination (row: n + 1 offsets, src: E sources, xe: E x 16 features). */
+int pe_surrogate_set_graph(PeSurrogate* s, int32_t n, int32_t E, const int32_t* row, const int32_t* src,
+                           const float* f, const float* xe, const uint8_t* fluid);
+int pe_surrogate_set_targets(PeSurrogate* s, const float* t); /* n x 4, normalised */
+int pe_surrogate_forward(PeSurrogate* s, float* y);           /* n x 4, normalised */
+/* Forward, loss (mean over fluid nodes of the squared error), backward; one
+ * Adam step when lr > 0. */
+int pe_surrogate_train_step(PeSurrogate* s, float lr, float* loss);
+
+/* The tensor-core GEMM the network runs on, on caller device buffers (a test
+ * and benchmark entry): C[M x N] = A[M x K] * Bt[N x K]^T (+ bias) (ReLU), bf16
+ * A and Bt with K contiguous, fp32 Cf and/or bf16 Cb; part (splits * M * ldc
+ * floats) when splits > 1. Synchronous on stream; *err = wait-timeout flag. */
+int pe_mlp_gemm_bf16(const void* A, const void* Bt, float* Cf, void* Cb, const float* bias, int M, int N, int K,
+                     int lda, int ldb, int ldc, int relu, int splits, float* part, void* stream, uint32_t* err);
+
+#pragma GCC visibility pop
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -24,7 +24,7 @@ def _declared_functions():
     for fn in os.listdir(HEADER_DIR):
         if fn.endswith(".h"):
             text = open(os.path.join(HEADER_DIR, fn)).read()
-            names |= set(re.findall(r"\b(pe_fluid_[a-z0-9_]+)\s*\(", text))
+            names |= set(re.findall(r"\b(pe_(?:fluid|surrogate|mlp)_[a-z0-9_]+)\s*\(", text))
     return names
 
 

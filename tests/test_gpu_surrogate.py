@@ -1,0 +1,70 @@
+"""The surrogate's GPU forward pass and gradients against the CPU oracle.
+
+Both sides round every GEMM operand to bf16 at the same points, so they differ
+by summation order and by the bf16 rounding flips that order causes, which
+compound through the backward pass. The tolerance is therefore measured, not
+guessed: the oracle is run twice, with fp64 and with fp32 accumulation (two
+legitimate summation orders), and for every parameter the GPU gradient must
+lie within 3x that noise floor (at least 2e-3) of the fp64 oracle, with cosine
+similarity above 0.9995. Outputs and loss: 2e-3 relative."""
+import numpy as np
+import pytest
+
+import surrogate_ref as S
+from physics_engine_rs.surrogate import Surrogate
+from test_oracle_surrogate import random_graph, random_params
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel(a, b):
+    return np.linalg.norm(np.asarray(a, np.float64) - b) / max(np.linalg.norm(b), 1e-30)
+
+
+def test_forward_and_gradients_match_oracle():
+    rng = np.random.default_rng(3)
+    p = {k: v.astype(np.float32) for k, v in random_params(rng).items()}
+    n, E = 300, 2400
+    f, xe, dst, src, fluid, t = random_graph(rng, n, E)
+    row = np.searchsorted(dst, np.arange(n + 1)).astype(np.int32)
+    s = Surrogate(seed=1)
+    s.set_params(p)
+    s.set_graph(f, xe, row, src, fluid)
+    s.set_targets(t)
+    y = s.forward()
+    net = S.Net({k: v.astype(np.float64) for k, v in p.items()})
+    # the oracle reads the same bf16-rounded inputs
+    fb, xb = S.bf16(f), S.bf16(xe)
+    loss_ref, y_ref, g_ref = net.loss_and_grads(fb, xb, dst, src, fluid, t)
+    assert _rel(y, y_ref) < 2e-3
+    loss = s.train_step(0.0)
+    assert abs(loss - loss_ref) <= 2e-3 * abs(loss_ref)
+    g = s.get_params(grads=True)
+    # noise floor: the same oracle with fp32 accumulation
+    exact_gemm = S.gemm
+    S.gemm = lambda a, b: (np.asarray(S.bf16(a), np.float32) @ np.asarray(S.bf16(b), np.float32)).astype(
+        np.float64)
+    try:
+        _, _, g_f32 = net.loss_and_grads(fb, xb, dst, src, fluid, t)
+    finally:
+        S.gemm = exact_gemm
+    for k in g_ref:
+        floor = max(_rel(g_f32[k], g_ref[k]), 2e-3 / 3)
+        err = _rel(g[k], g_ref[k])
+        assert err <= 3 * floor, (k, err, floor)
+        a, b = np.ravel(g[k]).astype(np.float64), np.ravel(g_ref[k])
+        assert a @ b / (np.linalg.norm(a) * np.linalg.norm(b)) > 0.9995, k
+
+
+def test_adam_steps_reduce_the_loss():
+    rng = np.random.default_rng(4)
+    n, E = 400, 3000
+    f, xe, dst, src, fluid, t = random_graph(rng, n, E)
+    row = np.searchsorted(dst, np.arange(n + 1)).astype(np.int32)
+    s = Surrogate(seed=2)
+    s.set_graph(f, xe, row, src, fluid)
+    s.set_targets(t * 0.5)
+    first = s.train_step(1e-3)
+    for _ in range(60):
+        last = s.train_step(1e-3)
+    assert last < 0.5 * first
