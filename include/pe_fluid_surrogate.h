@@ -45,6 +45,32 @@ int pe_surrogate_forward(PeSurrogate* s, float* y);           /* n x 4, normalis
  * Adam step when lr > 0. */
 int pe_surrogate_train_step(PeSurrogate* s, float lr, float* loss);
 
+/* Target normalisation (per output: mean and standard deviation). */
+int pe_surrogate_get_stats(PeSurrogate* s, float mean[4], float std_[4]);
+int pe_surrogate_set_stats(PeSurrogate* s, const float mean[4], const float std_[4]);
+
+/* Training on the plain step: the graph of slots [slot_begin, slot_end) of a
+ * world (a tank's range, pe_fluid_wcsph_tank_range), then, after the world
+ * took one plain step of dt, that graph's targets (velocity change and density
+ * change per dt); update_stats refits the normalisation first. */
+int pe_surrogate_graph_from_world(PeSurrogate* s, PeWcsph* w, uint32_t slot_begin, uint32_t slot_end);
+int pe_surrogate_targets_from_world(PeSurrogate* s, PeWcsph* w, double dt, int32_t update_stats);
+int pe_fluid_wcsph_tank_range(PeWcsph* w, uint32_t tank, uint32_t* slot_begin, uint32_t* slot_end);
+
+/* One learned step of all particles: the network's acceleration and density
+ * rate replace the pressure, viscosity and XSPH passes (v += dt a, x += dt v,
+ * rho += dt drho/dt). */
+int pe_fluid_wcsph_step_learned(PeWcsph* w, PeSurrogate* s, double dt);
+/* The plain step's SPH density of the current positions replaces the carried
+ * densities; *max_rel_error = max over fluid of |carried - SPH| / SPH. */
+int pe_fluid_wcsph_judge_density(PeWcsph* w, double* max_rel_error);
+/* steps in windows of judge_every learned steps; after each window the plain
+ * density judges it, and a window whose error exceeds bound is rerun from its
+ * start with the plain step. out (may be NULL) = {windows, fallbacks, learned
+ * steps, plain steps, largest error, last error}. */
+int pe_fluid_wcsph_run_learned(PeWcsph* w, PeSurrogate* s, double dt, uint64_t steps, uint32_t judge_every,
+                               double bound, double out[6]);
+
 /* The tensor-core GEMM the network runs on, on caller device buffers (a test
  * and benchmark entry): C[M x N] = A[M x K] * Bt[N x K]^T (+ bias) (ReLU), bf16
  * A and Bt with K contiguous, fp32 Cf and/or bf16 Cb; part (splits * M * ldc

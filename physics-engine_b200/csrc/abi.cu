@@ -11,6 +11,7 @@
 
 #include "../../include/pe_fluid_wcsph.h"
 #include "pe_math.cuh"
+#include "handles.cuh"
 #include "world.cuh"
 
 struct PeParticles {
@@ -21,9 +22,6 @@ struct PeParticles {
     uint64_t len() const { return kind.size(); }
 };
 
-struct PeWcsph {
-    pe::World* world;
-};
 
 namespace {
 

@@ -264,6 +264,7 @@ Surrogate::~Surrogate() {
     for (void* p : graph_allocs_) cudaFree(p);
     for (void* p : act_allocs_) cudaFree(p);
     if (part_) cudaFree(part_);
+    if (scan_tmp_) cudaFree(scan_tmp_);
     if (own_stream_ && st_) cudaStreamDestroy(st_);
 }
 
@@ -364,6 +365,7 @@ void Surrogate::ensure_graph(int n, int E) {
     cu(cudaStreamSynchronize(st_), "graph");
     for (void* p : graph_allocs_) cudaFree(p);
     graph_allocs_.clear();
+    if (scan_tmp_) cudaFree(scan_tmp_);
     const int cn = std::max(n, g_.cap_n), ce = std::max(E, g_.cap_e);
     auto ga = [&](size_t bytes) {
         void* p = nullptr;
@@ -378,17 +380,23 @@ void Surrogate::ensure_graph(int n, int E) {
     g_.f = static_cast<__nv_bfloat16*>(ga((size_t)cn * kNodeFeat * 2));
     g_.fluid = static_cast<uint8_t*>(ga((size_t)cn));
     node_orig_ = static_cast<uint32_t*>(ga((size_t)cn * 4));
-    node_v_ = static_cast<float*>(ga((size_t)cn * 4 * 4));
+    node_v_ = static_cast<double*>(ga((size_t)cn * 4 * 8));
     target_ = static_cast<float*>(ga((size_t)cn * kOut * 4));
+    raw_t_ = static_cast<float*>(ga((size_t)cn * kOut * 4));
+    cnt_ = static_cast<int*>(ga((size_t)(cn + 1) * 4));
+    scan_tmp_ = nullptr;
+    scan_bytes_ = 0;
     g_.cap_n = cn;
     g_.cap_e = ce;
     g_.n = n;
     g_.E = E;
 }
 
-void Surrogate::ensure_acts() {
+void Surrogate::ensure_acts(bool train) {
+    // Inference keeps one hop's edge activations and no backward buffers: at a
+    // million particles (~3e7 edges) that is ~1.5 KB per edge instead of ~4.6.
     const int n = g_.n, E = g_.E;
-    if (n <= act_n_ && E <= act_e_) return;
+    if (n <= act_n_ && E <= act_e_ && (act_train_ || !train)) return;
     cu(cudaStreamSynchronize(st_), "acts");
     for (void* p : act_allocs_) cudaFree(p);
     act_allocs_.clear();
@@ -414,8 +422,8 @@ void Surrogate::ensure_acts() {
     Q_ = fa(cn * W);
     ZE_ = fa(ce * W);
     for (int l = 0; l < 2; ++l) {
-        eh1_[l] = ba(ce * W);
-        eh2_[l] = ba(ce * W);
+        eh1_[l] = (l == 0 || train) ? ba(ce * W) : eh1_[0];
+        eh2_[l] = (l == 0 || train) ? ba(ce * W) : eh2_[0];
         xn_[l] = ba(cn * 2 * W);
         na1_[l] = ba(cn * W);
         na2_[l] = ba(cn * W);
@@ -430,18 +438,19 @@ void Surrogate::ensure_acts() {
     dH_ = fa(cn * W);
     dHp_ = fa(cn * W);
     dXN_ = fa(cn * 2 * W);
-    dE_ = fa(ce * W);
-    dE2_ = fa(ce * W);
+    dE_ = train ? fa(ce * W) : nullptr;
+    dE2_ = train ? fa(ce * W) : nullptr;
     dP_ = fa(cn * W);
     dQ_ = fa(cn * W);
     dT1_ = fa(cn * W);
     dT2_ = fa(cn * W);
-    const size_t rows = (size_t)std::max(cn, ce);
-    gb16_ = ba(rows * 2 * W);
-    gbT_ = ba(rows * 2 * W);
-    xT_ = ba(rows * 2 * W);
+    const size_t rows = train ? (size_t)std::max(cn, ce) : 0;
+    gb16_ = train ? ba(rows * 2 * W) : nullptr;
+    gbT_ = train ? ba(rows * 2 * W) : nullptr;
+    xT_ = train ? ba(rows * 2 * W) : nullptr;
     act_n_ = cn;
     act_e_ = ce;
+    act_train_ = train;
 }
 
 void Surrogate::gemm(const __nv_bfloat16* A, int lda, const __nv_bfloat16* Bt, int ldb, int M, int N, int K,
@@ -476,8 +485,8 @@ void Surrogate::mlp_fwd(int first, const __nv_bfloat16* X, int R, __nv_bfloat16*
     linear_fwd(layers_[first + 2], A2, R, Yf, nullptr, false);
 }
 
-void Surrogate::forward(bool /*keep_for_backward*/) {
-    ensure_acts();
+void Surrogate::forward(bool keep_for_backward) {
+    ensure_acts(keep_for_backward);
     const int n = g_.n, E = g_.E;
     const size_t nW = (size_t)n * kWidth, eW = (size_t)E * kWidth;
     mlp_fwd(0, g_.f, n, enc_a1_, enc_a2_, h_);

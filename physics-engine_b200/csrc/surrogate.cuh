@@ -87,7 +87,8 @@ class Surrogate {
     // lists must be current); keeps the nodes' original indices for targets
     void graph_from_world(World& w, uint32_t s0, uint32_t s1);
     // normalised targets of the current graph's fluid nodes from w's state one
-    // step of dt later; with update_stats the normalisation is refit first
+    // step of dt later; with update_stats these targets join the moments the
+    // normalisation is fitted on (all update_stats calls so far) and it is refit
     void targets_from_world(World& w, double dt, bool update_stats);
     // predicted acceleration and density rate per slot of w (whole world),
     // written to acc (double4 per slot, w = drho/dt)
@@ -103,7 +104,7 @@ class Surrogate {
    private:
     void alloc_params(uint64_t seed);
     void ensure_graph(int n, int E);
-    void ensure_acts();
+    void ensure_acts(bool train);
     void refresh_bf16(Linear& L);
     void gemm(const __nv_bfloat16* A, int lda, const __nv_bfloat16* Bt, int ldb, int M, int N, int K, float* Cf,
               __nv_bfloat16* Cb, int ldc, const float* bias, bool relu, int splits = 1);
@@ -125,6 +126,8 @@ class Surrogate {
     bool own_stream_ = false;
     double r_msg_over_h_;
     SurrogateStats stats_{};
+    double st_sum_[kOut] = {}, st_sq_[kOut] = {};  // moments of every target fitted so far
+    double st_count_ = 0.0;
     int adam_t_ = 0;
     uint32_t* err_ = nullptr;
     float* loss_ = nullptr;
@@ -133,10 +136,15 @@ class Surrogate {
 
     MsgGraph g_;
     uint32_t* node_orig_ = nullptr;   // original index of each graph node
-    float* node_v_ = nullptr;         // [n x 4]: velocity, density at the graph's time
+    double* node_v_ = nullptr;        // [n x 4]: velocity, density at the graph's time
+    float* raw_t_ = nullptr;          // [n x 4] targets before normalisation
+    int* cnt_ = nullptr;              // [n + 1] edges per node, then CSR offsets
+    void* scan_tmp_ = nullptr;
+    size_t scan_bytes_ = 0;
     float* target_ = nullptr;         // [n x 4] normalised targets
     // activations (rows: nodes or edges)
     int act_n_ = 0, act_e_ = 0;
+    bool act_train_ = false;
     __nv_bfloat16 *enc_a1_ = nullptr, *enc_a2_ = nullptr;
     float* h_ = nullptr;                   // latent fp32 [n x 128]
     __nv_bfloat16* hb_[3] = {};            // latent bf16 per level

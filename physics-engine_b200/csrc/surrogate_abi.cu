@@ -1,9 +1,11 @@
 // C ABI of the learned surrogate (include/pe_fluid_surrogate.h).
+#include <cmath>
 #include <cstring>
 #include <new>
 #include <stdexcept>
 
 #include "../../include/pe_fluid_surrogate.h"
+#include "handles.cuh"
 #include "surrogate.cuh"
 
 struct PeSurrogate {
@@ -18,6 +20,8 @@ int guard_s(F&& f) {
         return f();
     } catch (const std::bad_alloc&) {
         return PE_ERR_DEVICE;
+    } catch (const std::length_error&) {
+        return PE_ERR_BOUNDS;
     } catch (const std::out_of_range&) {
         return PE_ERR_BOUNDS;
     } catch (const std::invalid_argument&) {
@@ -133,5 +137,95 @@ int pe_surrogate_train_step(PeSurrogate* s, float lr, float* loss) {
         const float l = s->s->train_step(lr);
         if (loss) *loss = l;
         return s->s->device_error() ? PE_ERR_DEVICE : PE_OK;
+    });
+}
+
+int pe_surrogate_get_stats(PeSurrogate* s, float mean[4], float std_[4]) {
+    if (!s || !mean || !std_) return PE_ERR_NULL;
+    const pe::SurrogateStats& st = s->s->stats();
+    for (int c = 0; c < 4; ++c) {
+        mean[c] = st.mean[c];
+        std_[c] = st.std[c];
+    }
+    return PE_OK;
+}
+
+int pe_surrogate_set_stats(PeSurrogate* s, const float mean[4], const float std_[4]) {
+    if (!s || !mean || !std_) return PE_ERR_NULL;
+    pe::SurrogateStats st;
+    for (int c = 0; c < 4; ++c) {
+        if (!(std_[c] > 0.f) || !std::isfinite(mean[c])) return PE_ERR_ARG;
+        st.mean[c] = mean[c];
+        st.std[c] = std_[c];
+    }
+    s->s->set_stats(st);
+    return PE_OK;
+}
+
+int pe_surrogate_graph_from_world(PeSurrogate* s, PeWcsph* w, uint32_t slot_begin, uint32_t slot_end) {
+    if (!s || !w) return PE_ERR_NULL;
+    if (slot_end <= slot_begin || slot_end > w->world->len()) return PE_ERR_BOUNDS;
+    return guard_s([&] {
+        s->s->graph_from_world(*w->world, slot_begin, slot_end);
+        return PE_OK;
+    });
+}
+
+int pe_surrogate_targets_from_world(PeSurrogate* s, PeWcsph* w, double dt, int32_t update_stats) {
+    if (!s || !w) return PE_ERR_NULL;
+    if (!(std::isfinite(dt) && dt > 0.0)) return PE_ERR_ARG;
+    return guard_s([&] {
+        s->s->targets_from_world(*w->world, dt, update_stats != 0);
+        return PE_OK;
+    });
+}
+
+int pe_fluid_wcsph_tank_range(PeWcsph* w, uint32_t tank, uint32_t* slot_begin, uint32_t* slot_end) {
+    if (!w || !slot_begin || !slot_end) return PE_ERR_NULL;
+    if (tank >= w->world->tanks()) return PE_ERR_BOUNDS;
+    *slot_begin = w->world->tank_slot_begin(tank);
+    *slot_end = w->world->tank_slot_end(tank);
+    return PE_OK;
+}
+
+int pe_fluid_wcsph_step_learned(PeWcsph* w, PeSurrogate* s, double dt) {
+    if (!w || !s) return PE_ERR_NULL;
+    if (!(std::isfinite(dt) && dt > 0.0)) return PE_ERR_ARG;
+    return guard_s([&] {
+        w->world->step_learned(*s->s, dt);
+        const uint32_t st = w->world->status();
+        return (st & (PE_STATUS_DOMAIN | PE_STATUS_NEIGHBOUR_OVERFLOW)) ? PE_ERR_BOUNDS
+               : (st & PE_STATUS_NONFINITE)                            ? PE_ERR_ARG
+                                                                       : PE_OK;
+    });
+}
+
+int pe_fluid_wcsph_judge_density(PeWcsph* w, double* max_rel_error) {
+    if (!w || !max_rel_error) return PE_ERR_NULL;
+    return guard_s([&] {
+        *max_rel_error = w->world->judge_density();
+        return PE_OK;
+    });
+}
+
+int pe_fluid_wcsph_run_learned(PeWcsph* w, PeSurrogate* s, double dt, uint64_t steps, uint32_t judge_every,
+                               double bound, double out[6]) {
+    if (!w || !s) return PE_ERR_NULL;
+    if (!(std::isfinite(dt) && dt > 0.0) || !(bound > 0.0) || judge_every == 0) return PE_ERR_ARG;
+    return guard_s([&] {
+        pe::World::LearnedStats st{};
+        w->world->run_learned(*s->s, dt, steps, judge_every, bound, &st);
+        if (out) {
+            out[0] = (double)st.windows;
+            out[1] = (double)st.fallbacks;
+            out[2] = (double)st.learned_steps;
+            out[3] = (double)st.plain_steps;
+            out[4] = st.max_error;
+            out[5] = st.last_error;
+        }
+        const uint32_t code = w->world->status();
+        return (code & (PE_STATUS_DOMAIN | PE_STATUS_NEIGHBOUR_OVERFLOW)) ? PE_ERR_BOUNDS
+               : (code & PE_STATUS_NONFINITE)                            ? PE_ERR_ARG
+                                                                         : PE_OK;
     });
 }

@@ -358,6 +358,8 @@ void World::alloc_lists(unsigned long long groups) {
 World::~World() {
     if (st_) cudaStreamSynchronize(st_);
     release_graph();
+    for (void* p : {(void*)ck_pos_, (void*)ck_vel_, (void*)ck_p_, (void*)judge_err_})
+        if (p) cudaFree(p);
     for (void* p : list_allocs_) cudaFree(p);
     for (auto& r : recs_) {
         cudaEventDestroy(r.a);
@@ -529,8 +531,10 @@ void World::build_grid(const double4* pos_next, const double4* vel_next) {
     check(cudaGetLastError(), "grid build");
 }
 
-void World::ensure_lists() {
-    if (lists_valid_) return;
+void World::ensure_lists(bool visit_only) {
+    // the f32 form and the learned step read the visit list only
+    const bool build_visit_only = f32_ || visit_only;
+    if (lists_valid_ && (lists_full_ || build_visit_only)) return;
     if (!grid_built_) {
         // No grid yet: every neighbour query of the reference returns nothing.
         check(cudaMemsetAsync(lists_.desc, 0, sizeof(uint4) * lists_.nslots, st_), "memset");
@@ -542,9 +546,10 @@ void World::ensure_lists() {
         for (int attempt = 0;; ++attempt) {
             check(cudaMemsetAsync(&sc_->list_used, 0, sizeof(unsigned long long), st_), "memset");
             prof_begin(kLists);
-            launch_nlist(g_, tanks_, kc_, ucap_, nl_blocks_, occ_, cell_start_, cur_, lists_, sc_, st_, f32_);
+            launch_nlist(g_, tanks_, kc_, ucap_, nl_blocks_, occ_, cell_start_, cur_, lists_, sc_, st_,
+                         build_visit_only);
             prof_end();
-            launches_ += 1;
+            launches_ += build_visit_only ? 1 : 2;
             check(cudaGetLastError(), "neighbour lists");
             if (lists_checked_) break;
             // First build for these positions: size the pool from what the
@@ -581,10 +586,11 @@ void World::ensure_lists() {
     }
     check(cudaGetLastError(), "neighbour lists");
     lists_valid_ = true;
+    lists_full_ = grid_built_ && !build_visit_only;
 }
 
-void World::run_density() {
-    ensure_lists();
+void World::run_density(bool visit_only) {
+    ensure_lists(visit_only);
     prof_begin(kDensity);
     if (f32_) launch_density_f32((uint32_t)n_, shape_.density, kf_, cur_, fb_, lists_, st_);
     else launch_density((uint32_t)n_, shape_.density, kc_, cur_, lists_, st_);
@@ -698,7 +704,9 @@ void World::run(double dt, uint64_t steps) {
     uint64_t s = 0, last_poll = 0;
     while (s < steps) {
         if (cfg_.use_graph && steps - s >= kGraphSteps && graph_capturable()) {
-            if (!graph_exec_ || graph_dt_ != dt || graph_epoch_ != epoch_) capture_graph(dt);
+            if (!graph_exec_ || graph_dt_ != dt || graph_epoch_ != epoch_ ||
+                !same_rotation(graph_rot_, rotation()))
+                capture_graph(dt);
             if (graph_exec_) {
                 check(cudaGraphLaunch(graph_exec_, st_), "graph launch");
                 s += kGraphSteps;
@@ -737,8 +745,14 @@ void World::release_graph() {
 // (buffer rotations, time, launch count) is undone afterwards and replayed
 // per graph launch; the rotations return to their start after kGraphSteps
 // steps, which is checked here.
+bool World::same_rotation(const Rotation& a, const Rotation& b) {
+    return std::memcmp(&a.cur, &b.cur, sizeof(a.cur)) == 0 && std::memcmp(&a.alt, &b.alt, sizeof(a.alt)) == 0 &&
+           a.vel_nx == b.vel_nx && std::memcmp(&a.fb, &b.fb, sizeof(a.fb)) == 0 && a.velf_alt == b.velf_alt;
+}
+
 bool World::capture_graph(double dt) {
     release_graph();
+    graph_rot_ = rotation();
     const StateBufs cur0 = cur_, alt0 = alt_;
     double4* const vel_nx0 = vel_nx_;
     const F32Bufs fb0 = fb_;
@@ -858,7 +872,8 @@ World::Shapes World::autotune() {
             nl_blocks_ = sms_ * per_sm * m;
             const float ms = time_it([&] {
                 check(cudaMemsetAsync(&sc_->list_used, 0, sizeof(unsigned long long), st_), "memset");
-                launch_nlist(g_, tanks_, kc_, ucap_, nl_blocks_, occ_, cell_start_, cur_, lists_, sc_, st_, f32_);
+                launch_nlist(g_, tanks_, kc_, ucap_, nl_blocks_, occ_, cell_start_, cur_, lists_, sc_, st_,
+                             !lists_full_);
             });
             if (best_m == 0 || ms < best) {
                 best = ms;

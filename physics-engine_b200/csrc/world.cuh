@@ -40,6 +40,8 @@ class CudaError : public std::runtime_error {
     explicit CudaError(const std::string& s) : std::runtime_error(s) {}
 };
 
+class Surrogate;
+
 class World {
    public:
     // tank_offsets (n_tanks + 1 entries, from 0 to n) splits the particles into
@@ -114,11 +116,41 @@ class World {
     Shapes shapes() const;
     Shapes autotune();
 
+    // ---- learned surrogate (surrogate.cuh) ----
+    // One step with the network's acceleration and density rate in place of
+    // the pressure, viscosity and XSPH passes: v += dt a, x += dt v,
+    // rho += dt drho/dt (fluid particles).
+    void step_learned(Surrogate& s, double dt);
+    // Rebuilds the grid and computes the SPH density of the current positions
+    // (the plain step's density); returns the largest relative difference of
+    // the carried fluid densities from it and keeps the SPH densities.
+    double judge_density();
+    struct LearnedStats {
+        uint64_t windows, fallbacks, learned_steps, plain_steps;
+        double max_error, last_error;
+    };
+    // steps in windows of judge_every: each window runs learned steps from a
+    // checkpoint, is judged, and is replaced by plain steps from the
+    // checkpoint when the density error exceeds bound
+    void run_learned(Surrogate& s, double dt, uint64_t steps, uint32_t judge_every, double bound,
+                     LearnedStats* st);
+    uint32_t tank_slot_begin(uint32_t t) const { return tank_host_.at(t).slot_begin; }
+    uint32_t tank_slot_end(uint32_t t) const {
+        return t + 1 < n_tanks_ ? tank_host_[t + 1].slot_begin : (uint32_t)n_;
+    }
+
    private:
+    friend class Surrogate;
+    void save_checkpoint();
+    void restore_checkpoint();
+    double4 *ck_pos_ = nullptr, *ck_vel_ = nullptr;
+    double* ck_p_ = nullptr;
+    double ck_t_ = 0.0;
+    float* judge_err_ = nullptr;
     void check(cudaError_t e, const char* what);
     void build_grid(const double4* pos_next, const double4* vel_next);
-    void ensure_lists();
-    void run_density();
+    void ensure_lists(bool visit_only = false);
+    void run_density(bool visit_only = false);
     void run_pressure();
     void run_forces(bool integrate, double dt);
     void run_xsph();
@@ -180,6 +212,7 @@ class World {
     bool lists_valid_ = false;   // neighbour lists match the grid and positions
     bool lists_checked_ = false; // list capacity verified for the current positions
     bool lists_sized_ = false;   // the first list sizing has been done
+    bool lists_full_ = false;    // the last build wrote upper and lower lists too
     uint32_t launches_ = 0;
 
     // CUDA graph of kGraphSteps steps (the step's buffer rotations return to
@@ -189,6 +222,17 @@ class World {
     double graph_dt_ = 0.0;
     uint64_t epoch_ = 1, graph_epoch_ = 0;
     uint32_t graph_launches_ = 0;
+    // the buffer rotation the graph was captured in; a replay from any other
+    // rotation would read and write the wrong buffers
+    struct Rotation {
+        StateBufs cur, alt;
+        double4* vel_nx;
+        F32Bufs fb;
+        float4* velf_alt;
+    };
+    Rotation graph_rot_{};
+    Rotation rotation() const { return Rotation{cur_, alt_, vel_nx_, fb_, velf_alt_}; }
+    static bool same_rotation(const Rotation& a, const Rotation& b);
 
     struct PhaseRec {
         int phase;

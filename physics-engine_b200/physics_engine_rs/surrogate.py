@@ -21,6 +21,16 @@ _SIGS = {
     "pe_surrogate_set_targets": (C.c_int, [C.c_void_p, C.c_void_p]),
     "pe_surrogate_forward": (C.c_int, [C.c_void_p, C.c_void_p]),
     "pe_surrogate_train_step": (C.c_int, [C.c_void_p, C.c_float, C.POINTER(C.c_float)]),
+    "pe_surrogate_get_stats": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "pe_surrogate_set_stats": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "pe_surrogate_graph_from_world": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32]),
+    "pe_surrogate_targets_from_world": (C.c_int, [C.c_void_p, C.c_void_p, C.c_double, C.c_int32]),
+    "pe_fluid_wcsph_tank_range": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(C.c_uint32),
+                                            C.POINTER(C.c_uint32)]),
+    "pe_fluid_wcsph_step_learned": (C.c_int, [C.c_void_p, C.c_void_p, C.c_double]),
+    "pe_fluid_wcsph_judge_density": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
+    "pe_fluid_wcsph_run_learned": (C.c_int, [C.c_void_p, C.c_void_p, C.c_double, C.c_uint64, C.c_uint32,
+                                             C.c_double, C.c_void_p]),
 }
 
 
@@ -108,3 +118,85 @@ class Surrogate:
         loss = C.c_float()
         _ok(self._L.pe_surrogate_train_step(self._s, float(lr), C.byref(loss)), "train_step")
         return loss.value
+
+    # ---- normalisation, persistence ----
+    def stats(self):
+        m, sd = np.zeros(4, np.float32), np.zeros(4, np.float32)
+        _ok(self._L.pe_surrogate_get_stats(self._s, _ptr(m), _ptr(sd)), "get_stats")
+        return m, sd
+
+    def set_stats(self, mean, std):
+        m, sd = np.ascontiguousarray(mean, np.float32), np.ascontiguousarray(std, np.float32)
+        _ok(self._L.pe_surrogate_set_stats(self._s, _ptr(m), _ptr(sd)), "set_stats")
+
+    def save(self, path):
+        m, sd = self.stats()
+        np.savez(path, __mean=m, __std=sd, **self.get_params())
+
+    def load(self, path):
+        d = np.load(path)
+        self.set_params({k: d[k] for k in d.files if not k.startswith("__")})
+        self.set_stats(d["__mean"], d["__std"])
+
+    # ---- training on a world's plain steps ----
+    def graph_from_world(self, world, slot_begin: int, slot_end: int):
+        _ok(self._L.pe_surrogate_graph_from_world(self._s, world._w, int(slot_begin), int(slot_end)),
+            "graph_from_world")
+        self.n = int(slot_end) - int(slot_begin)
+
+    def targets_from_world(self, world, dt: float, update_stats: bool = False):
+        _ok(self._L.pe_surrogate_targets_from_world(self._s, world._w, float(dt), 1 if update_stats else 0),
+            "targets_from_world")
+
+
+def tank_range(world, tank: int):
+    L = _lib()
+    a, b = C.c_uint32(), C.c_uint32()
+    _ok(L.pe_fluid_wcsph_tank_range(world._w, int(tank), C.byref(a), C.byref(b)), "tank_range")
+    return a.value, b.value
+
+
+def step_learned(world, surrogate: Surrogate, dt: float):
+    _ok(_lib().pe_fluid_wcsph_step_learned(world._w, surrogate._s, float(dt)), "step_learned")
+
+
+def judge_density(world) -> float:
+    e = C.c_double()
+    _ok(_lib().pe_fluid_wcsph_judge_density(world._w, C.byref(e)), "judge_density")
+    return e.value
+
+
+def run_learned(world, surrogate: Surrogate, dt: float, steps: int, judge_every: int = 10,
+                bound: float = 0.01) -> dict:
+    """Learned steps judged every `judge_every` steps by the plain density; a
+    window whose relative density error exceeds `bound` is rerun with the
+    plain step from its start."""
+    out = np.zeros(6)
+    _ok(_lib().pe_fluid_wcsph_run_learned(world._w, surrogate._s, float(dt), int(steps), int(judge_every),
+                                          float(bound), _ptr(out)), "run_learned")
+    return dict(windows=int(out[0]), fallbacks=int(out[1]), learned_steps=int(out[2]),
+                plain_steps=int(out[3]), max_error=float(out[4]), last_error=float(out[5]))
+
+
+def train_on_rollouts(surrogate: Surrogate, world, dt: float, steps: int, iters_per_step: int = 2,
+                      lr: float = 1e-3, stat_steps: int = 20, log=None):
+    """Online training on a (batched) world's plain rollout. The first
+    `stat_steps` plain steps only fit the target normalisation (every tank in
+    turn); then, before each plain step the graph of one tank (in turn) is
+    taken, after it the targets, then `iters_per_step` Adam steps. Returns the
+    losses."""
+    tanks = world.tanks()
+    losses = []
+    for k in range(stat_steps + steps):
+        a, b = tank_range(world, k % tanks)
+        surrogate.graph_from_world(world, a, b)
+        world.step(dt)
+        fitting = k < stat_steps
+        surrogate.targets_from_world(world, dt, update_stats=fitting)
+        if fitting:
+            continue
+        for _ in range(iters_per_step):
+            losses.append(surrogate.train_step(lr))
+        if log and (k - stat_steps) % 50 == 0:
+            log(k - stat_steps, losses[-1])
+    return losses
