@@ -61,11 +61,16 @@ def _args():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="dam_break_1m")
     ap.add_argument("--e2e-steps", type=int, default=5)
-    ap.add_argument("--form", choices=("plain", "f32", "batched"), default="plain",
+    ap.add_argument("--train-tanks", type=int, default=16,
+                    help="learned form: seeded 64k-particle tanks rolled out for training")
+    ap.add_argument("--train-steps", type=int, default=300, help="learned form: plain steps trained on")
+    ap.add_argument("--rollout-steps", type=int, default=200, help="learned form: steps of the 1M rollout")
+    ap.add_argument("--form", choices=("plain", "f32", "batched", "learned"), default="plain",
                     help="plain: the f64 step (reference bits); f32: the single-precision "
                          "form, timed and compared with the f64 step after the same steps; "
                          "batched: 512 seeded tanks in one world against a loop of "
-                         "single-tank worlds")
+                         "single-tank worlds; learned: the surrogate trained on plain "
+                         "rollouts, judged every 10 steps, against the plain step")
     ap.add_argument("--precision", choices=("f64", "f32"), default="f64",
                     help="arithmetic of the batched form")
     ap.add_argument("--tanks", type=int, default=512)
@@ -402,13 +407,95 @@ def run_batched(args, ws, rank, local, torch, pe):
         print(json.dumps(line), flush=True)
 
 
+def run_learned_form(args, ws, rank, local, torch, pe):
+    """The learned surrogate: trained online on plain rollouts of seeded
+    64k-particle tanks (tank extents 0.45..1.0 m), then the 1M dam break run
+    with learned steps judged every 10 steps by the plain SPH density (a window
+    whose relative density error exceeds 1% is rerun with the plain step),
+    next to the plain f64 run of the same steps."""
+    import numpy as np
+    from physics_engine_rs import scenes
+    from physics_engine_rs import surrogate as S
+
+    prm = pe.WcsphParams.water(1000.0, 20.0, (0.0, 0.0, -9.81))
+    prm.adapt_sound_speed = False
+    # ---- training ----
+    tanks, _ = scenes.batch_dam_break(args.train_tanks, SEED + 7, 64000, 64000, 0.45, 1.0)
+    train = pe.WcsphWorld.from_tanks(prm, tanks, pe.WcsphConfig(device=local))
+    del tanks
+    sur = S.Surrogate(seed=SEED)
+    t0 = time.perf_counter()
+    losses = S.train_on_rollouts(sur, train, DT, args.train_steps, iters_per_step=2, lr=5e-4, stat_steps=20)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+    train.close()
+    # ---- rollouts at 1M ----
+    ps, _, nf = build_scene(pe, args.workload)
+    fluid = ps.arrays()["kind"] == 0
+    plain = pe.WcsphWorld(ps, prm, pe.WcsphConfig(device=local))
+    learned = pe.WcsphWorld(ps, prm, pe.WcsphConfig(device=local))
+    del ps
+    steps = args.rollout_steps
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    plain.run(DT, steps)
+    torch.cuda.synchronize()
+    plain_s = time.perf_counter() - t0
+    sampler = ClockSampler(local)
+    sampler.start()
+    t0 = time.perf_counter()
+    st = S.run_learned(learned, sur, DT, steps, judge_every=10, bound=0.01)
+    torch.cuda.synchronize()
+    learned_s = time.perf_counter() - t0
+    clocks = sampler.stop()
+    # ---- error against the plain f64 run ----
+    r64, r_l = plain.densities()[fluid], learned.densities()[fluid]
+    x64, x_l = plain.positions()[fluid], learned.positions()[fluid]
+    v64, v_l = plain.velocities()[fluid], learned.velocities()[fluid]
+    rel = np.abs(r_l - r64) / r64
+    mass = plain.mass
+
+    def energy(x, v):
+        return float((0.5 * mass * (v * v).sum(1)).sum() + (mass * 9.81 * x[:, 2]).sum())
+
+    e64, e_l = energy(x64, v64), energy(x_l, v_l)
+    value = nf * steps / learned_s
+    line = {
+        "metric": "SPH fluid particle-steps/s @1M (learned surrogate, judged every 10 steps)",
+        "value": value, "unit": UNIT, "n_gpus": 1, "steps": steps, "warmup": 0,
+        "ms_per_step": learned_s / steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "bf16 network, f64 state", "data": "synthetic", "form": "learned",
+        "config": {"workload": args.workload, "fluid_particles": nf, "dx": DX, "dt": DT,
+                   "network": "2-hop message passing, MLP width 128 x 2 hidden layers, r_msg = h",
+                   "judge_every": 10, "fallback_bound": 0.01,
+                   "training": {"tanks": args.train_tanks, "particles_per_tank": 64000,
+                                "plain_steps": args.train_steps, "normalisation_steps": 20,
+                                "adam_steps": len(losses), "lr": 5e-4, "seconds": train_s,
+                                "final_loss": float(np.mean(losses[-20:]))}},
+        "plain_f64": {"ms_per_step": plain_s / steps * 1e3, "value": nf * steps / plain_s},
+        "speedup_vs_plain_step": plain_s / learned_s,
+        "judge": st, "fallback_rate": st["fallbacks"] / max(1, st["windows"]),
+        "error_vs_f64": {"after_steps": steps, "density_rel_max": float(rel.max()),
+                         "density_rel_mean": float(rel.mean()),
+                         "position_rms_m": float(np.sqrt(((x_l - x64) ** 2).sum(1).mean())),
+                         "com_drift_m": float(np.linalg.norm(x_l.mean(0) - x64.mean(0))),
+                         "energy_rel_drift": float((e_l - e64) / abs(e64))},
+        "timing": "wall clock around synchronous runs (the learned run synchronises at every judge)",
+        "clocks": clocks,
+    }
+    plain.close()
+    learned.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = _args()
     ws, rank, local = _dist()
     if args.impl == "reference":
         run_reference(args, ws, rank)
         return
-    if args.form in ("f32", "batched"):
+    if args.form in ("f32", "batched", "learned"):
         import torch
 
         torch.cuda.set_device(local)
@@ -418,7 +505,8 @@ def main():
             torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
         import physics_engine_rs as pe
 
-        (run_f32 if args.form == "f32" else run_batched)(args, ws, rank, local, torch, pe)
+        {"f32": run_f32, "batched": run_batched, "learned": run_learned_form}[args.form](
+            args, ws, rank, local, torch, pe)
         if ws > 1:
             torch.distributed.destroy_process_group()
         return
