@@ -23,6 +23,13 @@ struct GemmArgs {
     const float* bias;
     int M, N, K, lda, ldb, ldc, relu;
     uint32_t* err;  // bit 0: a bounded wait ran out
+    // optional gathered addends, added after the bias and before the ReLU:
+    // C[r][c] += add0[idx0[r] * ld_add + c] + add1[idx1[r] * ld_add + c]
+    const float* add0 = nullptr;
+    const int* idx0 = nullptr;
+    const float* add1 = nullptr;
+    const int* idx1 = nullptr;
+    int ld_add = 0;
 };
 
 size_t gemm_smem_bytes();

@@ -172,25 +172,62 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm_bf16(GemmArgs g) {
     ok = (have ? mbar_wait(smem_addr(&mbar[2]), 0u) : true) && ok;
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 
-    const int row = m0 + warp * 32 + lane;
+    // Epilogue: the accumulator goes through shared memory (the operand stages
+    // are free once every MMA has completed) so that each warp then stores
+    // whole 512-byte rows. Row r's 4-float chunk q sits at chunk q ^ (r & 31):
+    // the row-per-lane writes and the chunk-per-lane reads both spread over
+    // all banks.
     const bool split = gridDim.z > 1;  // raw fp32 partials, summed by k_reduce_splits
     const size_t part = (size_t)blockIdx.z * (size_t)g.M * (size_t)g.ldc;
+    float4* stile = reinterpret_cast<float4*>(smem);  // 128 rows x 32 chunks
+    {
+        const int r = warp * 32 + lane;
 #pragma unroll 1
-    for (int cb = 0; cb < kBN / 32; ++cb) {
-        uint32_t r[32];
-        tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(cb * 32), r);
-        if (row < g.M) {
+        for (int cb = 0; cb < kBN / 32; ++cb) {
+            uint32_t v[32];
+            tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(cb * 32), v);
 #pragma unroll
-            for (int j = 0; j < 32; ++j) {
-                const int col = n0 + cb * 32 + j;
-                if (col >= g.N) break;
-                float v = have ? __uint_as_float(r[j]) : 0.f;
-                if (!split) {
-                    if (g.bias) v += g.bias[col];
-                    if (g.relu) v = fmaxf(v, 0.f);
-                    if (g.Cb) g.Cb[(size_t)row * g.ldc + col] = __float2bfloat16_rn(v);
-                }
-                if (g.Cf) g.Cf[part + (size_t)row * g.ldc + col] = v;
+            for (int j = 0; j < 8; ++j) {
+                const int q = cb * 8 + j;
+                stile[r * 32 + (q ^ (r & 31))] =
+                    have ? make_float4(__uint_as_float(v[4 * j]), __uint_as_float(v[4 * j + 1]),
+                                       __uint_as_float(v[4 * j + 2]), __uint_as_float(v[4 * j + 3]))
+                         : make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+        }
+    }
+    __syncthreads();
+    const int col = n0 + lane * 4;
+    const bool vec = (g.ldc & 3) == 0 && col + 3 < g.N;
+#pragma unroll 1
+    for (int r = warp; r < kBM; r += kGemmThreads / 32) {
+        const int row = m0 + r;
+        if (row >= g.M || col >= g.N) continue;
+        const float4 c4 = stile[r * 32 + (lane ^ (r & 31))];
+        float v[4] = {c4.x, c4.y, c4.z, c4.w};
+        if (!split) {
+            const float* a0 = g.add0 ? g.add0 + (size_t)g.idx0[row] * g.ld_add : nullptr;
+            const float* a1 = g.add1 ? g.add1 + (size_t)g.idx1[row] * g.ld_add : nullptr;
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                if (col + i >= g.N) break;
+                if (g.bias) v[i] += g.bias[col + i];
+                if (a0) v[i] += a0[col + i];
+                if (a1) v[i] += a1[col + i];
+                if (g.relu) v[i] = fmaxf(v[i], 0.f);
+            }
+        }
+        if (vec) {
+            if (g.Cf) *reinterpret_cast<float4*>(g.Cf + part + (size_t)row * g.ldc + col) = make_float4(v[0], v[1], v[2], v[3]);
+            if (g.Cb && !split) {
+                __nv_bfloat162 lo = __floats2bfloat162_rn(v[0], v[1]), hi = __floats2bfloat162_rn(v[2], v[3]);
+                uint2 packed = make_uint2(*reinterpret_cast<uint32_t*>(&lo), *reinterpret_cast<uint32_t*>(&hi));
+                *reinterpret_cast<uint2*>(g.Cb + (size_t)row * g.ldc + col) = packed;
+            }
+        } else {
+            for (int i = 0; i < 4 && col + i < g.N; ++i) {
+                if (g.Cf) g.Cf[part + (size_t)row * g.ldc + col + i] = v[i];
+                if (g.Cb && !split) g.Cb[(size_t)row * g.ldc + col + i] = __float2bfloat16_rn(v[i]);
             }
         }
     }

@@ -27,17 +27,6 @@ __global__ void k_to_bf16(size_t n, const float* __restrict__ src, __nv_bfloat16
     if (i < n) dst[i] = __float2bfloat16_rn(src[i]);
 }
 
-// layer 1 of the edge MLP: relu(ZE_e + P_dst + Q_src), bf16
-__global__ void k_edge_h1(int E, const float* __restrict__ ZE, const float* __restrict__ P,
-                          const float* __restrict__ Q, const int* __restrict__ dst, const int* __restrict__ src,
-                          __nv_bfloat16* __restrict__ out) {
-    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= (size_t)E * kWidth) return;
-    const int e = (int)(i / kWidth), c = (int)(i % kWidth);
-    const float z = ZE[i] + P[(size_t)dst[e] * kWidth + c] + Q[(size_t)src[e] * kWidth + c];
-    out[i] = __float2bfloat16_rn(fmaxf(z, 0.f));
-}
-
 // out_i = scale * sum of rows [row_i, row_{i+1}) of in (a warp per node)
 __global__ void k_segsum(int n, const int* __restrict__ row, const float* __restrict__ in, float scale,
                          float* __restrict__ out) {
@@ -420,7 +409,6 @@ void Surrogate::ensure_acts(bool train) {
     for (auto& p : hb_) p = ba(cn * W);
     P_ = fa(cn * W);
     Q_ = fa(cn * W);
-    ZE_ = fa(ce * W);
     for (int l = 0; l < 2; ++l) {
         eh1_[l] = (l == 0 || train) ? ba(ce * W) : eh1_[0];
         eh2_[l] = (l == 0 || train) ? ba(ce * W) : eh2_[0];
@@ -488,7 +476,7 @@ void Surrogate::mlp_fwd(int first, const __nv_bfloat16* X, int R, __nv_bfloat16*
 void Surrogate::forward(bool keep_for_backward) {
     ensure_acts(keep_for_backward);
     const int n = g_.n, E = g_.E;
-    const size_t nW = (size_t)n * kWidth, eW = (size_t)E * kWidth;
+    const size_t nW = (size_t)n * kWidth;
     mlp_fwd(0, g_.f, n, enc_a1_, enc_a2_, h_);
     k_to_bf16<<<blocks(nW, 256), 256, 0, st_>>>(nW, h_, hb_[0]);
     for (int l = 0; l < 2; ++l) {
@@ -496,8 +484,15 @@ void Surrogate::forward(bool keep_for_backward) {
         linear_fwd(layers_[base + 0], hb_[l], n, P_, nullptr, false);
         linear_fwd(layers_[base + 1], hb_[l], n, Q_, nullptr, false);
         if (E > 0) {
-            linear_fwd(layers_[base + 2], g_.xe, E, ZE_, nullptr, false);
-            k_edge_h1<<<blocks(eW, 256), 256, 0, st_>>>(E, ZE_, P_, Q_, g_.dst, g_.src, eh1_[l]);
+            // layer 1: relu(x_e Wc + b1 + P[dst] + Q[src]), the gathers fused into the GEMM's epilogue
+            const Linear& L0 = layers_[base + 2];
+            GemmArgs ga{g_.xe, L0.Wt16, nullptr, eh1_[l], L0.b, E, L0.Np, L0.K, L0.K, L0.K, L0.Np, 1, err_};
+            ga.add0 = P_;
+            ga.idx0 = g_.dst;
+            ga.add1 = Q_;
+            ga.idx1 = g_.src;
+            ga.ld_add = kWidth;
+            launch_gemm(ga, 1, st_);
             linear_fwd(layers_[base + 3], eh1_[l], E, nullptr, eh2_[l], true);
             linear_fwd(layers_[base + 4], eh2_[l], E, M_, nullptr, false);
         }

@@ -149,7 +149,6 @@ class Surrogate {
     float* h_ = nullptr;                   // latent fp32 [n x 128]
     __nv_bfloat16* hb_[3] = {};            // latent bf16 per level
     float *P_ = nullptr, *Q_ = nullptr;    // [n x 128]
-    float* ZE_ = nullptr;                  // [E x 128]
     __nv_bfloat16 *eh1_[2] = {}, *eh2_[2] = {};  // per hop, [E x 128]
     float* M_ = nullptr;                   // [E x 128]
     float* A_ = nullptr;                   // [n x 128]
