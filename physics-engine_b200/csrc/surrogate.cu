@@ -355,7 +355,9 @@ void Surrogate::ensure_graph(int n, int E) {
     for (void* p : graph_allocs_) cudaFree(p);
     graph_allocs_.clear();
     if (scan_tmp_) cudaFree(scan_tmp_);
-    const int cn = std::max(n, g_.cap_n), ce = std::max(E, g_.cap_e);
+    // grow with a quarter of headroom: the edge count creeps up step by step as
+    // the fluid compresses, and every growth reallocates
+    const int cn = std::max(n + n / 4, g_.cap_n), ce = std::max(E + E / 4, g_.cap_e);
     auto ga = [&](size_t bytes) {
         void* p = nullptr;
         cu(cudaMalloc(&p, std::max<size_t>(bytes, 256)), "cudaMalloc graph");
@@ -389,7 +391,11 @@ void Surrogate::ensure_acts(bool train) {
     cu(cudaStreamSynchronize(st_), "acts");
     for (void* p : act_allocs_) cudaFree(p);
     act_allocs_.clear();
-    const int cn = round8(std::max(n, act_n_)), ce = round8(std::max(E, act_e_));
+    // grow with a quarter of headroom; a switch to training sizes for the
+    // current graph only (training buffers cost ~3x per edge)
+    const bool keep = act_train_ || !train;
+    const int cn = round8(std::max(n + n / 4, keep ? act_n_ : 0));
+    const int ce = round8(std::max(E + E / 4, keep ? act_e_ : 0));
     auto fa = [&](size_t count) {
         void* p = nullptr;
         cu(cudaMalloc(&p, std::max<size_t>(count * 4, 256)), "cudaMalloc acts");
