@@ -15,8 +15,9 @@
 //
 // k_nlist_visit writes, for fluid particles, the "visit" list (in-support
 // candidates, self excluded, in visiting order, each flagged boundary /
-// oriented / lower) and the "upper" list (the visit list without the entries
-// flagged lower). k_nlist_lower writes the "lower" list: for fluid particles
+// oriented / lower; the force pass reads its unflagged entries as the
+// reference's j > i and boundary pairs). k_nlist_lower writes the "lower"
+// list: for fluid particles
 // the fluid neighbours with a smaller original index, for boundary particles
 // all fluid neighbours, both in ascending original index; the order comes
 // from a shared-memory radix sort of the union's fluid entries per cell.
@@ -215,7 +216,7 @@ __device__ __forceinline__ ChunkBlock reserve_chunk(const ListBufs& l, DeviceSca
 // Dynamic shared memory (ucap a multiple of kStageStep): float4 s_pos[ucap];
 // uint32 s_ent[ucap]; uint32 s_mask[(ucap / 32) * kChunk] (word w of chunk
 // lane c at s_mask[w * kChunk + c]).
-template <int DIM, bool UPPER>
+template <int DIM, bool LOWER_FLAGS>
 __global__ void __launch_bounds__(kNlThreads) k_nlist_visit(GridDesc g, Tanks tk, StepConst k, uint32_t ucap,
                                                             const uint32_t* __restrict__ occ,
                                                             const uint32_t* __restrict__ cell_start,
@@ -268,7 +269,7 @@ __global__ void __launch_bounds__(kNlThreads) k_nlist_visit(GridDesc g, Tanks tk
                     const uint32_t mw = __float_as_uint(me.w);
                     fluidc = !(mw & kStageBoundary);
                     myo = mw & kStageOrigMask;
-                    uint32_t cv = 0, cl = 0;
+                    uint32_t cv = 0;
                     if (fluidc) {
                         for (uint32_t w = wb; w < we; ++w) {
                             uint32_t m = 0;
@@ -279,65 +280,43 @@ __global__ void __launch_bounds__(kNlThreads) k_nlist_visit(GridDesc g, Tanks tk
                             if (w == (myu >> 5)) m &= ~(1u << (myu & 31u));
                             s_mask[w * kChunk + lane] = m;
                             cv += __popc(m);
-                            if (UPPER) {
-                                uint32_t mm = m;
-                                while (mm) {
-                                    const uint32_t u = (w << 5) + (__ffs(mm) - 1);
-                                    mm &= mm - 1u;
-                                    const uint32_t ow = __float_as_uint(s_pos[u].w);
-                                    cl += (!(ow & kStageBoundary) && (ow & kStageOrigMask) < myo) ? 1u : 0u;
-                                }
-                            }
                         }
                     }
                     s_cv[q][lane] = cv;
-                    s_cu[q][lane] = cv - cl;
                 }
                 __syncthreads();
                 // ---- list lengths, this quarter's offsets, the chunk's block
-                uint32_t nv = 0, nu = 0, ov = 0, ou = 0;
+                uint32_t nv = 0, ov = 0;
                 if (active) {
 #pragma unroll
                     for (uint32_t r = 0; r < kWays; ++r) {
-                        const uint32_t a = s_cv[r][lane], b = s_cu[r][lane];
-                        if (r < q) {
-                            ov += a;
-                            ou += b;
-                        }
+                        const uint32_t a = s_cv[r][lane];
+                        if (r < q) ov += a;
                         nv += a;
-                        nu += b;
                     }
-                    if (!UPPER) nu = ou = 0;
                 }
-                const ChunkBlock blk = reserve_chunk(l, sc, nc, nv, nu, s_red, &s_blk, &s_overflow);
+                const ChunkBlock blk = reserve_chunk(l, sc, nc, nv, 0u, s_red, &s_blk, &s_overflow);
                 // ---- pass 2: descriptors and entries
                 if (active) {
                     const uint32_t kslot = cu.cs + c0 + lane;
                     const uint32_t gv = (uint32_t)blk.base + lane;  // < pool_groups < 2^32 when ok
                     if (q == 0) {
-                        l.desc[kslot] = blk.ok ? make_uint4(gv, nc | (blk.rows_a << 16), nv | (nu << 16), 0u)
-                                               : make_uint4(0u, 0u, 0u, 0u);
+                        l.desc[kslot] = blk.ok ? make_uint4(gv, nc, nv, 0u) : make_uint4(0u, 0u, 0u, 0u);
                         l.ncand[kslot] = fluidc ? U : 0u;
                     }
                     if (blk.ok && fluidc) {
                         const size_t step = 4u * nc;
                         uint32_t* pv = l.pool + 4 * (size_t)gv;
-                        uint32_t* pu = l.pool + 4 * ((size_t)gv + (size_t)blk.rows_a * nc);
-                        uint32_t tv = ov, tu = ou;
+                        uint32_t tv = ov;
                         for (uint32_t w = wb; w < we; ++w) {
                             uint32_t m = s_mask[w * kChunk + lane];
                             while (m) {
                                 const uint32_t u = (w << 5) + (__ffs(m) - 1);
                                 m &= m - 1u;
                                 uint32_t e = s_ent[u];
-                                if (UPPER) {
+                                if (LOWER_FLAGS) {
                                     const uint32_t ow = __float_as_uint(s_pos[u].w);
-                                    if (!(ow & kStageBoundary) && (ow & kStageOrigMask) < myo) {
-                                        e |= kEntryLower;
-                                    } else {
-                                        pu[(tu >> 2) * step + (tu & 3u)] = e;
-                                        ++tu;
-                                    }
+                                    if (!(ow & kStageBoundary) && (ow & kStageOrigMask) < myo) e |= kEntryLower;
                                 }
                                 pv[(tv >> 2) * step + (tv & 3u)] = e;
                                 ++tv;
@@ -358,7 +337,7 @@ __global__ void __launch_bounds__(kNlThreads) k_nlist_visit(GridDesc g, Tanks tk
                 uint8_t mfl = 0;
                 uint32_t myo = 0;
                 float4 me = make_float4(0.f, 0.f, 0.f, 0.f);
-                uint32_t nv = 0, nl = 0;
+                uint32_t nv = 0;
                 bool fluidc = false;
                 if (active) {
                     me = stage_entry<DIM>(s, kslot, cu, &mfl, &myo);
@@ -370,25 +349,20 @@ __global__ void __launch_bounds__(kNlThreads) k_nlist_visit(GridDesc g, Tanks tk
                                 if (slot == kslot) continue;
                                 uint8_t fl;
                                 uint32_t o;
-                                if (!within(stage_entry<DIM>(s, slot, cu, &fl, &o), me, r2f)) continue;
-                                ++nv;
-                                if (!(fl & kFlagBoundary) && o < myo) ++nl;
+                                if (within(stage_entry<DIM>(s, slot, cu, &fl, &o), me, r2f)) ++nv;
                             }
                         }
                     }
                 }
-                const uint32_t nu = UPPER ? nv - nl : 0u;
-                const ChunkBlock blk = reserve_chunk(l, sc, nc, nv, nu, s_red, &s_blk, &s_overflow);
+                const ChunkBlock blk = reserve_chunk(l, sc, nc, nv, 0u, s_red, &s_blk, &s_overflow);
                 if (active) {
                     const uint32_t gv = (uint32_t)blk.base + tid;
-                    l.desc[kslot] = blk.ok ? make_uint4(gv, nc | (blk.rows_a << 16), nv | (nu << 16), 0u)
-                                           : make_uint4(0u, 0u, 0u, 0u);
+                    l.desc[kslot] = blk.ok ? make_uint4(gv, nc, nv, 0u) : make_uint4(0u, 0u, 0u, 0u);
                     l.ncand[kslot] = fluidc ? U : 0u;
                     if (blk.ok && fluidc) {
                         const size_t step = 4u * nc;
                         uint32_t* pv = l.pool + 4 * (size_t)gv;
-                        uint32_t* pu = l.pool + 4 * ((size_t)gv + (size_t)blk.rows_a * nc);
-                        uint32_t tv = 0, tu = 0;
+                        uint32_t tv = 0;
                         for (int c = 0; c < NC; ++c) {
                             const uint32_t q0 = s_cstart[c], q1 = q0 + (s_off[c + 1] - s_off[c]);
                             for (uint32_t slot = q0; slot < q1; ++slot) {
@@ -398,14 +372,7 @@ __global__ void __launch_bounds__(kNlThreads) k_nlist_visit(GridDesc g, Tanks tk
                                 const float4 qp = stage_entry<DIM>(s, slot, cu, &fl, &o);
                                 if (!within(qp, me, r2f)) continue;
                                 uint32_t e = slot | entry_flags(__float_as_uint(qp.w));
-                                if (UPPER) {
-                                    if (!(fl & kFlagBoundary) && o < myo) {
-                                        e |= kEntryLower;
-                                    } else {
-                                        if (tu < nu) pu[(tu >> 2) * step + (tu & 3u)] = e;
-                                        ++tu;
-                                    }
-                                }
+                                if (LOWER_FLAGS && !(fl & kFlagBoundary) && o < myo) e |= kEntryLower;
                                 if (tv < nv) pv[(tv >> 2) * step + (tv & 3u)] = e;
                                 ++tv;
                             }

@@ -49,6 +49,32 @@ __device__ __forceinline__ void for_each_entry(const ListRef r, F&& f) {
     }
 }
 
+// Calls f(entry, data) over a slot's list in order, where data = load(entry)
+// is issued one entry ahead: the gather of the next neighbour's state is in
+// flight while the current pair is computed.
+template <class Load, class F>
+__device__ __forceinline__ void for_each_loaded(const ListRef r, Load&& load, F&& f) {
+    const uint32_t n = r.n;
+    if (n == 0) return;
+    auto at = [&](uint32_t t) { return __ldg(r.p + (size_t)(t >> 2) * r.step + (t & 3u)); };
+    uint32_t e0 = at(0), e1 = n > 1 ? at(1) : 0u;
+    auto d0 = load(e0);
+    for (uint32_t t = 0; t < n; ++t) {
+        const uint32_t e = e0;
+        const auto d = d0;
+        if (t + 1 < n) {
+            e0 = e1;
+            d0 = load(e1);
+            if (t + 2 < n) e1 = at(t + 2);
+        }
+        f(e, d);
+    }
+}
+
+struct PosVel {
+    double4 x, v;
+};
+
 __global__ void __launch_bounds__(kMaxPassThreads) k_density(uint32_t n, StepConst k, StateBufs s,
                                                       ListBufs l) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -59,9 +85,10 @@ __global__ void __launch_bounds__(kMaxPassThreads) k_density(uint32_t n, StepCon
     }
     const double4 xi = s.pos[i];
     double rho = k.rho_self;  // 0.0 + mass * W(0)
-    for_each_entry(list_ref(l, i, kListVisit), [&](uint32_t e) {
+    for_each_loaded(
+        list_ref(l, i, kListVisit), [&](uint32_t e) { return s.pos[e & kEntrySlotMask]; },
+        [&](uint32_t e, const double4& xj) {
         const uint32_t j = e & kEntrySlotMask;
-        const double4 xj = s.pos[j];
         const double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
         const double r = sqrt(dx * dx + dy * dy + dz * dz);
         const double wij = kern_w(r, k);
@@ -199,16 +226,25 @@ __global__ void __launch_bounds__(kMaxPassThreads) k_forces(uint32_t n, StepCons
     const double4 vk = s.vel[k];
     double ax = 0.0, ay = 0.0, az = 0.0;
     // fluid i < k, ascending original index
-    for_each_entry(list_ref(l, k, kListLower), [&](uint32_t j) {
-        fluid_pair(kc, nac, xk, vk, s.pos[j], s.vel[j], ax, ay, az);
-    });
-    // fluid j > k and boundary j, visiting order
-    for_each_entry(list_ref(l, k, kListUpper), [&](uint32_t e) {
+    // neighbour state gathered one entry ahead (boundary samples need no velocity)
+    auto load = [&](uint32_t e) {
+        PosVel d;
         const uint32_t j = e & kEntrySlotMask;
+        d.x = s.pos[j];
+        d.v = (e & kEntryBoundary) ? make_double4(0.0, 0.0, 0.0, 0.0) : s.vel[j];
+        return d;
+    };
+    for_each_loaded(list_ref(l, k, kListLower), load, [&](uint32_t, const PosVel& d) {
+        fluid_pair(kc, nac, xk, vk, d.x, d.v, ax, ay, az);
+    });
+    // fluid j > k and boundary j, visiting order: the visit list without the
+    // entries flagged lower (those came from the lower list, in index order)
+    for_each_loaded(list_ref(l, k, kListVisit), load, [&](uint32_t e, const PosVel& d) {
+        if (e & kEntryLower) return;
         if (e & kEntryBoundary) {
-            boundary_pair(kc, xk, s.pos[j], (e & kEntryOriented) != 0u, s.nout, j, ax, ay, az);
+            boundary_pair(kc, xk, d.x, (e & kEntryOriented) != 0u, s.nout, e & kEntrySlotMask, ax, ay, az);
         } else {
-            fluid_pair(kc, nac, xk, vk, s.pos[j], s.vel[j], ax, ay, az);
+            fluid_pair(kc, nac, xk, vk, d.x, d.v, ax, ay, az);
         }
     });
     ax += kc.gx;
@@ -270,14 +306,23 @@ __global__ void __launch_bounds__(kMaxPassThreads) k_xsph(uint32_t n, StepConst 
     }
     const double4 xi = s.pos[i];
     double dvx = 0.0, dvy = 0.0, dvz = 0.0;
-    for_each_entry(list_ref(l, i, kListVisit), [&](uint32_t e) {
+    for_each_loaded(
+        list_ref(l, i, kListVisit),
+        [&](uint32_t e) {
+            PosVel d{};
+            if (!(e & kEntryBoundary)) {
+                d.x = s.pos[e & kEntrySlotMask];
+                d.v = s.vel[e & kEntrySlotMask];
+            }
+            return d;
+        },
+        [&](uint32_t e, const PosVel& d) {
         if (e & kEntryBoundary) return;
-        const uint32_t j = e & kEntrySlotMask;
-        const double4 xj = s.pos[j];
+        const double4 xj = d.x;
         const double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
         const double r = sqrt(dx * dx + dy * dy + dz * dz);
         const double wij = kern_w(r, kc);
-        const double4 vj = s.vel[j];
+        const double4 vj = d.v;
         const double rho_bar = 0.5 * (vi.w + vj.w);
         const double f = kc.mass / rho_bar * wij;
         dvx += (vj.x - vi.x) * f;

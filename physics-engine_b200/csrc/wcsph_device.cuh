@@ -13,9 +13,10 @@
 //     linear cell order equals the reference's CellKey order), cell_start,
 //     and the list of occupied cells.
 //   * per-slot neighbour lists in one pool, reserved per chunk of a cell's
-//     slots with exact capacities (see ListBufs): the "visit" list holds in-support candidates in the
-//     reference's visiting order; the "upper" list is the visit list without
-//     the entries flagged lower; the "lower" list holds, for fluid slots, the
+//     slots with exact capacities (see ListBufs): the "visit" list holds
+//     in-support candidates in the reference's visiting order, flagged lower
+//     where the force pass takes them from the "lower" list instead, which
+//     holds, for fluid slots, the
 //     fluid neighbours with a lower original index in ascending original-index
 //     order, and, for boundary slots, all fluid neighbours in ascending
 //     original index.
@@ -102,7 +103,7 @@ struct StateBufs {
 
 struct ListBufs {
     uint32_t* pool;                   // list entries, allocated in 16-byte groups
-    uint4* desc;                      // per slot: visit and upper lists, see list_ref
+    uint4* desc;                      // per slot: visit list, see list_ref
     uint2* ldesc;                     // per slot: lower list, see list_ref
     uint32_t* ncand;                  // candidates examined per slot (fluid: union size)
     unsigned long long pool_groups;   // capacity of pool in 16-byte groups (< 2^32)
@@ -115,11 +116,10 @@ struct ListBufs {
 // (rounded up to 4 entries). Entries t..t+3 of a slot's list are one group,
 // and the chunk's slots' groups of a row are contiguous, so the lanes of a
 // warp reading entry t of consecutive slots read consecutive 16-byte groups.
-//   desc[s]  = (group of row 0 of the visit list (chunk base + lane),
-//               stride | first row of the upper list << 16,
-//               visit count | upper count << 16, 0)
+//   desc[s]  = (group of row 0 of the visit list (chunk base + lane), stride,
+//               visit count, 0)
 //   ldesc[s] = (group of row 0 of the lower list, lower count | stride << 16)
-enum ListKind : int { kListVisit = 0, kListUpper = 1, kListLower = 2 };
+enum ListKind : int { kListVisit = 0, kListLower = 2 };
 
 struct ListRef {
     const uint32_t* p;  // entry t at p[(t >> 2) * step + (t & 3)]
@@ -137,11 +137,9 @@ __device__ __forceinline__ ListRef list_ref(const ListBufs& l, uint32_t s, int k
         return r;
     }
     const uint4 d = __ldg(l.desc + s);
-    const uint32_t stride = d.y & 0xffffu;
-    const uint32_t row = kind == kListUpper ? d.y >> 16 : 0u;
-    r.p = l.pool + 4 * ((size_t)d.x + (size_t)row * stride);
-    r.step = 4 * stride;
-    r.n = kind == kListUpper ? d.z >> 16 : d.z & 0xffffu;
+    r.p = l.pool + 4 * (size_t)d.x;
+    r.step = 4 * d.y;
+    r.n = d.z;
     return r;
 }
 
