@@ -471,7 +471,7 @@ def run_learned_form(args, ws, rank, local, torch, pe):
                    "training": {"tanks": args.train_tanks, "particles_per_tank": 64000,
                                 "plain_steps": args.train_steps, "normalisation_steps": 20,
                                 "adam_steps": len(losses), "lr": 5e-4, "seconds": train_s,
-                                "final_loss": float(np.mean(losses[-20:]))}},
+                                "final_loss": float(np.mean(losses[-20:])) if losses else None}},
         "plain_f64": {"ms_per_step": plain_s / steps * 1e3, "value": nf * steps / plain_s},
         "speedup_vs_plain_step": plain_s / learned_s,
         "judge": st, "fallback_rate": st["fallbacks"] / max(1, st["windows"]),

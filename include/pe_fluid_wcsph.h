@@ -170,6 +170,26 @@ int pe_fluid_wcsph_create_from_arrays(const PeWcsphParams* params, int32_t dim, 
                                       double mass, double h, uint64_t n, const double* x,
                                       const double* v, const uint8_t* kind, const double* psi,
                                       const double* n_out, const PeWcsphConfig* cfg, PeWcsph** out);
+/* Fluid side of CoupledWcsphWorld::step (coupling.rs:853-866). A coupler holds
+ * the rigid samples of a world: sample k is world particle particle[k] (an
+ * oriented boundary sample) on body body[k] < n_bodies, at body-frame offset
+ * local[3k..] with body-frame normal local_n[3k..] (FluidRigidCoupler::samples,
+ * coupling.rs:42-51, insertion order). The rigid bodies stay with the caller. */
+typedef struct PeCoupler PeCoupler;
+int pe_fluid_coupler_create(PeWcsph* w, uint32_t n_bodies, uint64_t n_samples, const int64_t* body,
+                            const double* local, const double* local_n, const int64_t* particle,
+                            PeCoupler** out);
+void pe_fluid_coupler_destroy(PeCoupler* c);
+/* FluidRigidCoupler::sync_from_rigid (coupling.rs:289-306): per body the
+ * centre of mass X (3), orientation q (4: w, x, y, z), velocity V (3) and
+ * world-frame angular velocity omega (3); the samples' positions, velocities
+ * and normals follow, and the next step rebuilds the grid. */
+int pe_fluid_coupler_sync(PeCoupler* c, const double* X, const double* q, const double* V, const double* omega);
+/* FluidRigidCoupler::reduce_with_state (coupling.rs:308-330): per body the sum
+ * of its samples' boundary reactions (force, 3 per body) and of r x f with
+ * r = x - X (torque, 3 per body), in sample order. */
+int pe_fluid_coupler_reduce(PeCoupler* c, const double* X, double* force, double* torque);
+
 /* Batched form (no reference counterpart; replaces a loop of WcsphWorld::step
  * over independent tanks): n_tanks tanks with the same material and physics,
  * particles stored tank-major, tank t owning particles [tank_offsets[t],

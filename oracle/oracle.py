@@ -124,6 +124,8 @@ def lib():
             "o_mean_density_error": (d, [vp]),
             "o_max_density_error": (d, [vp]),
             "o_suggested_dt": (d, [d, d, d, d, d, d]),
+            "o_coupler_sync": (None, [vp, u64, vp, vp, vp, vp, vp, vp, vp, vp]),
+            "o_coupler_reduce": (None, [vp, u64, vp, vp, u64, vp, vp, vp]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -313,6 +315,33 @@ class World:
     def max_density_error(self):
         return lib().o_max_density_error(self._w)
 
+
+
+class Coupler:
+    """`FluidRigidCoupler` restated (coupling.rs:42-51, 289-330): sample k is
+    particle `particle[k]` on body `body[k]` with body-frame offset `local[k]`
+    and normal `local_n[k]`."""
+
+    def __init__(self, world: World, n_bodies, body, local, local_n, particle):
+        self.w, self.nb = world, int(n_bodies)
+        self.body = np.ascontiguousarray(body, np.int64).reshape(-1)
+        ns = self.body.shape[0]
+        self.local = np.ascontiguousarray(local, np.float64).reshape(ns, 3)
+        self.local_n = np.ascontiguousarray(local_n, np.float64).reshape(ns, 3)
+        self.particle = np.ascontiguousarray(particle, np.int64).reshape(ns)
+
+    def sync_from_rigid(self, x, q, v, omega):
+        a = [np.ascontiguousarray(t, np.float64) for t in (x, q, v, omega)]
+        lib().o_coupler_sync(self.w._w, self.body.shape[0], _ptr(self.body), _ptr(self.local),
+                             _ptr(self.local_n), _ptr(self.particle), *[_ptr(t) for t in a])
+
+    def reduce_with_state(self, x):
+        xb = np.ascontiguousarray(x, np.float64)
+        f = np.zeros((self.nb, 3))
+        t = np.zeros((self.nb, 3))
+        lib().o_coupler_reduce(self.w._w, self.body.shape[0], _ptr(self.body), _ptr(self.particle), self.nb,
+                               _ptr(xb), _ptr(f), _ptr(t))
+        return f, t
 
 def kernel_w(kernel, r, h, dim):
     return lib().o_kernel_w(kernel, r, h, dim)

@@ -844,6 +844,62 @@ void ow_get_x(OWorld* w, double* out) { put3(W(w).parts.x, out); }
 void ow_get_v(OWorld* w, double* out) { put3(W(w).parts.v, out); }
 void ow_get_a(OWorld* w, double* out) { put3(W(w).parts.a, out); }
 void ow_get_boundary_force(OWorld* w, double* out) { put3(W(w).boundary_force, out); }
+
+// ---- fluid side of the WCSPH-rigid coupling (coupling.rs:289-330) ----
+// quat.rs:119-137 to_matrix and quat.rs:102-109 rotate, q = (w, x, y, z)
+static V3 quat_rotate(const double* q, V3 v) {
+    const double w = q[0], x = q[1], y = q[2], z = q[3];
+    const double r00 = 1.0 - 2.0 * (y * y + z * z), r01 = 2.0 * (x * y - w * z), r02 = 2.0 * (x * z + w * y);
+    const double r10 = 2.0 * (x * y + w * z), r11 = 1.0 - 2.0 * (x * x + z * z), r12 = 2.0 * (y * z - w * x);
+    const double r20 = 2.0 * (x * z - w * y), r21 = 2.0 * (y * z + w * x), r22 = 1.0 - 2.0 * (x * x + y * y);
+    return V3{r00 * v.x + r01 * v.y + r02 * v.z, r10 * v.x + r11 * v.y + r12 * v.z,
+              r20 * v.x + r21 * v.y + r22 * v.z};
+}
+
+// vec3.rs:87-93
+static V3 cross3(V3 a, V3 b) {
+    return V3{a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+
+// FluidRigidCoupler::sync_from_rigid (coupling.rs:289-306): per sample, in
+// order, x = X + R(q) local, v = V + omega x r, n_out = R(q) local_n; bodies
+// give X (3), q (4: w, x, y, z), V (3) and the world-frame omega (3).
+void o_coupler_sync(OWorld* wp, uint64_t ns, const int64_t* body, const double* local, const double* local_n,
+                    const int64_t* particle, const double* X, const double* Q, const double* V,
+                    const double* Om) {
+    Particles& parts = W(wp).parts;
+    for (uint64_t k = 0; k < ns; ++k) {
+        const int64_t b = body[k], i = particle[k];
+        const V3 xb{X[3 * b], X[3 * b + 1], X[3 * b + 2]}, vb{V[3 * b], V[3 * b + 1], V[3 * b + 2]};
+        const V3 wb{Om[3 * b], Om[3 * b + 1], Om[3 * b + 2]};
+        const V3 r = quat_rotate(Q + 4 * b, V3{local[3 * k], local[3 * k + 1], local[3 * k + 2]});
+        parts.x[i] = xb + r;
+        parts.v[i] = vb + cross3(wb, r);
+        parts.n_out[i] = quat_rotate(Q + 4 * b, V3{local_n[3 * k], local_n[3 * k + 1], local_n[3 * k + 2]});
+        if (parts.dim == D2) {
+            parts.x[i].z = 0.0;
+            parts.v[i].z = 0.0;
+            parts.n_out[i].z = 0.0;
+        }
+    }
+}
+
+// FluidRigidCoupler::reduce_with_state (coupling.rs:308-330): per body the sum
+// of its samples' boundary forces and of r x f with r = x - X, in sample order.
+void o_coupler_reduce(OWorld* wp, uint64_t ns, const int64_t* body, const int64_t* particle, uint64_t nb,
+                      const double* X, double* force, double* torque) {
+    World& w = W(wp);
+    std::vector<V3> f(nb, zero3()), t(nb, zero3());
+    for (uint64_t k = 0; k < ns; ++k) {
+        const int64_t b = body[k], i = particle[k];
+        const V3 fb = (size_t)i < w.boundary_force.size() ? w.boundary_force[i] : zero3();
+        f[b] += fb;
+        const V3 r = w.parts.x[i] - V3{X[3 * b], X[3 * b + 1], X[3 * b + 2]};
+        t[b] += cross3(r, fb);
+    }
+    put3(f, force);
+    put3(t, torque);
+}
 void ow_get_rho(OWorld* w, double* out) { std::copy(W(w).parts.rho.begin(), W(w).parts.rho.end(), out); }
 void ow_get_p(OWorld* w, double* out) { std::copy(W(w).parts.p.begin(), W(w).parts.p.end(), out); }
 void ow_set_x(OWorld* w, const double* in) { get3(W(w).parts.x, in); }

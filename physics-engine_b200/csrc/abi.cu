@@ -12,6 +12,7 @@
 #include "../../include/pe_fluid_wcsph.h"
 #include "pe_math.cuh"
 #include "handles.cuh"
+#include "coupling.cuh"
 #include "world.cuh"
 
 struct PeParticles {
@@ -899,3 +900,57 @@ double pe_fluid_suggested_dt(double h, double sound_speed, double v_max, double 
 const char* pe_fluid_version(void) { return "physics-engine-b200 wcsph 0.1.0 (sm_100a)"; }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------- coupling
+
+struct PeCoupler {
+    pe::Coupler* c;
+    PeWcsph* w;
+};
+
+int pe_fluid_coupler_create(PeWcsph* w, uint32_t n_bodies, uint64_t n_samples, const int64_t* body,
+                            const double* local, const double* local_n, const int64_t* particle,
+                            PeCoupler** out) {
+    if (!w || !out) return PE_ERR_NULL;
+    *out = nullptr;
+    if (n_samples && (!body || !local || !local_n || !particle)) return PE_ERR_NULL;
+    const uint64_t n = w->world->len();
+    for (uint64_t k = 0; k < n_samples; ++k) {
+        if (body[k] < 0 || (uint64_t)body[k] >= n_bodies || particle[k] < 0 || (uint64_t)particle[k] >= n)
+            return PE_ERR_BOUNDS;
+        if (!finite3(local + 3 * k) || !finite3(local_n + 3 * k)) return PE_ERR_ARG;
+    }
+    return guard([&] {
+        *out = new PeCoupler{new pe::Coupler(*w->world, n_bodies, n_samples, body, local, local_n, particle), w};
+        return PE_OK;
+    });
+}
+
+void pe_fluid_coupler_destroy(PeCoupler* c) {
+    if (!c) return;
+    try {
+        delete c->c;
+    } catch (...) {
+    }
+    delete c;
+}
+
+int pe_fluid_coupler_sync(PeCoupler* c, const double* X, const double* Q, const double* V, const double* omega) {
+    if (!c || (c->c->bodies() && (!X || !Q || !V || !omega))) return PE_ERR_NULL;
+    for (uint32_t b = 0; b < c->c->bodies(); ++b)
+        if (!finite3(X + 3 * b) || !finite3(V + 3 * b) || !finite3(omega + 3 * b) || !finite3(Q + 4 * b) ||
+            !std::isfinite(Q[4 * b + 3]))
+            return PE_ERR_ARG;
+    return guard([&] {
+        c->c->sync(X, Q, V, omega);
+        return PE_OK;
+    });
+}
+
+int pe_fluid_coupler_reduce(PeCoupler* c, const double* X, double* force, double* torque) {
+    if (!c || (c->c->bodies() && (!X || !force || !torque))) return PE_ERR_NULL;
+    return guard([&] {
+        c->c->reduce(X, force, torque);
+        return PE_OK;
+    });
+}

@@ -41,6 +41,7 @@ class CudaError : public std::runtime_error {
 };
 
 class Surrogate;
+class Coupler;
 
 class World {
    public:
@@ -141,6 +142,7 @@ class World {
 
    private:
     friend class Surrogate;
+    friend class Coupler;
     void save_checkpoint();
     void restore_checkpoint();
     double4 *ck_pos_ = nullptr, *ck_vel_ = nullptr;

@@ -186,6 +186,10 @@ def load_library():
         "pe_fluid_wcsph_profile": (C.c_int, [vp, i32]),
         "pe_fluid_wcsph_profile_read": (C.c_int, [vp, C.POINTER(_Profile), i32]),
         "pe_fluid_wcsph_stream": (C.c_int, [vp, C.POINTER(vp)]),
+        "pe_fluid_coupler_create": (C.c_int, [vp, u32, u64, vp, vp, vp, vp, C.POINTER(vp)]),
+        "pe_fluid_coupler_destroy": (None, [vp]),
+        "pe_fluid_coupler_sync": (C.c_int, [vp, vp, vp, vp, vp]),
+        "pe_fluid_coupler_reduce": (C.c_int, [vp, vp, vp, vp]),
         "pe_fluid_kernel_w": (d, [i32, d, d, i32]),
         "pe_fluid_grad_w": (C.c_int, [i32, D3, d, i32, D3]),
         "pe_fluid_tait_pressure": (d, [d, d, d, d]),
@@ -674,6 +678,60 @@ class WcsphWorld:
 # --------------------------------------------------------------------------
 # stateless helpers
 # --------------------------------------------------------------------------
+# --------------------------------------------------------------------------
+# Fluid side of the WCSPH-rigid coupling (crates/pe-fluid/src/coupling.rs)
+# --------------------------------------------------------------------------
+class FluidRigidCoupler:
+    """The rigid samples of a world (`FluidRigidCoupler`, coupling.rs:42-51).
+
+    Sample k is world particle `particle[k]`, an oriented boundary sample on
+    body `body[k]` at body-frame offset `local[k]` with body-frame normal
+    `local_n[k]`. The rigid bodies stay with the caller: each coupled step
+    (`CoupledWcsphWorld::step`, coupling.rs:853-866) is `sync_from_rigid`,
+    `world.step(dt)`, `reduce_with_state`, then the caller's rigid step.
+    """
+
+    def __init__(self, world: "WcsphWorld", n_bodies: int, body, local, local_n, particle):
+        L = load_library()
+        body = _arr(body, np.int64, (-1,))
+        ns = body.shape[0]
+        self._keep = (_arr(local, np.float64, (ns, 3)), _arr(local_n, np.float64, (ns, 3)),
+                      _arr(particle, np.int64, (ns,)))
+        self.n_bodies, self.n_samples, self.world = int(n_bodies), ns, world
+        self.body = body
+        h = C.c_void_p()
+        _ok(L.pe_fluid_coupler_create(world._w, self.n_bodies, ns, _ptr(body), _ptr(self._keep[0]),
+                                      _ptr(self._keep[1]), _ptr(self._keep[2]), C.byref(h)), "coupler_create")
+        self._c = h
+
+    def close(self):
+        if getattr(self, "_c", None) and _lib is not None:
+            _lib.pe_fluid_coupler_destroy(self._c)
+        self._c = None
+
+    def __del__(self):
+        self.close()
+
+    def sync_from_rigid(self, x, q, v, omega):
+        """Sample positions, velocities and normals from per-body centre of mass
+        `x`, orientation `q` (w, x, y, z), velocity `v` and world-frame angular
+        velocity `omega` (`sync_from_rigid`, coupling.rs:289-306)."""
+        nb = self.n_bodies
+        a = [_arr(x, np.float64, (nb, 3)), _arr(q, np.float64, (nb, 4)), _arr(v, np.float64, (nb, 3)),
+             _arr(omega, np.float64, (nb, 3))]
+        _ok(_lib.pe_fluid_coupler_sync(self._c, *[_ptr(t) for t in a]), "coupler_sync")
+
+    def reduce_with_state(self, x):
+        """Per-body (force, torque) of the samples' boundary reactions about the
+        centres of mass `x` (`reduce_with_state`, coupling.rs:308-330)."""
+        nb = self.n_bodies
+        xb = _arr(x, np.float64, (nb, 3))
+        f = np.empty((nb, 3))
+        t = np.empty((nb, 3))
+        _ok(_lib.pe_fluid_coupler_reduce(self._c, _ptr(xb), _ptr(f), _ptr(t)), "coupler_reduce")
+        return f, t
+
+
 def kernel_w(kernel, r, h, dim):
     return load_library().pe_fluid_kernel_w(int(kernel), float(r), float(h), int(dim))
 
