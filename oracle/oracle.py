@@ -40,6 +40,70 @@ class OParams(C.Structure):
     ]
 
 
+
+class PParams(C.Structure):
+    """Mirror of `PParams` in wcsph_oracle.cpp (fields of `PbfParams`, pbf.rs:26-53)."""
+
+    _fields_ = [
+        ("density_kernel", C.c_int32),
+        ("grad_kernel", C.c_int32),
+        ("iterations", C.c_int64),
+        ("epsilon_lambda", C.c_double),
+        ("art_pressure_k", C.c_double),
+        ("art_pressure_n", C.c_double),
+        ("art_pressure_dq_over_h", C.c_double),
+        ("viscosity_eps", C.c_double),
+        ("vorticity_eps", C.c_double),
+        ("gravity", C.c_double * 3),
+        ("reuse_neighbours", C.c_int32),
+    ]
+
+
+def pbf_default_params() -> PParams:
+    """`PbfParams::default` (pbf.rs:55-74)."""
+    p = PParams()
+    p.density_kernel, p.grad_kernel, p.iterations = POLY6, SPIKY, 5
+    p.epsilon_lambda, p.art_pressure_k, p.art_pressure_n, p.art_pressure_dq_over_h = 0.01, 0.01, 4.0, 0.25
+    p.viscosity_eps, p.vorticity_eps = 0.01, 0.0
+    p.gravity[:] = (0.0, 0.0, -9.80665)
+    p.reuse_neighbours = 1
+    return p
+
+
+class DParams(C.Structure):
+    """Mirror of `DParams` in wcsph_oracle.cpp (fields of `DfsphParams`,
+    dfsph.rs:33-80; the four free-slip planes as flag + value)."""
+
+    _fields_ = [
+        ("kernel", C.c_int32),
+        ("max_density_iters", C.c_int64),
+        ("max_divergence_iters", C.c_int64),
+        ("density_error_tol", C.c_double),
+        ("divergence_error_tol", C.c_double),
+        ("gravity", C.c_double * 3),
+        ("xsph_epsilon", C.c_double),
+        ("particle_diameter", C.c_double),
+        ("cfl_lambda", C.c_double),
+        ("adaptive_dt", C.c_int32),
+        ("warm_start", C.c_int32),
+        ("has_slip", C.c_int32 * 4),
+        ("slip", C.c_double * 4),
+        ("solver_omega", C.c_double),
+        ("max_velocity_correction", C.c_double),
+    ]
+
+
+def dfsph_default_params() -> DParams:
+    """`DfsphParams::default` (dfsph.rs:82-104)."""
+    p = DParams()
+    p.kernel, p.max_density_iters, p.max_divergence_iters = CUBIC, 50, 50
+    p.density_error_tol, p.divergence_error_tol = 0.001, 0.001
+    p.gravity[:] = (0.0, 0.0, -9.80665)
+    p.xsph_epsilon, p.particle_diameter, p.cfl_lambda = 0.05, 0.0, 0.4
+    p.adaptive_dt, p.warm_start = 1, 1
+    p.solver_omega, p.max_velocity_correction = 1.0, 0.0
+    return p
+
 def water_params(rest_density, sound_speed, gravity, materialize=True) -> OParams:
     """`WcsphParams::water` defaults (wcsph.rs:43-53, viscosity.rs:39,82)."""
     p = OParams()
@@ -124,6 +188,28 @@ def lib():
             "o_mean_density_error": (d, [vp]),
             "o_max_density_error": (d, [vp]),
             "o_suggested_dt": (d, [d, d, d, d, d, d]),
+            "opbf_create": (vp, [vp, C.POINTER(PParams)]),
+            "opbf_free": (None, [vp]),
+            "opbf_run": (None, [vp, d, i64]),
+            "opbf_hash": (u64, [vp]),
+            "opbf_time": (d, [vp]),
+            "opbf_get_x": (None, [vp, vp]),
+            "opbf_get_v": (None, [vp, vp]),
+            "opbf_get_rho": (None, [vp, vp]),
+            "opbf_get_lambda": (None, [vp, vp]),
+            "odfsph_create": (vp, [vp, C.POINTER(DParams)]),
+            "odfsph_free": (None, [vp]),
+            "odfsph_run": (None, [vp, d, i64]),
+            "odfsph_step_adaptive": (d, [vp]),
+            "odfsph_hash": (u64, [vp]),
+            "odfsph_time": (d, [vp]),
+            "odfsph_iters": (None, [vp, vp]),
+            "odfsph_get_x": (None, [vp, vp]),
+            "odfsph_get_v": (None, [vp, vp]),
+            "odfsph_get_boundary_force": (None, [vp, vp]),
+            "odfsph_get_rho": (None, [vp, vp]),
+            "odfsph_get_p": (None, [vp, vp]),
+            "odfsph_get_alpha": (None, [vp, vp]),
             "o_coupler_sync": (None, [vp, u64, vp, vp, vp, vp, vp, vp, vp, vp]),
             "o_coupler_reduce": (None, [vp, u64, vp, vp, u64, vp, vp, vp]),
         }
@@ -316,6 +402,139 @@ class World:
         return lib().o_max_density_error(self._w)
 
 
+
+
+class PbfWorld:
+    """`PbfWorld` restated (pbf.rs:77-459)."""
+
+    def __init__(self, scene: Scene, params: PParams):
+        self.params = params
+        self._w = lib().opbf_create(scene._s, C.byref(params))
+        self.n = len(scene)
+
+    def __del__(self):
+        if getattr(self, "_w", None):
+            lib().opbf_free(self._w)
+            self._w = None
+
+    def run(self, dt, steps):
+        lib().opbf_run(self._w, dt, steps)
+
+    def step(self, dt):
+        self.run(dt, 1)
+
+    @property
+    def t(self):
+        return lib().opbf_time(self._w)
+
+    def hash64(self):
+        return lib().opbf_hash(self._w)
+
+    def _get(self, fn, shape):
+        out = np.empty(shape)
+        fn(self._w, _ptr(out))
+        return out
+
+    def x(self):
+        return self._get(lib().opbf_get_x, (self.n, 3))
+
+    def v(self):
+        return self._get(lib().opbf_get_v, (self.n, 3))
+
+    def rho(self):
+        return self._get(lib().opbf_get_rho, (self.n,))
+
+    def lam(self):
+        return self._get(lib().opbf_get_lambda, (self.n,))
+
+
+def pbf_hash_world():
+    """The reference's canonical PBF tank (scenarios.rs:28-61): a 4x4x4 block,
+    dx 0.05, h 2 dx, in a 0.4 x 0.4 x 0.45 shell; 4 iterations, no tensile
+    correction, no vorticity."""
+    dx, rho0 = 0.05, 1000.0
+    s = Scene(3, rho0, mass_from_spacing(rho0, dx, 3), 2.0 * dx)
+    s.fill_box((0.1, 0.1, 0.1), 4, 4, 4, dx)
+    s.fill_box_boundary((0.0, 0.0, 0.0), (0.4, 0.4, 0.45), dx, 1)
+    p = pbf_default_params()
+    p.gravity[:] = (0.0, 0.0, -9.80665)
+    p.iterations, p.art_pressure_k, p.vorticity_eps = 4, 0.0, 0.0
+    return PbfWorld(s, p)
+
+
+class DfsphWorld:
+    """`DfsphWorld` restated (dfsph.rs:107-800)."""
+
+    def __init__(self, scene: Scene, params: DParams):
+        self.params = params
+        self._w = lib().odfsph_create(scene._s, C.byref(params))
+        self.n = len(scene)
+
+    def __del__(self):
+        if getattr(self, "_w", None):
+            lib().odfsph_free(self._w)
+            self._w = None
+
+    def run(self, dt, steps):
+        lib().odfsph_run(self._w, dt, steps)
+
+    def step(self, dt):
+        self.run(dt, 1)
+
+    def step_adaptive(self):
+        return lib().odfsph_step_adaptive(self._w)
+
+    @property
+    def t(self):
+        return lib().odfsph_time(self._w)
+
+    def hash64(self):
+        return lib().odfsph_hash(self._w)
+
+    def iterations(self):
+        out = np.zeros(2, np.int64)
+        lib().odfsph_iters(self._w, _ptr(out))
+        return int(out[0]), int(out[1])
+
+    def _get(self, fn, shape):
+        out = np.empty(shape)
+        fn(self._w, _ptr(out))
+        return out
+
+    def x(self):
+        return self._get(lib().odfsph_get_x, (self.n, 3))
+
+    def v(self):
+        return self._get(lib().odfsph_get_v, (self.n, 3))
+
+    def boundary_force(self):
+        return self._get(lib().odfsph_get_boundary_force, (self.n, 3))
+
+    def rho(self):
+        return self._get(lib().odfsph_get_rho, (self.n,))
+
+    def p(self):
+        return self._get(lib().odfsph_get_p, (self.n,))
+
+    def alpha(self):
+        return self._get(lib().odfsph_get_alpha, (self.n,))
+
+
+def dfsph_hash_world():
+    """The reference's canonical DFSPH tank (scenarios.rs:76-116): the PBF
+    tank's geometry with the calibrated mass and recomputed Akinci volumes."""
+    dx, rho0 = 0.05, 1000.0
+    h = 2.0 * dx
+    s = Scene(3, rho0, mass_calibrated_to_rest(rho0, dx, h, 3, CUBIC), h)
+    s.fill_box((0.1, 0.1, 0.1), 4, 4, 4, dx)
+    s.fill_box_boundary((0.0, 0.0, 0.0), (0.4, 0.4, 0.45), dx, 1)
+    s.recompute_psi(CUBIC)
+    p = dfsph_default_params()
+    p.particle_diameter = dx
+    p.density_error_tol, p.divergence_error_tol = 0.01, 0.01
+    p.max_density_iters, p.max_divergence_iters = 8, 8
+    p.xsph_epsilon, p.adaptive_dt, p.warm_start = 0.05, 0, 1
+    return DfsphWorld(s, p)
 
 class Coupler:
     """`FluidRigidCoupler` restated (coupling.rs:42-51, 289-330): sample k is

@@ -1,7 +1,8 @@
 // TEST INFRASTRUCTURE — NOT PART OF THE PRODUCT.
 //
 // CPU oracle: an order-exact C++ restatement of eranyid/physics-engine's
-// `pe-fluid` WCSPH solver path (Rust). Only the test suite, the smoke check
+// `pe-fluid` WCSPH solver path (Rust), with its PBF and DFSPH siblings and the
+// fluid side of the rigid coupling. Only the test suite, the smoke check
 // and the CPU-baseline leg of bench.py load this library; the product
 // (physics-engine_b200/) never links, calls or falls back to it.
 //
@@ -18,7 +19,9 @@
 // is restated as a correctly rounded integer power evaluated in binary128
 // (`oracle_pow`), falling back to the C library for non-integer exponents.
 // The crate's pow is documented as "nearly rounded", so the two agree except
-// in rare last-ulp cases; parity at the pow boundary is therefore unpinned.
+// in rare last-ulp cases. The PBF and DFSPH restatements below reproduce the
+// reference's locked tank hashes (9d9e0da856fd43d4, f1f2825b5eeaab0d), which
+// pins the pow normalisations of the poly6 and spiky kernels.
 
 #include <algorithm>
 #include <cmath>
@@ -699,6 +702,639 @@ static uint64_t particles_hash64(const Particles& p) {
     return h;
 }
 
+
+// ---------------------------------------------------------------------------
+// Position Based Fluids (pbf.rs:25-459)
+// ---------------------------------------------------------------------------
+static inline V3 cross(V3 a, V3 b) {  // vec3.rs:87-93
+    return V3{a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+
+struct PParams {                 // pbf.rs:26-53
+    int32_t density_kernel, grad_kernel;
+    int64_t iterations;
+    double epsilon_lambda, art_pressure_k, art_pressure_n, art_pressure_dq_over_h;
+    double viscosity_eps, vorticity_eps;
+    double gravity[3];
+    int32_t reuse_neighbours;
+};
+
+struct PbfWorld {
+    Particles parts;
+    UniformGrid grid;
+    PParams prm;
+    double t = 0.0;
+    std::vector<V3> pred, dp, dv_scratch, omega_scratch;
+    std::vector<double> lambda, rho_pred;
+    std::vector<std::vector<size_t>> neigh_lists;
+
+    KernelKind dk() const { return (KernelKind)prm.density_kernel; }
+    KernelKind gk() const { return (KernelKind)prm.grad_kernel; }
+
+    // pbf.rs:112-130 new: the grid cell is the larger support radius
+    PbfWorld(const Particles& p, const PParams& q) : parts(p), prm(q) {
+        double s0 = support_radius(dk(), parts.h), s1 = support_radius(gk(), parts.h);
+        grid.cell_size = std::fmax(s0, s1);
+        grid.dim = parts.dim;
+        ensure_buffers();
+    }
+    // pbf.rs:132-144
+    void ensure_buffers() {
+        size_t n = parts.len();
+        pred.resize(n, zero3());
+        lambda.resize(n, 0.0);
+        dp.resize(n, zero3());
+        rho_pred.resize(n, 0.0);
+        dv_scratch.resize(n, zero3());
+        omega_scratch.resize(n, zero3());
+        neigh_lists.resize(n);
+    }
+    // pbf.rs:146-156: lists for fluid particles only
+    void rebuild_neighbours(const std::vector<V3>& pos) {
+        grid.rebuild(pos);
+        for (size_t i = 0; i < parts.len(); ++i) {
+            neigh_lists[i].clear();
+            if (parts.kind[i] == FLUID) grid.neighbours(i, neigh_lists[i]);
+        }
+    }
+    // pbf.rs:159-187
+    void density_at_pred() {
+        const double h = parts.h, mass = parts.mass, rho0 = parts.rest_density;
+        const Dim dim = parts.dim;
+        for (size_t i = 0; i < parts.len(); ++i) {
+            if (parts.kind[i] != FLUID) {
+                rho_pred[i] = rho0;
+                parts.rho[i] = rho0;
+                continue;
+            }
+            V3 xi = pred[i];
+            double rho = mass * kern_w(dk(), 0.0, h, dim);
+            for (size_t j : neigh_lists[i]) {
+                if (j == i) continue;
+                double r = norm(pred[j] - xi);
+                double wij = kern_w(dk(), r, h, dim);
+                if (parts.kind[j] == FLUID) rho += mass * wij;
+                else rho += rho0 * parts.psi[j] * wij;
+            }
+            rho_pred[i] = std::fmax(rho, 1e-12);
+            parts.rho[i] = rho_pred[i];
+        }
+    }
+    // pbf.rs:189-227
+    void compute_lambdas() {
+        const double h = parts.h, mass = parts.mass, rho0 = parts.rest_density, eps = prm.epsilon_lambda;
+        const Dim dim = parts.dim;
+        for (size_t i = 0; i < parts.len(); ++i) {
+            if (parts.kind[i] != FLUID) {
+                lambda[i] = 0.0;
+                continue;
+            }
+            double ci = rho_pred[i] / rho0 - 1.0;
+            V3 xi = pred[i];
+            double sum_grad_sq = 0.0;
+            V3 grad_i = zero3();
+            for (size_t j : neigh_lists[i]) {
+                if (j == i) continue;
+                V3 gw = grad_w(gk(), pred[j] - xi, h, dim);
+                double scale = parts.kind[j] == FLUID ? mass / rho0 : parts.psi[j];
+                V3 contrib = gw * scale;
+                grad_i += contrib;
+                if (parts.kind[j] == FLUID) sum_grad_sq += norm2(contrib);
+            }
+            sum_grad_sq += norm2(grad_i);
+            lambda[i] = -ci / (sum_grad_sq + eps);
+        }
+    }
+    // pbf.rs:229-235
+    double artificial_pressure(double wij, double w_dq) const {
+        if (w_dq <= 1e-30 || prm.art_pressure_k == 0.0) return 0.0;
+        double ratio = std::fmin(wij / w_dq, 1.0);
+        return -prm.art_pressure_k * oracle_pow(ratio, prm.art_pressure_n);
+    }
+    // pbf.rs:237-286
+    void compute_delta_p() {
+        const double h = parts.h, mass = parts.mass, rho0 = parts.rest_density;
+        const Dim dim = parts.dim;
+        const double dq = prm.art_pressure_dq_over_h * h;
+        const double w_dq = kern_w(dk(), dq, h, dim);
+        for (auto& d : dp) d = zero3();
+        for (size_t i = 0; i < parts.len(); ++i) {
+            if (parts.kind[i] != FLUID) continue;
+            V3 xi = pred[i];
+            V3 corr = zero3();
+            for (size_t j : neigh_lists[i]) {
+                if (j == i) continue;
+                V3 rij = pred[j] - xi;
+                double r = norm(rij);
+                double wij = kern_w(dk(), r, h, dim);
+                V3 gw = grad_w(gk(), rij, h, dim);
+                double s_corr = artificial_pressure(wij, w_dq);
+                if (parts.kind[j] == FLUID) {
+                    double coeff = lambda[i] + lambda[j] + s_corr;
+                    corr += gw * (mass / rho0 * coeff);
+                } else {
+                    double coeff = lambda[i] + s_corr;
+                    corr += gw * (parts.psi[j] * coeff);
+                }
+            }
+            double max_corr = 0.4 * h;
+            double mag = norm(corr);
+            if (mag > max_corr && mag > 0.0) corr = corr * (max_corr / mag);
+            dp[i] = corr;
+        }
+    }
+    // pbf.rs:288-381
+    void apply_viscosity_and_vorticity(double dt) {
+        const double h = parts.h, mass = parts.mass;
+        const Dim dim = parts.dim;
+        rebuild_neighbours(parts.x);
+        const size_t n = parts.len();
+        if (prm.viscosity_eps != 0.0) {
+            for (auto& d : dv_scratch) d = zero3();
+            for (size_t i = 0; i < n; ++i) {
+                if (parts.kind[i] != FLUID) continue;
+                V3 xi = parts.x[i], vi = parts.v[i];
+                V3 corr = zero3();
+                for (size_t j : neigh_lists[i]) {
+                    if (j == i || parts.kind[j] != FLUID) continue;
+                    double r = norm(parts.x[j] - xi);
+                    double wij = kern_w(dk(), r, h, dim);
+                    double rho_bar = 0.5 * (parts.rho[i] + parts.rho[j]);
+                    corr += (parts.v[j] - vi) * (mass / std::fmax(rho_bar, 1e-12) * wij);
+                }
+                dv_scratch[i] = corr * prm.viscosity_eps;
+            }
+            for (size_t i = 0; i < n; ++i) parts.v[i] += dv_scratch[i];
+        }
+        if (prm.vorticity_eps == 0.0 || dt == 0.0) return;
+        for (auto& o : omega_scratch) o = zero3();
+        for (size_t i = 0; i < n; ++i) {
+            if (parts.kind[i] != FLUID) continue;
+            V3 xi = parts.x[i], vi = parts.v[i];
+            V3 w_i = zero3();
+            for (size_t j : neigh_lists[i]) {
+                if (j == i || parts.kind[j] != FLUID) continue;
+                V3 gw = grad_w(gk(), parts.x[j] - xi, h, dim);
+                double rho_bar = 0.5 * (parts.rho[i] + parts.rho[j]);
+                w_i += cross(parts.v[j] - vi, gw) * (mass / std::fmax(rho_bar, 1e-12));
+            }
+            omega_scratch[i] = w_i;
+        }
+        for (size_t i = 0; i < n; ++i) {
+            if (parts.kind[i] != FLUID) continue;
+            V3 xi = parts.x[i];
+            V3 eta = zero3();
+            double om_i = norm(omega_scratch[i]);
+            for (size_t j : neigh_lists[i]) {
+                if (j == i || parts.kind[j] != FLUID) continue;
+                V3 gw = grad_w(gk(), parts.x[j] - xi, h, dim);
+                double rho_bar = 0.5 * (parts.rho[i] + parts.rho[j]);
+                eta += gw * (mass / std::fmax(rho_bar, 1e-12) * (norm(omega_scratch[j]) - om_i));
+            }
+            double nrm = norm(eta);
+            if (nrm > 1e-12) {
+                V3 n_hat{eta.x / nrm, eta.y / nrm, eta.z / nrm};
+                V3 f = cross(n_hat, omega_scratch[i]) * prm.vorticity_eps;
+                parts.v[i] += f * dt;
+            }
+        }
+    }
+    // pbf.rs:384-436
+    void step(double dt) {
+        ensure_buffers();
+        const size_t n = parts.len();
+        const V3 g{prm.gravity[0], prm.gravity[1], prm.gravity[2]};
+        for (size_t i = 0; i < n; ++i) {
+            if (parts.kind[i] != FLUID) {
+                pred[i] = parts.x[i];
+                continue;
+            }
+            parts.v[i] += g * dt;
+            pred[i] = parts.x[i] + parts.v[i] * dt;
+            if (parts.dim == D2) {
+                pred[i].z = 0.0;
+                parts.v[i].z = 0.0;
+            }
+        }
+        rebuild_neighbours(pred);
+        for (int64_t it = 0; it < prm.iterations; ++it) {
+            density_at_pred();
+            compute_lambdas();
+            compute_delta_p();
+            for (size_t i = 0; i < n; ++i)
+                if (parts.kind[i] == FLUID) {
+                    pred[i] += dp[i];
+                    if (parts.dim == D2) pred[i].z = 0.0;
+                }
+            if (!prm.reuse_neighbours) rebuild_neighbours(pred);
+        }
+        for (size_t i = 0; i < n; ++i) {
+            if (parts.kind[i] != FLUID) continue;
+            if (dt > 0.0) parts.v[i] = (pred[i] - parts.x[i]) * (1.0 / dt);
+            parts.x[i] = pred[i];
+        }
+        for (size_t i = 0; i < n; ++i) pred[i] = parts.x[i];
+        rebuild_neighbours(pred);
+        density_at_pred();
+        apply_viscosity_and_vorticity(dt);
+        t += dt;
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Divergence-free SPH (dfsph.rs:33-800); surface tension (sigma != 0) is not
+// restated.
+// ---------------------------------------------------------------------------
+struct DParams {                 // dfsph.rs:33-80
+    int32_t kernel;
+    int64_t max_density_iters, max_divergence_iters;
+    double density_error_tol, divergence_error_tol;
+    double gravity[3];
+    double xsph_epsilon;
+    double particle_diameter, cfl_lambda;
+    int32_t adaptive_dt, warm_start;
+    int32_t has_slip[4];         // free_slip_{xmin, ymin, xmax, ymax}.is_some()
+    double slip[4];
+    double solver_omega, max_velocity_correction;
+};
+
+// cfl.rs:36 suggested_dt
+static double cfl_suggested_dt(double h, double c, double vmax, double amax, double lv, double lf) {
+    double dt_v = lv * h / std::fmax(c + vmax, 1e-12);
+    double dt_f = amax > 1e-12 ? lf * std::sqrt(h / amax) : std::numeric_limits<double>::infinity();
+    return std::fmin(dt_v, dt_f);
+}
+
+struct DfsphWorld {
+    Particles parts;
+    UniformGrid grid;
+    DParams prm;
+    double t = 0.0, last_dt = 0.0;
+    std::vector<double> alpha, kappa, kappa_v, kappa_warm, kappa_v_warm;
+    std::vector<V3> v_star, a_adv, scratch_dv, dv_bound, boundary_force;
+    std::vector<std::vector<size_t>> neigh_lists;
+    std::vector<std::pair<size_t, double>> reaction_tmp;
+    int64_t last_density_iters = 0, last_divergence_iters = 0;
+
+    KernelKind kk() const { return (KernelKind)prm.kernel; }
+
+    // dfsph.rs:137-180 new
+    DfsphWorld(const Particles& p, const DParams& q) : parts(p), prm(q) {
+        if (prm.particle_diameter <= 0.0) prm.particle_diameter = parts.h;
+        grid.cell_size = support_radius(kk(), parts.h);
+        grid.dim = parts.dim;
+        if (parts.dim == D2)
+            for (size_t i = 0; i < parts.len(); ++i) {
+                parts.x[i].z = 0.0;
+                parts.v[i].z = 0.0;
+            }
+        rebuild_neighbours();
+        compute_density();
+        compute_alpha();
+    }
+    // dfsph.rs:182-198
+    void ensure_buffers() {
+        size_t n = parts.len();
+        alpha.resize(n, 0.0);
+        v_star.resize(n, zero3());
+        kappa.resize(n, 0.0);
+        kappa_v.resize(n, 0.0);
+        kappa_warm.resize(n, 0.0);
+        kappa_v_warm.resize(n, 0.0);
+        a_adv.resize(n, zero3());
+        scratch_dv.resize(n, zero3());
+        dv_bound.resize(n, zero3());
+        boundary_force.resize(n, zero3());
+        neigh_lists.resize(n);
+    }
+    // dfsph.rs:201-211
+    void rebuild_neighbours() {
+        ensure_buffers();
+        grid.rebuild(parts.x);
+        for (size_t i = 0; i < parts.len(); ++i) {
+            neigh_lists[i].clear();
+            if (parts.kind[i] == FLUID) grid.neighbours(i, neigh_lists[i]);
+        }
+    }
+    // dfsph.rs:214-244
+    void compute_density() {
+        const double h = parts.h, mass = parts.mass, rho0 = parts.rest_density;
+        const Dim dim = parts.dim;
+        for (size_t i = 0; i < parts.len(); ++i) {
+            if (parts.kind[i] != FLUID) {
+                parts.rho[i] = rho0;
+                continue;
+            }
+            V3 xi = parts.x[i];
+            double rho = mass * kern_w(kk(), 0.0, h, dim);
+            for (size_t j : neigh_lists[i]) {
+                if (j == i) continue;
+                double wij = kern_w(kk(), norm(parts.x[j] - xi), h, dim);
+                if (parts.kind[j] == FLUID) rho += mass * wij;
+                else if (parts.boundary_sees_fluid(j, xi)) rho += rho0 * parts.psi[j] * wij;
+            }
+            parts.rho[i] = std::fmax(rho, 1e-12);
+        }
+    }
+    // dfsph.rs:252-307
+    void compute_alpha() {
+        const double h = parts.h, mass = parts.mass, rho0 = parts.rest_density;
+        const Dim dim = parts.dim;
+        double h_safe = std::fmax(h, 1e-12);
+        double char_grad = dim == D2 ? mass / (h_safe * h_safe * h_safe) : mass / (h_safe * h_safe * h_safe * h_safe);
+        double denom_floor = std::fmax(1e-6 * char_grad * char_grad, 1e-12);
+        for (size_t i = 0; i < parts.len(); ++i) {
+            if (parts.kind[i] != FLUID) {
+                alpha[i] = 0.0;
+                continue;
+            }
+            V3 xi = parts.x[i];
+            V3 sum_grad = zero3();
+            double sum_grad_sq = 0.0;
+            size_t n_nbr = 0;
+            for (size_t j : neigh_lists[i]) {
+                if (j == i) continue;
+                V3 gw = grad_w(kk(), parts.x[j] - xi, h, dim);
+                double mj = parts.kind[j] == FLUID ? mass
+                            : (parts.boundary_sees_fluid(j, xi) ? rho0 * parts.psi[j] : 0.0);
+                if (mj == 0.0 && parts.kind[j] == BOUNDARY) continue;
+                V3 g = gw * mj;
+                sum_grad += g;
+                sum_grad_sq += norm2(g);
+                n_nbr += 1;
+            }
+            if (n_nbr < 2) {
+                alpha[i] = 0.0;
+                continue;
+            }
+            double denom = std::fmax(norm2(sum_grad) + sum_grad_sq, denom_floor);
+            alpha[i] = parts.rho[i] / denom;
+        }
+    }
+    // dfsph.rs:309-323
+    double neighbour_mass_for(size_t i, size_t j) const {
+        if (parts.kind[j] == FLUID) return parts.mass;
+        return parts.boundary_sees_fluid(j, parts.x[i]) ? parts.rest_density * parts.psi[j] : 0.0;
+    }
+    // dfsph.rs:326-351
+    double density_derivative(size_t i) const {
+        const double h = parts.h;
+        const Dim dim = parts.dim;
+        V3 xi = parts.x[i], vi = v_star[i];
+        double drho = 0.0;
+        for (size_t j : neigh_lists[i]) {
+            if (j == i) continue;
+            double mj = neighbour_mass_for(i, j);
+            if (mj == 0.0) continue;
+            V3 gw = grad_w(kk(), parts.x[j] - xi, h, dim);
+            V3 vj = parts.kind[j] == FLUID ? v_star[j] : parts.v[j];
+            drho += mj * dot(vi - vj, gw);
+        }
+        return drho;
+    }
+    // dfsph.rs:353-379 (surface tension not restated)
+    void compute_nonpressure_accel() {
+        const V3 g{prm.gravity[0], prm.gravity[1], prm.gravity[2]};
+        for (size_t i = 0; i < parts.len(); ++i) a_adv[i] = parts.kind[i] == FLUID ? g : zero3();
+    }
+    // dfsph.rs:382-416
+    void apply_xsph_on_vstar() {
+        const double eps = prm.xsph_epsilon;
+        if (eps == 0.0) return;
+        const double h = parts.h, mass = parts.mass;
+        const Dim dim = parts.dim;
+        for (auto& d : scratch_dv) d = zero3();
+        for (size_t i = 0; i < parts.len(); ++i) {
+            if (parts.kind[i] != FLUID) continue;
+            V3 xi = parts.x[i], vi = v_star[i];
+            double rho_i = parts.rho[i];
+            V3 dv = zero3();
+            for (size_t j : neigh_lists[i]) {
+                if (j == i || parts.kind[j] != FLUID) continue;
+                double wij = kern_w(kk(), norm(parts.x[j] - xi), h, dim);
+                double rho_bar = 0.5 * (rho_i + parts.rho[j]);
+                dv += (v_star[j] - vi) * (mass / std::fmax(rho_bar, 1e-12) * wij);
+            }
+            scratch_dv[i] = dv * eps;
+        }
+        for (size_t i = 0; i < parts.len(); ++i)
+            if (parts.kind[i] == FLUID) v_star[i] += scratch_dv[i];
+    }
+    // dfsph.rs:422-530
+    void apply_pressure_velocity_update(double dt, bool use_divergence) {
+        const double h = parts.h;
+        const Dim dim = parts.dim;
+        const std::vector<double>& kap = use_divergence ? kappa_v : kappa;
+        const size_t n = parts.len();
+        for (auto& d : scratch_dv) d = zero3();
+        for (auto& d : dv_bound) d = zero3();
+        for (size_t i = 0; i < n; ++i) {
+            if (parts.kind[i] != FLUID) continue;
+            V3 xi = parts.x[i];
+            double rho_i = std::fmax(parts.rho[i], 1e-12);
+            double ki = kap[i];
+            V3 dv = zero3(), dv_b = zero3();
+            for (size_t j : neigh_lists[i]) {
+                if (j == i) continue;
+                double mj = neighbour_mass_for(i, j);
+                if (mj == 0.0) continue;
+                V3 gw = grad_w(kk(), parts.x[j] - xi, h, dim);
+                double kj = parts.kind[j] == FLUID ? kap[j] : 0.0;
+                double rho_j = parts.kind[j] == FLUID ? std::fmax(parts.rho[j], 1e-12) : parts.rest_density;
+                double coeff = mj * (ki / rho_i + kj / rho_j);
+                V3 term = gw * coeff;
+                dv += term;
+                if (parts.kind[j] == BOUNDARY) dv_b += term;
+            }
+            scratch_dv[i] = dv * (-dt);
+            dv_bound[i] = dv_b * (-dt);
+        }
+        const double dv_cap = prm.max_velocity_correction, mass = parts.mass;
+        const double inv_dt = 1.0 / std::fmax(dt, 1e-12);
+        for (size_t i = 0; i < n; ++i) {
+            if (parts.kind[i] != FLUID) continue;
+            V3 dv = scratch_dv[i];
+            double scale = 1.0;
+            if (dv_cap > 0.0) {
+                double s2 = norm2(dv);
+                if (s2 > dv_cap * dv_cap) {
+                    scale = dv_cap / std::sqrt(s2);
+                    dv = dv * scale;
+                }
+            }
+            V3 dv_b = dv_bound[i] * scale;
+            if (norm2(dv_b) > 0.0) {
+                V3 xi = parts.x[i];
+                double wsum = 0.0;
+                reaction_tmp.clear();
+                for (size_t j : neigh_lists[i]) {
+                    if (parts.kind[j] != BOUNDARY) continue;
+                    if (!parts.boundary_sees_fluid(j, xi)) continue;
+                    double r = norm(parts.x[j] - xi);
+                    double wt = std::fmin(1.0 / std::fmax(r, 1e-9), 1e6);
+                    wsum += wt;
+                    reaction_tmp.push_back({j, wt});
+                }
+                if (wsum > 0.0) {
+                    V3 fb_total = dv_b * (-mass * inv_dt);
+                    for (auto& jw : reaction_tmp) boundary_force[jw.first] += fb_total * (jw.second / wsum);
+                }
+            }
+            v_star[i] += dv;
+            if (parts.dim == D2) v_star[i].z = 0.0;
+        }
+    }
+    // dfsph.rs:533-584
+    int64_t correct_density_error(double dt) {
+        const size_t n = parts.len();
+        const double rho0 = parts.rest_density, dt2 = dt * dt;
+        int64_t iters = 0;
+        if (prm.warm_start) {
+            for (size_t i = 0; i < n; ++i) kappa[i] = kappa_warm[i];
+            apply_pressure_velocity_update(dt, false);
+        }
+        std::fill(kappa_warm.begin(), kappa_warm.end(), 0.0);
+        for (;;) {
+            double avg_err = 0.0;
+            size_t count = 0;
+            for (size_t i = 0; i < n; ++i) {
+                if (parts.kind[i] != FLUID) {
+                    kappa[i] = 0.0;
+                    continue;
+                }
+                double rho_star = parts.rho[i] + dt * density_derivative(i);
+                double err = std::fmax(rho_star - rho0, 0.0);
+                avg_err += err / rho0;
+                count += 1;
+                kappa[i] = prm.solver_omega * err / dt2 * alpha[i];
+                if (prm.warm_start) kappa_warm[i] += kappa[i];
+            }
+            if (count > 0) avg_err /= (double)count;
+            apply_pressure_velocity_update(dt, false);
+            iters += 1;
+            if ((avg_err <= prm.density_error_tol && iters >= 2) || iters >= prm.max_density_iters) break;
+        }
+        return iters;
+    }
+    // dfsph.rs:587-630
+    int64_t correct_divergence_error(double dt) {
+        const size_t n = parts.len();
+        const double rho0 = parts.rest_density;
+        int64_t iters = 0;
+        if (prm.warm_start) {
+            for (size_t i = 0; i < n; ++i) kappa_v[i] = kappa_v_warm[i];
+            apply_pressure_velocity_update(dt, true);
+        }
+        std::fill(kappa_v_warm.begin(), kappa_v_warm.end(), 0.0);
+        for (;;) {
+            double avg = 0.0;
+            size_t count = 0;
+            for (size_t i = 0; i < n; ++i) {
+                if (parts.kind[i] != FLUID) {
+                    kappa_v[i] = 0.0;
+                    continue;
+                }
+                double drho = std::fmax(density_derivative(i), 0.0);
+                avg += drho / rho0;
+                count += 1;
+                kappa_v[i] = prm.solver_omega * (1.0 / dt) * drho * alpha[i];
+                if (prm.warm_start) kappa_v_warm[i] += kappa_v[i];
+            }
+            if (count > 0) avg /= (double)count;
+            apply_pressure_velocity_update(dt, true);
+            iters += 1;
+            if ((avg <= prm.divergence_error_tol && iters >= 1) || iters >= prm.max_divergence_iters) break;
+        }
+        return iters;
+    }
+    // dfsph.rs:633-665 suggest_dt
+    double suggest_dt() const {
+        double vmax = 0.0, amax = 0.0;
+        for (size_t i = 0; i < parts.len(); ++i) {
+            if (parts.kind[i] != FLUID) continue;
+            vmax = std::fmax(vmax, norm2(parts.v[i]));
+            amax = std::fmax(amax, norm2(a_adv[i]));
+        }
+        vmax = std::sqrt(vmax);
+        amax = std::sqrt(amax);
+        double d = std::fmax(prm.particle_diameter, 1e-12);
+        double dt_v = prm.cfl_lambda * d / std::fmax(vmax, 1e-6);
+        double dt_f = cfl_suggested_dt(parts.h, 0.0, vmax, std::fmax(amax, 1e-6), prm.cfl_lambda, 0.25);
+        double r = std::fmin(dt_v, dt_f);
+        return r < 1e-6 ? 1e-6 : (r > 1e-2 ? 1e-2 : r);  // f64::clamp
+    }
+    // dfsph.rs:668-715
+    void apply_free_slip_walls() {
+        if (!prm.has_slip[0] && !prm.has_slip[1] && !prm.has_slip[2] && !prm.has_slip[3]) return;
+        for (size_t i = 0; i < parts.len(); ++i) {
+            if (parts.kind[i] != FLUID) continue;
+            V3 x = parts.x[i], v = v_star[i];
+            if (prm.has_slip[0] && x.x < prm.slip[0]) {
+                x.x = prm.slip[0];
+                if (v.x < 0.0) v.x = 0.0;
+            }
+            if (prm.has_slip[1] && x.y < prm.slip[1]) {
+                x.y = prm.slip[1];
+                if (v.y < 0.0) v.y = 0.0;
+            }
+            if (prm.has_slip[2] && x.x > prm.slip[2]) {
+                x.x = prm.slip[2];
+                if (v.x > 0.0) v.x = 0.0;
+            }
+            if (prm.has_slip[3] && x.y > prm.slip[3]) {
+                x.y = prm.slip[3];
+                if (v.y > 0.0) v.y = 0.0;
+            }
+            parts.x[i] = x;
+            v_star[i] = v;
+        }
+    }
+    // dfsph.rs:718-769 step
+    void step(double dt_in) {
+        ensure_buffers();
+        const size_t n = parts.len();
+        const double dt = std::fmax(dt_in, 1e-12);
+        last_dt = dt;
+        for (auto& f : boundary_force) f = zero3();
+        compute_nonpressure_accel();
+        for (size_t i = 0; i < n; ++i) {
+            if (parts.kind[i] != FLUID) {
+                v_star[i] = parts.v[i];
+                continue;
+            }
+            v_star[i] = parts.v[i] + a_adv[i] * dt;
+            if (parts.dim == D2) v_star[i].z = 0.0;
+        }
+        apply_xsph_on_vstar();
+        last_density_iters = correct_density_error(dt);
+        for (size_t i = 0; i < n; ++i) {
+            if (parts.kind[i] != FLUID) continue;
+            parts.x[i] += v_star[i] * dt;
+            if (parts.dim == D2) parts.x[i].z = 0.0;
+        }
+        apply_free_slip_walls();
+        rebuild_neighbours();
+        compute_density();
+        compute_alpha();
+        last_divergence_iters = correct_divergence_error(dt);
+        apply_free_slip_walls();
+        for (size_t i = 0; i < n; ++i)
+            if (parts.kind[i] == FLUID) {
+                parts.v[i] = v_star[i];
+                parts.p[i] = kappa[i];
+                if (parts.dim == D2) parts.v[i].z = 0.0;
+            }
+        t += dt;
+    }
+    // dfsph.rs:772-784 step_adaptive
+    double step_adaptive() {
+        ensure_buffers();
+        compute_nonpressure_accel();
+        double dt = prm.adaptive_dt ? suggest_dt() : std::fmax(last_dt, 1e-4);
+        step(dt);
+        return dt;
+    }
+};
 }  // namespace oracle
 
 // ===========================================================================
@@ -992,4 +1628,45 @@ double o_suggested_dt(double h, double c, double vmax, double amax, double lv, d
     return std::fmin(dt_v, dt_f);
 }
 
+
+// ---- PBF (pbf.rs) ----
+struct OPbf;
+static PbfWorld& P(OPbf* w) { return *reinterpret_cast<PbfWorld*>(w); }
+OPbf* opbf_create(OScene* s, const PParams* prm) {
+    return reinterpret_cast<OPbf*>(new PbfWorld(*reinterpret_cast<Particles*>(s), *prm));
+}
+void opbf_free(OPbf* w) { delete reinterpret_cast<PbfWorld*>(w); }
+void opbf_run(OPbf* w, double dt, long steps) {
+    for (long k = 0; k < steps; ++k) P(w).step(dt);
+}
+uint64_t opbf_hash(OPbf* w) { return particles_hash64(P(w).parts); }
+double opbf_time(OPbf* w) { return P(w).t; }
+void opbf_get_x(OPbf* w, double* out) { put3(P(w).parts.x, out); }
+void opbf_get_v(OPbf* w, double* out) { put3(P(w).parts.v, out); }
+void opbf_get_rho(OPbf* w, double* out) { std::copy(P(w).parts.rho.begin(), P(w).parts.rho.end(), out); }
+void opbf_get_lambda(OPbf* w, double* out) { std::copy(P(w).lambda.begin(), P(w).lambda.end(), out); }
+
+// ---- DFSPH (dfsph.rs) ----
+struct ODfsph;
+static DfsphWorld& D(ODfsph* w) { return *reinterpret_cast<DfsphWorld*>(w); }
+ODfsph* odfsph_create(OScene* s, const DParams* prm) {
+    return reinterpret_cast<ODfsph*>(new DfsphWorld(*reinterpret_cast<Particles*>(s), *prm));
+}
+void odfsph_free(ODfsph* w) { delete reinterpret_cast<DfsphWorld*>(w); }
+void odfsph_run(ODfsph* w, double dt, long steps) {
+    for (long k = 0; k < steps; ++k) D(w).step(dt);
+}
+double odfsph_step_adaptive(ODfsph* w) { return D(w).step_adaptive(); }
+uint64_t odfsph_hash(ODfsph* w) { return particles_hash64(D(w).parts); }
+double odfsph_time(ODfsph* w) { return D(w).t; }
+void odfsph_iters(ODfsph* w, int64_t* out) {
+    out[0] = D(w).last_density_iters;
+    out[1] = D(w).last_divergence_iters;
+}
+void odfsph_get_x(ODfsph* w, double* out) { put3(D(w).parts.x, out); }
+void odfsph_get_v(ODfsph* w, double* out) { put3(D(w).parts.v, out); }
+void odfsph_get_boundary_force(ODfsph* w, double* out) { put3(D(w).boundary_force, out); }
+void odfsph_get_rho(ODfsph* w, double* out) { std::copy(D(w).parts.rho.begin(), D(w).parts.rho.end(), out); }
+void odfsph_get_p(ODfsph* w, double* out) { std::copy(D(w).parts.p.begin(), D(w).parts.p.end(), out); }
+void odfsph_get_alpha(ODfsph* w, double* out) { std::copy(D(w).alpha.begin(), D(w).alpha.end(), out); }
 }  // extern "C"
