@@ -46,6 +46,15 @@ DX, DT, SEED, JITTER = 0.01, 1e-4, 0x5EED5EED, 1e-4
 # Algorithmic HBM bytes per fluid particle of the fused force + kick + drift
 # pass: read x, v, rho (56 B), write x, v (48 B).
 FORCE_BYTES_PER_FLUID = 104.0
+# Algorithmic FP64 operations per visited in-support pair (add, mul, div, sqrt
+# counted as one each): force pass 65, density 18, XSPH 31.
+FORCE_OPS_PER_PAIR = 65.0
+# DRAM bytes (read + write) of one force-pass launch per fluid particle, from
+# the ncu capture of the 262,144-particle dam break (the neighbour lists
+# dominate; traffic grows with the particle count).
+FORCE_TRAFFIC_PER_FLUID = (426.466304e6 + 20.284160e6) / 262144
+# sm__pipe_fp64_cycles_active of the force pass in the same capture
+FORCE_FP64_PIPE_ACTIVE = 0.599
 # Whole step, per fluid / per boundary particle (cell key 28 + sort 8 +
 # density 32 + XSPH 80 + forces 104; boundary 28 + 8 + 3 x 24).
 STEP_BYTES_FLUID, STEP_BYTES_BOUNDARY = 252.0, 108.0
@@ -78,6 +87,15 @@ def _args():
                     help="tanks of the batch timed one by one for the per-tank loop")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
+
+
+def fp64_rate(pe, device):
+    """The device's measured FP64 issue rate (Gop/s) of non-fused DMUL/DADD."""
+    import ctypes as C
+
+    g = C.c_double(0.0)
+    rc = pe.load_library().pe_fluid_probe_fp64_rate(int(device), C.byref(g))
+    return g.value if rc == 0 else None
 
 
 def _peaks():
@@ -591,6 +609,14 @@ def main():
     hbm_peak, peak_kind = _peaks()
     f_ms, f_n = prof["forces"]
     achieved = FORCE_BYTES_PER_FLUID * nf * f_n / (f_ms / 1e3) / 1e9 if f_ms > 0 else 0.0
+    # FP64 axis: visited in-support pairs of the force pass against the
+    # device's measured non-fused FP64 issue rate
+    _, in_sup = world.neighbour_counts()
+    fluid_mask = world.kinds() == 0
+    pairs = int(in_sup[fluid_mask].astype(np.int64).sum())
+    fp64_peak = fp64_rate(pe, local)
+    f_launch_s = f_ms / max(1, f_n) / 1e3
+    fp64_achieved = pairs * FORCE_OPS_PER_PAIR / f_launch_s / 1e9 if f_launch_s > 0 else 0.0
     total_prof = sum(v[0] for v in prof.values())
     step_bytes = STEP_BYTES_FLUID * nf + STEP_BYTES_BOUNDARY * nb
     line = {
@@ -610,10 +636,21 @@ def main():
                             "union_stage": cap["union_capacity"], "max_union": cap["max_union"]},
         "roofline": {"bound": "hbm", "kernel": "k_forces (force + kick + drift)",
                      "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                     "frac": achieved / hbm_peak, "peak_kind": peak_kind, "traffic": None,
+                     "frac": achieved / hbm_peak, "peak_kind": peak_kind,
+                     "traffic": FORCE_TRAFFIC_PER_FLUID * nf if FORCE_TRAFFIC_PER_FLUID else None,
                      "bytes_per_unit": FORCE_BYTES_PER_FLUID, "units_per_launch": nf,
                      "launch_ms": f_ms / max(1, f_n),
-                     "note": "algorithmic bytes; the pass is FP64-ALU bound, not HBM bound"},
+                     "binding": "fp64 (roofline_fp64): the pass is FP64-ALU bound, not HBM bound"},
+        "roofline_fp64": {"bound": "fp64", "kernel": "k_forces (force + kick + drift)",
+                          "achieved": fp64_achieved, "peak": fp64_peak, "unit": "Gop/s",
+                          "frac": fp64_achieved / fp64_peak if fp64_peak else None,
+                          "peak_kind": "measured: independent DMUL + DADD issue rate of this device "
+                                       "(pe_fluid_probe_fp64_rate; the f64 passes compile without FMA)",
+                          "ops_per_pair": FORCE_OPS_PER_PAIR, "pairs_per_launch": pairs,
+                          "pairs_per_fluid": pairs / max(1, nf),
+                          "ncu_fp64_pipe_active": FORCE_FP64_PIPE_ACTIVE,
+                          "note": "pairs are visited (ordered) in-support pairs: the gather evaluates each "
+                                  "fluid pair from both sides, the reference's scatter once"},
         "step_roofline": {"algorithmic_bytes_per_step": step_bytes,
                           "achieved_gbs": step_bytes / (ms / args.steps / 1e3) / 1e9,
                           "profiled_ms_per_step": total_prof / max(1, args.steps)},

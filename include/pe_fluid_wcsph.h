@@ -325,6 +325,12 @@ int pe_fluid_density_noalloc(int32_t dim, double rest_density, double mass, doub
                              const double* x, const uint8_t* kind, const double* psi,
                              const double* n_out, double* rho, void* stream);
 
+/* Measured FP64 issue rate of the device (no reference counterpart): independent
+ * non-fused multiplies and adds, the instruction mix the step's f64 passes
+ * compile to, in 1e9 operations per second. The denominator of the step's FP64
+ * roofline. */
+int pe_fluid_probe_fp64_rate(int32_t device, double* gops);
+
 /* Library version string. */
 const char* pe_fluid_version(void);
 

@@ -196,6 +196,7 @@ def load_library():
         "pe_fluid_pi_ij": (d, [d, d, d, d, d, D3, D3, D3, D3, d, d]),
         "pe_fluid_suggested_dt": (d, [d, d, d, d, d, d]),
         "pe_fluid_version": (C.c_char_p, []),
+        "pe_fluid_probe_fp64_rate": (C.c_int, [i32, D3]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
