@@ -57,6 +57,9 @@ extern "C" {
 /* KernelKind (crates/pe-fluid/src/kernels.rs:19); the WCSPH path supports the
  * cubic spline, the reference's default (wcsph.rs:45). */
 #define PE_KERNEL_CUBIC_SPLINE 0
+#define PE_KERNEL_WENDLAND_C2 1
+#define PE_KERNEL_POLY6 2
+#define PE_KERNEL_SPIKY 3
 
 /* ParticleKind (crates/pe-fluid/src/particles.rs:11). */
 #define PE_PARTICLE_FLUID 0
@@ -170,6 +173,54 @@ int pe_fluid_wcsph_create_from_arrays(const PeWcsphParams* params, int32_t dim, 
                                       double mass, double h, uint64_t n, const double* x,
                                       const double* v, const uint8_t* kind, const double* psi,
                                       const double* n_out, const PeWcsphConfig* cfg, PeWcsph** out);
+/* ---- Position Based Fluids (crates/pe-fluid/src/pbf.rs) ----
+ * PbfParams (pbf.rs:26-53); kernels are PE_KERNEL_* values. */
+typedef struct PePbfParams {
+    int32_t density_kernel;
+    int32_t grad_kernel;
+    uint64_t iterations;
+    double epsilon_lambda;
+    double art_pressure_k;
+    double art_pressure_n;
+    double art_pressure_dq_over_h;
+    double viscosity_eps;
+    double vorticity_eps;
+    double gravity[3];
+    int32_t reuse_neighbours;
+} PePbfParams;
+typedef struct PePbf PePbf;
+/* PbfParams::default (pbf.rs:55-74). */
+int pe_fluid_pbf_params_default(PePbfParams* out);
+/* PbfWorld::new (pbf.rs:112-130): grid cell = the larger support radius of the
+ * two kernels. cfg: device and capacity fields only (precision f64, no graphs). */
+int pe_fluid_pbf_create(const PeParticles* particles, const PePbfParams* params, const PeWcsphConfig* cfg,
+                        PePbf** out);
+int pe_fluid_pbf_create_from_arrays(const PePbfParams* params, int32_t dim, double rest_density, double mass,
+                                    double h, uint64_t n, const double* x, const double* v, const uint8_t* kind,
+                                    const double* psi, const double* n_out, const PeWcsphConfig* cfg,
+                                    PePbf** out);
+void pe_fluid_pbf_destroy(PePbf* w);
+/* PbfWorld::step (pbf.rs:384-436); dt >= 0. */
+int pe_fluid_pbf_step(PePbf* w, double dt);
+int pe_fluid_pbf_run(PePbf* w, double dt, uint64_t steps);
+int pe_fluid_pbf_len(const PePbf* w, uint64_t* out_len);
+int pe_fluid_pbf_get_time(const PePbf* w, double* t);
+int pe_fluid_pbf_get_params(const PePbf* w, PePbfParams* out);
+/* The kernels' support radius is fixed at creation. */
+int pe_fluid_pbf_set_params(PePbf* w, const PePbfParams* params);
+/* particles.{x, v, rho} and the last iteration's lambda, original order. */
+int pe_fluid_pbf_get_positions(PePbf* w, double* out, uint64_t n);
+int pe_fluid_pbf_get_velocities(PePbf* w, double* out, uint64_t n);
+int pe_fluid_pbf_get_densities(PePbf* w, double* out, uint64_t n);
+int pe_fluid_pbf_get_lambdas(PePbf* w, double* out, uint64_t n);
+int pe_fluid_pbf_set_positions(PePbf* w, const double* in, uint64_t n);
+int pe_fluid_pbf_set_velocities(PePbf* w, const double* in, uint64_t n);
+/* pbf.rs:440-455 mean |rho/rho0 - 1|, pbf.rs:458 v_max. */
+int pe_fluid_pbf_mean_density_error(PePbf* w, double* out);
+int pe_fluid_pbf_v_max(PePbf* w, double* out);
+int pe_fluid_pbf_status(PePbf* w, uint32_t* status);
+int pe_fluid_pbf_kernel_launches(PePbf* w, uint64_t* out, int32_t reset);
+
 /* Fluid side of CoupledWcsphWorld::step (coupling.rs:853-866). A coupler holds
  * the rigid samples of a world: sample k is world particle particle[k] (an
  * oriented boundary sample) on body body[k] < n_bodies, at body-frame offset

@@ -15,39 +15,9 @@
 #include "coupling.cuh"
 #include "world.cuh"
 
-struct PeParticles {
-    int32_t dim;
-    double rest_density, mass, h;
-    std::vector<double> x, v, psi, n_out;  // [n*3], [n*3], [n], [n*3]
-    std::vector<uint8_t> kind;
-    uint64_t len() const { return kind.size(); }
-};
-
+using namespace peabi;
 
 namespace {
-
-template <class F>
-int guard(F&& f) {
-    try {
-        return f();
-    } catch (const pe::CudaError&) {
-        return PE_ERR_DEVICE;
-    } catch (const std::length_error&) {
-        return PE_ERR_BOUNDS;
-    } catch (const std::invalid_argument&) {
-        return PE_ERR_ARG;
-    } catch (const std::bad_alloc&) {
-        return PE_ERR_DEVICE;
-    } catch (...) {
-        return PE_ERR_PANIC;
-    }
-}
-
-inline bool finite3(const double* a) {
-    return std::isfinite(a[0]) && std::isfinite(a[1]) && std::isfinite(a[2]);
-}
-
-inline bool valid_dim(int32_t d) { return d == PE_DIM_2 || d == PE_DIM_3; }
 
 void push(PeParticles* p, const double* x, const double* v, uint8_t kind, double psi,
           const double* n) {
@@ -136,24 +106,6 @@ int check_params(const PeWcsphParams* p) {
     return PE_OK;
 }
 
-int status_code(uint32_t st) {
-    if (st & (PE_STATUS_DOMAIN | PE_STATUS_NEIGHBOUR_OVERFLOW)) return PE_ERR_BOUNDS;
-    if (st & PE_STATUS_NONFINITE) return PE_ERR_ARG;
-    return PE_OK;
-}
-
-pe::WorldConfig to_config(const PeWcsphConfig* c) {
-    pe::WorldConfig w{};
-    w.device = c ? c->device : -1;
-    w.max_neighbours = c ? c->max_neighbours : 0;
-    w.max_lower = c ? c->max_lower : 0;
-    w.domain_margin = c ? c->domain_margin : -1.0;
-    w.domain_margin_cells = c ? c->domain_margin_cells : 0;
-    w.precision = c ? c->precision : 0;
-    w.use_graph = c ? c->use_graph : 0;
-    if (!c) w.domain_margin = -1.0;
-    return w;
-}
 
 uint64_t fnv1a(uint64_t h, double x) {
     uint64_t bits;

@@ -1,0 +1,236 @@
+// C ABI of the sibling solvers that share the WCSPH world's grid, lists and
+// state: Position Based Fluids (pbf.rs). Same conventions as abi.cu: pe-ffi
+// error codes, no unwinding across the boundary, caller-owned host buffers in
+// original particle order.
+#include <cmath>
+#include <cstring>
+
+#include "handles.cuh"
+#include "pbf.cuh"
+
+using namespace peabi;
+
+struct PePbf {
+    pe::PbfSolver* s;
+};
+
+namespace {
+
+int check_pbf(const PePbfParams* p) {
+    if (!p) return PE_ERR_NULL;
+    if (p->density_kernel < 0 || p->density_kernel > 3 || p->grad_kernel < 0 || p->grad_kernel > 3)
+        return PE_ERR_ARG;
+    const double v[] = {p->epsilon_lambda, p->art_pressure_k, p->art_pressure_n, p->art_pressure_dq_over_h,
+                        p->viscosity_eps, p->vorticity_eps};
+    for (double d : v)
+        if (!std::isfinite(d)) return PE_ERR_ARG;
+    if (!finite3(p->gravity)) return PE_ERR_ARG;
+    if (p->iterations > (1u << 20)) return PE_ERR_BOUNDS;
+    return PE_OK;
+}
+
+pe::PbfParams to_pbf(const PePbfParams& p) {
+    pe::PbfParams q{};
+    q.density_kernel = p.density_kernel;
+    q.grad_kernel = p.grad_kernel;
+    q.iterations = p.iterations;
+    q.epsilon_lambda = p.epsilon_lambda;
+    q.art_pressure_k = p.art_pressure_k;
+    q.art_pressure_n = p.art_pressure_n;
+    q.art_pressure_dq_over_h = p.art_pressure_dq_over_h;
+    q.viscosity_eps = p.viscosity_eps;
+    q.vorticity_eps = p.vorticity_eps;
+    for (int a = 0; a < 3; ++a) q.gravity[a] = p.gravity[a];
+    q.reuse_neighbours = p.reuse_neighbours;
+    return q;
+}
+
+PePbfParams from_pbf(const pe::PbfParams& q) {
+    PePbfParams p{};
+    p.density_kernel = q.density_kernel;
+    p.grad_kernel = q.grad_kernel;
+    p.iterations = q.iterations;
+    p.epsilon_lambda = q.epsilon_lambda;
+    p.art_pressure_k = q.art_pressure_k;
+    p.art_pressure_n = q.art_pressure_n;
+    p.art_pressure_dq_over_h = q.art_pressure_dq_over_h;
+    p.viscosity_eps = q.viscosity_eps;
+    p.vorticity_eps = q.vorticity_eps;
+    for (int a = 0; a < 3; ++a) p.gravity[a] = q.gravity[a];
+    p.reuse_neighbours = q.reuse_neighbours;
+    return p;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pe_fluid_pbf_params_default(PePbfParams* out) {
+    if (!out) return PE_ERR_NULL;
+    PePbfParams p{};
+    p.density_kernel = PE_KERNEL_POLY6;
+    p.grad_kernel = PE_KERNEL_SPIKY;
+    p.iterations = 5;
+    p.epsilon_lambda = 0.01;
+    p.art_pressure_k = 0.01;
+    p.art_pressure_n = 4.0;
+    p.art_pressure_dq_over_h = 0.25;
+    p.viscosity_eps = 0.01;
+    p.vorticity_eps = 0.0;
+    p.gravity[0] = 0.0;
+    p.gravity[1] = 0.0;
+    p.gravity[2] = -9.80665;
+    p.reuse_neighbours = 1;
+    *out = p;
+    return PE_OK;
+}
+
+int pe_fluid_pbf_create_from_arrays(const PePbfParams* params, int32_t dim, double rest_density, double mass,
+                                    double h, uint64_t n, const double* x, const double* v, const uint8_t* kind,
+                                    const double* psi, const double* n_out, const PeWcsphConfig* cfg,
+                                    PePbf** out) {
+    if (!out) return PE_ERR_NULL;
+    *out = nullptr;
+    int rc = check_pbf(params);
+    if (rc != PE_OK) return rc;
+    rc = check_arrays(dim, rest_density, mass, h, n, x, v, kind, psi, n_out);
+    if (rc != PE_OK) return rc;
+    return guard([&] {
+        std::vector<double> zero;
+        const double* ps = psi;
+        if (!ps) {
+            zero.assign(n ? n : 1, 0.0);
+            ps = zero.data();
+        }
+        auto* s = new pe::PbfSolver(to_pbf(*params), to_config(cfg), dim, rest_density, mass, h, n, x, v, kind,
+                                    ps, n_out);
+        *out = new PePbf{s};
+        return PE_OK;
+    });
+}
+
+int pe_fluid_pbf_create(const PeParticles* particles, const PePbfParams* params, const PeWcsphConfig* cfg,
+                        PePbf** out) {
+    if (!particles) return PE_ERR_NULL;
+    const PeParticles& p = *particles;
+    return pe_fluid_pbf_create_from_arrays(params, p.dim, p.rest_density, p.mass, p.h, p.len(), p.x.data(),
+                                           p.v.data(), p.kind.data(), p.psi.data(), p.n_out.data(), cfg, out);
+}
+
+void pe_fluid_pbf_destroy(PePbf* w) {
+    if (!w) return;
+    try {
+        delete w->s;
+    } catch (...) {
+    }
+    delete w;
+}
+
+int pe_fluid_pbf_step(PePbf* w, double dt) {
+    if (!w) return PE_ERR_NULL;
+    if (!(std::isfinite(dt) && dt >= 0.0)) return PE_ERR_ARG;
+    return guard([&] {
+        w->s->step(dt);
+        return status_code(w->s->world().status());
+    });
+}
+
+int pe_fluid_pbf_run(PePbf* w, double dt, uint64_t steps) {
+    if (!w) return PE_ERR_NULL;
+    if (!(std::isfinite(dt) && dt >= 0.0)) return PE_ERR_ARG;
+    return guard([&] {
+        w->s->run(dt, steps);
+        return status_code(w->s->world().status());
+    });
+}
+
+int pe_fluid_pbf_len(const PePbf* w, uint64_t* out_len) {
+    if (!w || !out_len) return PE_ERR_NULL;
+    *out_len = w->s->world().len();
+    return PE_OK;
+}
+
+int pe_fluid_pbf_get_time(const PePbf* w, double* t) {
+    if (!w || !t) return PE_ERR_NULL;
+    *t = w->s->world().time();
+    return PE_OK;
+}
+
+int pe_fluid_pbf_get_params(const PePbf* w, PePbfParams* out) {
+    if (!w || !out) return PE_ERR_NULL;
+    *out = from_pbf(w->s->params());
+    return PE_OK;
+}
+
+int pe_fluid_pbf_set_params(PePbf* w, const PePbfParams* params) {
+    if (!w) return PE_ERR_NULL;
+    int rc = check_pbf(params);
+    if (rc != PE_OK) return rc;
+    return guard([&] {
+        w->s->set_params(to_pbf(*params));
+        return PE_OK;
+    });
+}
+
+#define PE_PBF_GET(name, call)                                        \
+    int pe_fluid_pbf_##name(PePbf* w, double* out, uint64_t n) {      \
+        if (!w || !out) return PE_ERR_NULL;                           \
+        if (n != w->s->world().len()) return PE_ERR_BOUNDS;           \
+        return guard([&] {                                            \
+            call;                                                     \
+            return PE_OK;                                             \
+        });                                                           \
+    }
+PE_PBF_GET(get_positions, w->s->world().get_vec(0, out))
+PE_PBF_GET(get_velocities, w->s->world().get_vec(1, out))
+PE_PBF_GET(get_densities, w->s->world().get_scalar(0, out))
+PE_PBF_GET(get_lambdas, w->s->get_lambda(out))
+#undef PE_PBF_GET
+
+#define PE_PBF_SET(name, which)                                           \
+    int pe_fluid_pbf_##name(PePbf* w, const double* in, uint64_t n) {     \
+        if (!w || !in) return PE_ERR_NULL;                                \
+        if (n != w->s->world().len()) return PE_ERR_BOUNDS;               \
+        for (uint64_t i = 0; i < 3 * n; ++i)                              \
+            if (!std::isfinite(in[i])) return PE_ERR_ARG;                 \
+        return guard([&] {                                                \
+            w->s->world().set_vec(which, in);                             \
+            return PE_OK;                                                 \
+        });                                                               \
+    }
+PE_PBF_SET(set_positions, 0)
+PE_PBF_SET(set_velocities, 1)
+#undef PE_PBF_SET
+
+int pe_fluid_pbf_mean_density_error(PePbf* w, double* out) {
+    if (!w || !out) return PE_ERR_NULL;
+    return guard([&] {
+        *out = w->s->mean_density_error();
+        return PE_OK;
+    });
+}
+
+int pe_fluid_pbf_v_max(PePbf* w, double* out) {
+    if (!w || !out) return PE_ERR_NULL;
+    return guard([&] {
+        *out = w->s->v_max();
+        return PE_OK;
+    });
+}
+
+int pe_fluid_pbf_status(PePbf* w, uint32_t* status) {
+    if (!w || !status) return PE_ERR_NULL;
+    return guard([&] {
+        *status = w->s->world().status();
+        return PE_OK;
+    });
+}
+
+int pe_fluid_pbf_kernel_launches(PePbf* w, uint64_t* out, int32_t reset) {
+    if (!w || !out) return PE_ERR_NULL;
+    *out = w->s->world().kernel_launches();
+    if (reset) w->s->world().reset_launch_count();
+    return PE_OK;
+}
+
+}  // extern "C"

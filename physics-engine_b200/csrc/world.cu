@@ -116,8 +116,9 @@ T* World::alloc(size_t count) {
 World::World(const WorldParams& prm, const WorldConfig& cfg, int dim, double rest_density,
              double mass, double h, uint64_t n, const double* x, const double* v,
              const uint8_t* kind, const double* psi, const double* n_out,
-             const uint64_t* tank_offsets, uint32_t n_tanks)
-    : dim_(dim), rho0_(rest_density), mass_(mass), h_(h), n_(n), prm_(prm), cfg_(cfg) {
+             const uint64_t* tank_offsets, uint32_t n_tanks, double support)
+    : dim_(dim), rho0_(rest_density), mass_(mass), h_(h), support_(support > 0.0 ? support : 2.0 * h),
+      n_(n), prm_(prm), cfg_(cfg) {
     if (cfg_.device >= 0) check(cudaSetDevice(cfg_.device), "cudaSetDevice");
     check(cudaGetDevice(&device_), "cudaGetDevice");
     // ---- tanks: contiguous particle ranges ----
@@ -136,7 +137,7 @@ World::World(const WorldParams& prm, const WorldConfig& cfg, int dim, double res
     check(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking), "cudaStreamCreate");
     try {
         // ---- each tank's grid domain from its initial keys (grid.rs:62 key_of) ----
-        const double cell = 2.0 * h_;  // support_radius(CubicSpline, h), kernels.rs:32
+        const double cell = support_;  // support_radius, kernels.rs:32 (grid.rs:48 cell = support)
         const double inv = 1.0 / cell;
         const double frac = cfg_.domain_margin < 0.0 ? 0.25 : cfg_.domain_margin;
         const long long minc = cfg_.domain_margin_cells ? cfg_.domain_margin_cells : 4;
@@ -443,8 +444,10 @@ void World::refresh_step_const() {
     k.xsph_eps = prm_.xsph_epsilon;
     k.boundary_eps_h = 0.15 * h_;  // particles.rs:132
     k.adapt_sound_speed = prm_.adapt_sound_speed;
-    double sup = 2.0 * h_;
-    k.r2_filter = std::nextafter((float)(sup * sup * (1.0 + 1e-4)), std::numeric_limits<float>::infinity());
+    double sup = support_;
+    k.r2_filter = list_all_candidates_
+                      ? std::numeric_limits<float>::infinity()
+                      : std::nextafter((float)(sup * sup * (1.0 + 1e-4)), std::numeric_limits<float>::infinity());
     kc_ = k;
 
     F32Const f{};

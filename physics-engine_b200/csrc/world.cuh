@@ -42,6 +42,8 @@ class CudaError : public std::runtime_error {
 
 class Surrogate;
 class Coupler;
+class PbfSolver;
+class DfsphSolver;
 
 class World {
    public:
@@ -50,7 +52,7 @@ class World {
     World(const WorldParams& prm, const WorldConfig& cfg, int dim, double rest_density, double mass,
           double h, uint64_t n, const double* x, const double* v, const uint8_t* kind,
           const double* psi, const double* n_out, const uint64_t* tank_offsets = nullptr,
-          uint32_t n_tanks = 1);
+          uint32_t n_tanks = 1, double support = 0.0);
     ~World();
     World(const World&) = delete;
     World& operator=(const World&) = delete;
@@ -143,6 +145,8 @@ class World {
    private:
     friend class Surrogate;
     friend class Coupler;
+    friend class PbfSolver;
+    friend class DfsphSolver;
     void save_checkpoint();
     void restore_checkpoint();
     double4 *ck_pos_ = nullptr, *ck_vel_ = nullptr;
@@ -170,6 +174,11 @@ class World {
 
     int dim_;
     double rho0_, mass_, h_;
+    double support_;  // grid cell size and list radius (the WCSPH cubic spline: 2h)
+    // Lists keep every candidate of the 27 (9) neighbour cells, not only those
+    // in support: solvers that reuse a list while particles move (PBF's
+    // constraint iterations) need the reference's complete candidate set.
+    bool list_all_candidates_ = false;
     uint64_t n_;
     WorldParams prm_;
     WorldConfig cfg_;

@@ -36,7 +36,8 @@ PE_OK, PE_ERR_NULL, PE_ERR_BOUNDS, PE_ERR_ARG, PE_ERR_PANIC, PE_ERR_SCENE = 0, 1
 PE_ERR_UNSUPPORTED, PE_ERR_DEVICE = 6, 7
 STATUS_DOMAIN, STATUS_NEIGHBOUR_OVERFLOW, STATUS_NONFINITE, STATUS_SLOW_UNION = 1, 2, 4, 8
 FLUID, BOUNDARY = 0, 1
-CUBIC_SPLINE = 0
+CUBIC_SPLINE, WENDLAND_C2, POLY6, SPIKY = 0, 1, 2, 3
+DIM_2, DIM_3 = 2, 3
 STANDARD_GRAVITY = 9.80665  # pe-math units.rs:7
 
 _ERRNAMES = {1: "PE_ERR_NULL", 2: "PE_ERR_BOUNDS", 3: "PE_ERR_ARG", 4: "PE_ERR_PANIC",
@@ -87,6 +88,22 @@ class _Config(C.Structure):
 
 
 PRECISION_F64, PRECISION_F32 = 0, 1
+
+
+class _PbfParams(C.Structure):
+    _fields_ = [
+        ("density_kernel", C.c_int32),
+        ("grad_kernel", C.c_int32),
+        ("iterations", C.c_uint64),
+        ("epsilon_lambda", C.c_double),
+        ("art_pressure_k", C.c_double),
+        ("art_pressure_n", C.c_double),
+        ("art_pressure_dq_over_h", C.c_double),
+        ("viscosity_eps", C.c_double),
+        ("vorticity_eps", C.c_double),
+        ("gravity", C.c_double * 3),
+        ("reuse_neighbours", C.c_int32),
+    ]
 
 
 class _Profile(C.Structure):
@@ -186,6 +203,25 @@ def load_library():
         "pe_fluid_wcsph_profile": (C.c_int, [vp, i32]),
         "pe_fluid_wcsph_profile_read": (C.c_int, [vp, C.POINTER(_Profile), i32]),
         "pe_fluid_wcsph_stream": (C.c_int, [vp, C.POINTER(vp)]),
+        "pe_fluid_pbf_params_default": (C.c_int, [C.POINTER(_PbfParams)]),
+        "pe_fluid_pbf_create": (C.c_int, [vp, C.POINTER(_PbfParams), C.POINTER(_Config), C.POINTER(vp)]),
+        "pe_fluid_pbf_destroy": (None, [vp]),
+        "pe_fluid_pbf_step": (C.c_int, [vp, d]),
+        "pe_fluid_pbf_run": (C.c_int, [vp, d, u64]),
+        "pe_fluid_pbf_len": (C.c_int, [vp, C.POINTER(u64)]),
+        "pe_fluid_pbf_get_time": (C.c_int, [vp, D3]),
+        "pe_fluid_pbf_get_params": (C.c_int, [vp, C.POINTER(_PbfParams)]),
+        "pe_fluid_pbf_set_params": (C.c_int, [vp, C.POINTER(_PbfParams)]),
+        "pe_fluid_pbf_get_positions": (C.c_int, [vp, vp, u64]),
+        "pe_fluid_pbf_get_velocities": (C.c_int, [vp, vp, u64]),
+        "pe_fluid_pbf_get_densities": (C.c_int, [vp, vp, u64]),
+        "pe_fluid_pbf_get_lambdas": (C.c_int, [vp, vp, u64]),
+        "pe_fluid_pbf_set_positions": (C.c_int, [vp, vp, u64]),
+        "pe_fluid_pbf_set_velocities": (C.c_int, [vp, vp, u64]),
+        "pe_fluid_pbf_mean_density_error": (C.c_int, [vp, D3]),
+        "pe_fluid_pbf_v_max": (C.c_int, [vp, D3]),
+        "pe_fluid_pbf_status": (C.c_int, [vp, C.POINTER(u32)]),
+        "pe_fluid_pbf_kernel_launches": (C.c_int, [vp, C.POINTER(u64), i32]),
         "pe_fluid_coupler_create": (C.c_int, [vp, u32, u64, vp, vp, vp, vp, C.POINTER(vp)]),
         "pe_fluid_coupler_destroy": (None, [vp]),
         "pe_fluid_coupler_sync": (C.c_int, [vp, vp, vp, vp, vp]),
@@ -680,6 +716,168 @@ class WcsphWorld:
 # stateless helpers
 # --------------------------------------------------------------------------
 # --------------------------------------------------------------------------
+# Position Based Fluids (crates/pe-fluid/src/pbf.rs)
+# --------------------------------------------------------------------------
+class PbfParams:
+    """`PbfParams` (pbf.rs:26-53); the defaults are `PbfParams::default` (pbf.rs:55-74)."""
+
+    _FIELDS = ("density_kernel", "grad_kernel", "iterations", "epsilon_lambda", "art_pressure_k",
+               "art_pressure_n", "art_pressure_dq_over_h", "viscosity_eps", "vorticity_eps", "gravity",
+               "reuse_neighbours")
+
+    def __init__(self, **kw):
+        c = _PbfParams()
+        _ok(load_library().pe_fluid_pbf_params_default(C.byref(c)), "pbf_params_default")
+        for k in self._FIELDS:
+            v = getattr(c, k)
+            setattr(self, k, tuple(v) if k == "gravity" else v)
+        self.reuse_neighbours = bool(self.reuse_neighbours)
+        for k, v in kw.items():
+            if k not in self._FIELDS:
+                raise TypeError(f"unknown PbfParams field {k!r}")
+            setattr(self, k, v)
+
+    def _to_c(self) -> _PbfParams:
+        c = _PbfParams()
+        c.density_kernel, c.grad_kernel = int(self.density_kernel), int(self.grad_kernel)
+        c.iterations = int(self.iterations)
+        c.epsilon_lambda, c.art_pressure_k = float(self.epsilon_lambda), float(self.art_pressure_k)
+        c.art_pressure_n, c.art_pressure_dq_over_h = float(self.art_pressure_n), float(self.art_pressure_dq_over_h)
+        c.viscosity_eps, c.vorticity_eps = float(self.viscosity_eps), float(self.vorticity_eps)
+        c.gravity[:] = [float(g) for g in self.gravity]
+        c.reuse_neighbours = 1 if self.reuse_neighbours else 0
+        return c
+
+    def __repr__(self):
+        return "PbfParams(" + ", ".join(f"{k}={getattr(self, k)!r}" for k in self._FIELDS) + ")"
+
+
+class PbfWorld:
+    """`PbfWorld` (pbf.rs:77-459) on one B200, bit-identical to the reference's
+    step. State arrays are in original order."""
+
+    def __init__(self, particles: Particles, params: PbfParams | None = None,
+                 config: WcsphConfig | None = None):
+        L = load_library()
+        self._w = None
+        params = params if params is not None else PbfParams()
+        h = C.c_void_p()
+        cfg = config._to_c() if config is not None else None
+        _ok(L.pe_fluid_pbf_create(particles._p, C.byref(params._to_c()),
+                                  C.byref(cfg) if cfg is not None else None, C.byref(h)), "pbf_create")
+        self._w = h
+        self.n = len(particles)
+        self._kinds = particles.arrays()["kind"].copy()
+        self.dim, self.mass, self.h, self.rest_density = particles.dim, particles.mass, particles.h, particles.rest_density
+
+    def close(self):
+        if getattr(self, "_w", None) and _lib is not None:
+            _lib.pe_fluid_pbf_destroy(self._w)
+        self._w = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def step(self, dt: float):
+        _ok(_lib.pe_fluid_pbf_step(self._w, float(dt)), "pbf_step")
+
+    def run(self, dt: float, steps: int):
+        _ok(_lib.pe_fluid_pbf_run(self._w, float(dt), int(steps)), "pbf_run")
+
+    @property
+    def t(self) -> float:
+        t = C.c_double()
+        _ok(_lib.pe_fluid_pbf_get_time(self._w, C.byref(t)), "pbf_time")
+        return t.value
+
+    @property
+    def params(self) -> PbfParams:
+        c = _PbfParams()
+        _ok(_lib.pe_fluid_pbf_get_params(self._w, C.byref(c)), "pbf_params")
+        p = PbfParams()
+        for k in PbfParams._FIELDS:
+            v = getattr(c, k)
+            setattr(p, k, tuple(v) if k == "gravity" else v)
+        p.reuse_neighbours = bool(p.reuse_neighbours)
+        return p
+
+    @params.setter
+    def params(self, p: PbfParams):
+        _ok(_lib.pe_fluid_pbf_set_params(self._w, C.byref(p._to_c())), "pbf_set_params")
+
+    def _get(self, fn, shape, what):
+        out = np.empty(shape)
+        _ok(fn(self._w, _ptr(out), self.n), what)
+        return out
+
+    def positions(self):
+        return self._get(_lib.pe_fluid_pbf_get_positions, (self.n, 3), "pbf_positions")
+
+    def velocities(self):
+        return self._get(_lib.pe_fluid_pbf_get_velocities, (self.n, 3), "pbf_velocities")
+
+    def densities(self):
+        return self._get(_lib.pe_fluid_pbf_get_densities, (self.n,), "pbf_densities")
+
+    def lambdas(self):
+        return self._get(_lib.pe_fluid_pbf_get_lambdas, (self.n,), "pbf_lambdas")
+
+    def set_positions(self, x):
+        x = _arr(x, np.float64, (self.n, 3))
+        _ok(_lib.pe_fluid_pbf_set_positions(self._w, _ptr(x), self.n), "pbf_set_positions")
+
+    def set_velocities(self, v):
+        v = _arr(v, np.float64, (self.n, 3))
+        _ok(_lib.pe_fluid_pbf_set_velocities(self._w, _ptr(v), self.n), "pbf_set_velocities")
+
+    def mean_density_error(self) -> float:
+        d = C.c_double()
+        _ok(_lib.pe_fluid_pbf_mean_density_error(self._w, C.byref(d)), "pbf_mean_density_error")
+        return d.value
+
+    def v_max(self) -> float:
+        d = C.c_double()
+        _ok(_lib.pe_fluid_pbf_v_max(self._w, C.byref(d)), "pbf_v_max")
+        return d.value
+
+    def status(self) -> int:
+        s = C.c_uint32()
+        _ok(_lib.pe_fluid_pbf_status(self._w, C.byref(s)), "pbf_status")
+        return s.value
+
+    def kernel_launches(self, reset=False) -> int:
+        c = C.c_uint64()
+        _ok(_lib.pe_fluid_pbf_kernel_launches(self._w, C.byref(c), 1 if reset else 0), "pbf_launches")
+        return c.value
+
+    def kinds(self):
+        """Particle kinds in original order (fixed at creation)."""
+        return self._kinds
+
+    def hash64(self) -> int:
+        """`particles_hash64` (diagnostics.rs:10-33) of the current state."""
+        return particles_hash64(self.positions(), self.velocities(), self._kinds)
+
+
+def particles_hash64(x, v, kind) -> int:
+    """FNV-1a 64 over the IEEE bits of fluid (x, v), little-endian, in index
+    order (diagnostics.rs:10-33)."""
+    fluid = np.asarray(kind) == FLUID
+    data = np.concatenate([np.asarray(x, np.float64)[fluid], np.asarray(v, np.float64)[fluid]], axis=1)
+    h = 0xCBF29CE484222325
+    for b in np.ascontiguousarray(data).astype("<f8").tobytes():
+        h ^= b
+        h = (h * 0x100000001B3) & 0xFFFFFFFFFFFFFFFF
+    return h
+
+
+# --------------------------------------------------------------------------
 # Fluid side of the WCSPH-rigid coupling (crates/pe-fluid/src/coupling.rs)
 # --------------------------------------------------------------------------
 class FluidRigidCoupler:
@@ -768,8 +966,30 @@ def suggested_dt(h, sound_speed, v_max, a_max, lambda_v=0.25, lambda_f=0.25):
 _NOT_ON_PATH = ("this build provides the WCSPH solver path only; the {} solver is not included")
 
 
+FLUID_HASH_STEPS, FLUID_HASH_DT = 40, 1.0 / 120.0
+
+
+def fluid_hash_world(config: WcsphConfig | None = None) -> PbfWorld:
+    """The canonical PBF tank (scenarios.rs:28-61): a 4x4x4 block (dx 0.05,
+    h 2 dx) in a 0.4 x 0.4 x 0.45 shell; 4 iterations, no tensile correction,
+    no vorticity."""
+    dx, rho0 = 0.05, 1000.0
+    parts = Particles(DIM_3, rho0, mass_from_spacing(rho0, dx, DIM_3), 2.0 * dx)
+    parts.fill_box((0.1, 0.1, 0.1), 4, 4, 4, dx)
+    parts.fill_box_boundary((0.0, 0.0, 0.0), (0.4, 0.4, 0.45), dx, 1)
+    params = PbfParams(gravity=(0.0, 0.0, -STANDARD_GRAVITY), iterations=4, art_pressure_k=0.0,
+                       vorticity_eps=0.0)
+    return PbfWorld(parts, params, config)
+
+
 def canonical_fluid_hash() -> int:
-    raise NotImplementedError(_NOT_ON_PATH.format("PBF"))
+    """`fluid_tank_hash` (scenarios.rs:64-71): the canonical PBF tank after 40
+    steps of 1/120 s, hashed; stepped on the GPU."""
+    w = fluid_hash_world()
+    w.run(FLUID_HASH_DT, FLUID_HASH_STEPS)
+    h = w.hash64()
+    w.close()
+    return h
 
 
 def canonical_dfsph_hash() -> int:
@@ -831,8 +1051,48 @@ def fluid_sphere_freefall_accel_added_mass(rho_s: float, rho_f: float, g: float)
     return g * (rho_s - rho_f) / max(rho_s + 0.5 * rho_f, 1e-12)
 
 
+def _parse_dim(dim) -> int:
+    d = str(dim).lower().replace("d", "")
+    if d not in ("2", "3"):
+        raise ValueError(f"dim must be '2' or '3', got {dim!r}")
+    return int(d)
+
+
+def _mean_density_error_diag(rho, kind, rest_density) -> float:
+    """diagnostics.rs:74-88, summed in index order."""
+    s, n = 0.0, 0
+    for r, k in zip(np.asarray(rho).tolist(), np.asarray(kind).tolist()):
+        if k == FLUID:
+            s += abs(r - rest_density) / rest_density
+            n += 1
+    return 0.0 if n == 0 else s / n
+
+
+def _tank_parts(dim, n_side, dx, h, mass, rho0):
+    parts = Particles(dim, rho0, mass, h)
+    nz = 1 if dim == DIM_2 else n_side
+    parts.fill_box((0.1, 0.1, 0.1), n_side, n_side, nz, dx)
+    zmax = 0.0 if dim == DIM_2 else 0.1 + n_side * dx + 0.05
+    ext = 0.1 + n_side * dx + 0.1
+    parts.fill_box_boundary((0.0, 0.0, 0.0), (ext, ext, max(zmax, 0.45)), dx, 1)
+    return parts
+
+
 def fluid_pbf_tank_demo(n_side=4, steps=40, dt=1.0 / 120.0, dim="3"):
-    raise NotImplementedError(_NOT_ON_PATH.format("PBF"))
+    """Small PBF tank (python/src/fluid.rs:188-243): returns (fluid positions
+    [N, 3], fluid densities [N], mean density error)."""
+    d = _parse_dim(dim)
+    dx, rho0 = 0.05, 1000.0
+    h = 2.2 * dx
+    parts = _tank_parts(d, int(n_side), dx, h, mass_from_spacing(rho0, dx, d), rho0)
+    g = (0.0, -STANDARD_GRAVITY, 0.0) if d == DIM_2 else (0.0, 0.0, -STANDARD_GRAVITY)
+    w = PbfWorld(parts, PbfParams(gravity=g, iterations=2, art_pressure_k=0.0))
+    w.run(float(dt), int(steps))
+    fluid = w.kinds() == FLUID
+    x, rho = w.positions(), w.densities()
+    err = _mean_density_error_diag(rho, w.kinds(), rho0)
+    w.close()
+    return x[fluid], rho[fluid], err
 
 
 def fluid_dfsph_tank_demo(n_side=4, steps=40, dt=1.0 / 120.0, dim="3"):

@@ -72,7 +72,7 @@ def test_analytic_functions():
     assert pe.fluid_canonical_mass() == pe.mass_from_spacing(1000.0, 0.05, 3) * 64
     assert pe.fluid_poly6_w0(0.1) > 0
     with pytest.raises(NotImplementedError):
-        pe.canonical_fluid_hash()
+        pe.canonical_coupling_hash()
 
 
 def test_scene_builders_match_oracle():
