@@ -221,6 +221,73 @@ int pe_fluid_pbf_v_max(PePbf* w, double* out);
 int pe_fluid_pbf_status(PePbf* w, uint32_t* status);
 int pe_fluid_pbf_kernel_launches(PePbf* w, uint64_t* out, int32_t reset);
 
+/* ---- Divergence-free SPH (crates/pe-fluid/src/dfsph.rs) ----
+ * DfsphParams (dfsph.rs:33-80) without surface tension; the optional free-slip
+ * planes x >= xmin, y >= ymin, x <= xmax, y <= ymax are free_slip[0..3],
+ * active where free_slip_set[k] is nonzero. */
+typedef struct PeDfsphParams {
+    int32_t kernel;
+    uint64_t max_density_iters;
+    uint64_t max_divergence_iters;
+    double density_error_tol;
+    double divergence_error_tol;
+    double gravity[3];
+    double xsph_epsilon;
+    double particle_diameter;
+    double cfl_lambda;
+    int32_t adaptive_dt;
+    int32_t warm_start;
+    int32_t free_slip_set[4];
+    double free_slip[4];
+    double solver_omega;
+    double max_velocity_correction;
+} PeDfsphParams;
+typedef struct PeDfsph PeDfsph;
+/* DfsphParams::default (dfsph.rs:82-104). */
+int pe_fluid_dfsph_params_default(PeDfsphParams* out);
+/* DfsphWorld::new (dfsph.rs:137-180): builds the grid and lists and computes
+ * densities and alpha. cfg: device and capacity fields only. */
+int pe_fluid_dfsph_create(const PeParticles* particles, const PeDfsphParams* params, const PeWcsphConfig* cfg,
+                          PeDfsph** out);
+int pe_fluid_dfsph_create_from_arrays(const PeDfsphParams* params, int32_t dim, double rest_density,
+                                      double mass, double h, uint64_t n, const double* x, const double* v,
+                                      const uint8_t* kind, const double* psi, const double* n_out,
+                                      const PeWcsphConfig* cfg, PeDfsph** out);
+void pe_fluid_dfsph_destroy(PeDfsph* w);
+/* DfsphWorld::step (dfsph.rs:718-769), step_adaptive (dfsph.rs:772-784, the
+ * dt used goes to *dt_out), suggest_dt (dfsph.rs:633-665). */
+int pe_fluid_dfsph_step(PeDfsph* w, double dt);
+int pe_fluid_dfsph_run(PeDfsph* w, double dt, uint64_t steps);
+int pe_fluid_dfsph_step_adaptive(PeDfsph* w, double* dt_out);
+int pe_fluid_dfsph_suggest_dt(PeDfsph* w, double* out);
+/* The public phase methods (dfsph.rs:201, 214, 252). */
+int pe_fluid_dfsph_rebuild_neighbours(PeDfsph* w);
+int pe_fluid_dfsph_compute_density(PeDfsph* w);
+int pe_fluid_dfsph_compute_alpha(PeDfsph* w);
+int pe_fluid_dfsph_len(const PeDfsph* w, uint64_t* out_len);
+int pe_fluid_dfsph_get_time(const PeDfsph* w, double* t);
+int pe_fluid_dfsph_get_last_dt(const PeDfsph* w, double* out);
+int pe_fluid_dfsph_get_params(const PeDfsph* w, PeDfsphParams* out);
+int pe_fluid_dfsph_set_params(PeDfsph* w, const PeDfsphParams* params);
+/* particles.{x, v, rho, p}, boundary_force, alpha; original order. */
+int pe_fluid_dfsph_get_positions(PeDfsph* w, double* out, uint64_t n);
+int pe_fluid_dfsph_get_velocities(PeDfsph* w, double* out, uint64_t n);
+int pe_fluid_dfsph_get_densities(PeDfsph* w, double* out, uint64_t n);
+int pe_fluid_dfsph_get_pressures(PeDfsph* w, double* out, uint64_t n);
+int pe_fluid_dfsph_get_boundary_forces(PeDfsph* w, double* out, uint64_t n);
+int pe_fluid_dfsph_get_alphas(PeDfsph* w, double* out, uint64_t n);
+/* Setting state keeps the neighbour lists, as writing the reference's public
+ * fields does; rebuild_neighbours refreshes them. */
+int pe_fluid_dfsph_set_positions(PeDfsph* w, const double* in, uint64_t n);
+int pe_fluid_dfsph_set_velocities(PeDfsph* w, const double* in, uint64_t n);
+/* Iterations of the last step's density and divergence solvers. */
+int pe_fluid_dfsph_last_iterations(PeDfsph* w, uint64_t out[2]);
+/* diagnostics.rs:74-88 mean |rho - rho0| / rho0; dfsph.rs:792 v_max. */
+int pe_fluid_dfsph_mean_density_error(PeDfsph* w, double* out);
+int pe_fluid_dfsph_v_max(PeDfsph* w, double* out);
+int pe_fluid_dfsph_status(PeDfsph* w, uint32_t* status);
+int pe_fluid_dfsph_kernel_launches(PeDfsph* w, uint64_t* out, int32_t reset);
+
 /* Fluid side of CoupledWcsphWorld::step (coupling.rs:853-866). A coupler holds
  * the rigid samples of a world: sample k is world particle particle[k] (an
  * oriented boundary sample) on body body[k] < n_bodies, at body-frame offset

@@ -90,6 +90,26 @@ class _Config(C.Structure):
 PRECISION_F64, PRECISION_F32 = 0, 1
 
 
+class _DfsphParams(C.Structure):
+    _fields_ = [
+        ("kernel", C.c_int32),
+        ("max_density_iters", C.c_uint64),
+        ("max_divergence_iters", C.c_uint64),
+        ("density_error_tol", C.c_double),
+        ("divergence_error_tol", C.c_double),
+        ("gravity", C.c_double * 3),
+        ("xsph_epsilon", C.c_double),
+        ("particle_diameter", C.c_double),
+        ("cfl_lambda", C.c_double),
+        ("adaptive_dt", C.c_int32),
+        ("warm_start", C.c_int32),
+        ("free_slip_set", C.c_int32 * 4),
+        ("free_slip", C.c_double * 4),
+        ("solver_omega", C.c_double),
+        ("max_velocity_correction", C.c_double),
+    ]
+
+
 class _PbfParams(C.Structure):
     _fields_ = [
         ("density_kernel", C.c_int32),
@@ -222,6 +242,34 @@ def load_library():
         "pe_fluid_pbf_v_max": (C.c_int, [vp, D3]),
         "pe_fluid_pbf_status": (C.c_int, [vp, C.POINTER(u32)]),
         "pe_fluid_pbf_kernel_launches": (C.c_int, [vp, C.POINTER(u64), i32]),
+        "pe_fluid_dfsph_params_default": (C.c_int, [C.POINTER(_DfsphParams)]),
+        "pe_fluid_dfsph_create": (C.c_int, [vp, C.POINTER(_DfsphParams), C.POINTER(_Config), C.POINTER(vp)]),
+        "pe_fluid_dfsph_destroy": (None, [vp]),
+        "pe_fluid_dfsph_step": (C.c_int, [vp, d]),
+        "pe_fluid_dfsph_run": (C.c_int, [vp, d, u64]),
+        "pe_fluid_dfsph_step_adaptive": (C.c_int, [vp, D3]),
+        "pe_fluid_dfsph_suggest_dt": (C.c_int, [vp, D3]),
+        "pe_fluid_dfsph_rebuild_neighbours": (C.c_int, [vp]),
+        "pe_fluid_dfsph_compute_density": (C.c_int, [vp]),
+        "pe_fluid_dfsph_compute_alpha": (C.c_int, [vp]),
+        "pe_fluid_dfsph_len": (C.c_int, [vp, C.POINTER(u64)]),
+        "pe_fluid_dfsph_get_time": (C.c_int, [vp, D3]),
+        "pe_fluid_dfsph_get_last_dt": (C.c_int, [vp, D3]),
+        "pe_fluid_dfsph_get_params": (C.c_int, [vp, C.POINTER(_DfsphParams)]),
+        "pe_fluid_dfsph_set_params": (C.c_int, [vp, C.POINTER(_DfsphParams)]),
+        "pe_fluid_dfsph_get_positions": (C.c_int, [vp, vp, u64]),
+        "pe_fluid_dfsph_get_velocities": (C.c_int, [vp, vp, u64]),
+        "pe_fluid_dfsph_get_densities": (C.c_int, [vp, vp, u64]),
+        "pe_fluid_dfsph_get_pressures": (C.c_int, [vp, vp, u64]),
+        "pe_fluid_dfsph_get_boundary_forces": (C.c_int, [vp, vp, u64]),
+        "pe_fluid_dfsph_get_alphas": (C.c_int, [vp, vp, u64]),
+        "pe_fluid_dfsph_set_positions": (C.c_int, [vp, vp, u64]),
+        "pe_fluid_dfsph_set_velocities": (C.c_int, [vp, vp, u64]),
+        "pe_fluid_dfsph_last_iterations": (C.c_int, [vp, vp]),
+        "pe_fluid_dfsph_mean_density_error": (C.c_int, [vp, D3]),
+        "pe_fluid_dfsph_v_max": (C.c_int, [vp, D3]),
+        "pe_fluid_dfsph_status": (C.c_int, [vp, C.POINTER(u32)]),
+        "pe_fluid_dfsph_kernel_launches": (C.c_int, [vp, C.POINTER(u64), i32]),
         "pe_fluid_coupler_create": (C.c_int, [vp, u32, u64, vp, vp, vp, vp, C.POINTER(vp)]),
         "pe_fluid_coupler_destroy": (None, [vp]),
         "pe_fluid_coupler_sync": (C.c_int, [vp, vp, vp, vp, vp]),
@@ -878,6 +926,205 @@ def particles_hash64(x, v, kind) -> int:
 
 
 # --------------------------------------------------------------------------
+# Divergence-free SPH (crates/pe-fluid/src/dfsph.rs)
+# --------------------------------------------------------------------------
+class DfsphParams:
+    """`DfsphParams` (dfsph.rs:33-80) without surface tension; the defaults are
+    `DfsphParams::default` (dfsph.rs:82-104). The free-slip planes are
+    `free_slip_xmin`, `free_slip_ymin`, `free_slip_xmax`, `free_slip_ymax`
+    (None = off)."""
+
+    _FIELDS = ("kernel", "max_density_iters", "max_divergence_iters", "density_error_tol",
+               "divergence_error_tol", "gravity", "xsph_epsilon", "particle_diameter", "cfl_lambda",
+               "adaptive_dt", "warm_start", "free_slip_xmin", "free_slip_ymin", "free_slip_xmax",
+               "free_slip_ymax", "solver_omega", "max_velocity_correction")
+    _SLIPS = ("free_slip_xmin", "free_slip_ymin", "free_slip_xmax", "free_slip_ymax")
+
+    def __init__(self, **kw):
+        c = _DfsphParams()
+        _ok(load_library().pe_fluid_dfsph_params_default(C.byref(c)), "dfsph_params_default")
+        self._load(c)
+        for k, v in kw.items():
+            if k not in self._FIELDS:
+                raise TypeError(f"unknown DfsphParams field {k!r}")
+            setattr(self, k, v)
+
+    def _load(self, c):
+        for k in self._FIELDS:
+            if k in self._SLIPS:
+                a = self._SLIPS.index(k)
+                setattr(self, k, float(c.free_slip[a]) if c.free_slip_set[a] else None)
+            elif k == "gravity":
+                self.gravity = tuple(c.gravity)
+            else:
+                setattr(self, k, getattr(c, k))
+        self.adaptive_dt, self.warm_start = bool(self.adaptive_dt), bool(self.warm_start)
+
+    def _to_c(self) -> _DfsphParams:
+        c = _DfsphParams()
+        c.kernel = int(self.kernel)
+        c.max_density_iters, c.max_divergence_iters = int(self.max_density_iters), int(self.max_divergence_iters)
+        c.density_error_tol, c.divergence_error_tol = float(self.density_error_tol), float(self.divergence_error_tol)
+        c.gravity[:] = [float(g) for g in self.gravity]
+        c.xsph_epsilon, c.particle_diameter = float(self.xsph_epsilon), float(self.particle_diameter)
+        c.cfl_lambda = float(self.cfl_lambda)
+        c.adaptive_dt, c.warm_start = 1 if self.adaptive_dt else 0, 1 if self.warm_start else 0
+        for a, k in enumerate(self._SLIPS):
+            v = getattr(self, k)
+            c.free_slip_set[a] = 0 if v is None else 1
+            c.free_slip[a] = 0.0 if v is None else float(v)
+        c.solver_omega, c.max_velocity_correction = float(self.solver_omega), float(self.max_velocity_correction)
+        return c
+
+    def __repr__(self):
+        return "DfsphParams(" + ", ".join(f"{k}={getattr(self, k)!r}" for k in self._FIELDS) + ")"
+
+
+class DfsphWorld:
+    """`DfsphWorld` (dfsph.rs:107-800) on one B200, bit-identical to the
+    reference's step. State arrays are in original order."""
+
+    def __init__(self, particles: Particles, params: DfsphParams | None = None,
+                 config: WcsphConfig | None = None):
+        L = load_library()
+        self._w = None
+        params = params if params is not None else DfsphParams()
+        h = C.c_void_p()
+        cfg = config._to_c() if config is not None else None
+        _ok(L.pe_fluid_dfsph_create(particles._p, C.byref(params._to_c()),
+                                    C.byref(cfg) if cfg is not None else None, C.byref(h)), "dfsph_create")
+        self._w = h
+        self.n = len(particles)
+        self._kinds = particles.arrays()["kind"].copy()
+        self.dim, self.mass, self.h, self.rest_density = particles.dim, particles.mass, particles.h, particles.rest_density
+
+    def close(self):
+        if getattr(self, "_w", None) and _lib is not None:
+            _lib.pe_fluid_dfsph_destroy(self._w)
+        self._w = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def step(self, dt: float):
+        _ok(_lib.pe_fluid_dfsph_step(self._w, float(dt)), "dfsph_step")
+
+    def run(self, dt: float, steps: int):
+        _ok(_lib.pe_fluid_dfsph_run(self._w, float(dt), int(steps)), "dfsph_run")
+
+    def step_adaptive(self) -> float:
+        d = C.c_double()
+        _ok(_lib.pe_fluid_dfsph_step_adaptive(self._w, C.byref(d)), "dfsph_step_adaptive")
+        return d.value
+
+    def suggest_dt(self) -> float:
+        d = C.c_double()
+        _ok(_lib.pe_fluid_dfsph_suggest_dt(self._w, C.byref(d)), "dfsph_suggest_dt")
+        return d.value
+
+    def rebuild_neighbours(self):
+        _ok(_lib.pe_fluid_dfsph_rebuild_neighbours(self._w), "dfsph_rebuild_neighbours")
+
+    def compute_density(self):
+        _ok(_lib.pe_fluid_dfsph_compute_density(self._w), "dfsph_compute_density")
+
+    def compute_alpha(self):
+        _ok(_lib.pe_fluid_dfsph_compute_alpha(self._w), "dfsph_compute_alpha")
+
+    @property
+    def t(self) -> float:
+        t = C.c_double()
+        _ok(_lib.pe_fluid_dfsph_get_time(self._w, C.byref(t)), "dfsph_time")
+        return t.value
+
+    @property
+    def last_dt(self) -> float:
+        t = C.c_double()
+        _ok(_lib.pe_fluid_dfsph_get_last_dt(self._w, C.byref(t)), "dfsph_last_dt")
+        return t.value
+
+    @property
+    def params(self) -> DfsphParams:
+        c = _DfsphParams()
+        _ok(_lib.pe_fluid_dfsph_get_params(self._w, C.byref(c)), "dfsph_params")
+        p = DfsphParams()
+        p._load(c)
+        return p
+
+    @params.setter
+    def params(self, p: DfsphParams):
+        _ok(_lib.pe_fluid_dfsph_set_params(self._w, C.byref(p._to_c())), "dfsph_set_params")
+
+    def _get(self, fn, shape, what):
+        out = np.empty(shape)
+        _ok(fn(self._w, _ptr(out), self.n), what)
+        return out
+
+    def positions(self):
+        return self._get(_lib.pe_fluid_dfsph_get_positions, (self.n, 3), "dfsph_positions")
+
+    def velocities(self):
+        return self._get(_lib.pe_fluid_dfsph_get_velocities, (self.n, 3), "dfsph_velocities")
+
+    def densities(self):
+        return self._get(_lib.pe_fluid_dfsph_get_densities, (self.n,), "dfsph_densities")
+
+    def pressures(self):
+        return self._get(_lib.pe_fluid_dfsph_get_pressures, (self.n,), "dfsph_pressures")
+
+    def boundary_forces(self):
+        return self._get(_lib.pe_fluid_dfsph_get_boundary_forces, (self.n, 3), "dfsph_boundary_forces")
+
+    def alphas(self):
+        return self._get(_lib.pe_fluid_dfsph_get_alphas, (self.n,), "dfsph_alphas")
+
+    def set_positions(self, x):
+        x = _arr(x, np.float64, (self.n, 3))
+        _ok(_lib.pe_fluid_dfsph_set_positions(self._w, _ptr(x), self.n), "dfsph_set_positions")
+
+    def set_velocities(self, v):
+        v = _arr(v, np.float64, (self.n, 3))
+        _ok(_lib.pe_fluid_dfsph_set_velocities(self._w, _ptr(v), self.n), "dfsph_set_velocities")
+
+    def last_iterations(self):
+        out = np.zeros(2, np.uint64)
+        _ok(_lib.pe_fluid_dfsph_last_iterations(self._w, _ptr(out)), "dfsph_iterations")
+        return int(out[0]), int(out[1])
+
+    def mean_density_error(self) -> float:
+        d = C.c_double()
+        _ok(_lib.pe_fluid_dfsph_mean_density_error(self._w, C.byref(d)), "dfsph_mean_density_error")
+        return d.value
+
+    def v_max(self) -> float:
+        d = C.c_double()
+        _ok(_lib.pe_fluid_dfsph_v_max(self._w, C.byref(d)), "dfsph_v_max")
+        return d.value
+
+    def status(self) -> int:
+        s = C.c_uint32()
+        _ok(_lib.pe_fluid_dfsph_status(self._w, C.byref(s)), "dfsph_status")
+        return s.value
+
+    def kernel_launches(self, reset=False) -> int:
+        c = C.c_uint64()
+        _ok(_lib.pe_fluid_dfsph_kernel_launches(self._w, C.byref(c), 1 if reset else 0), "dfsph_launches")
+        return c.value
+
+    def kinds(self):
+        return self._kinds
+
+    def hash64(self) -> int:
+        return particles_hash64(self.positions(), self.velocities(), self._kinds)
+
+
+# --------------------------------------------------------------------------
 # Fluid side of the WCSPH-rigid coupling (crates/pe-fluid/src/coupling.rs)
 # --------------------------------------------------------------------------
 class FluidRigidCoupler:
@@ -992,8 +1239,33 @@ def canonical_fluid_hash() -> int:
     return h
 
 
+DFSPH_HASH_STEPS, DFSPH_HASH_DT = 40, 1.0 / 120.0
+
+
+def dfsph_hash_world(config: WcsphConfig | None = None) -> DfsphWorld:
+    """The canonical DFSPH tank (scenarios.rs:74-116): the PBF tank's geometry
+    with the calibrated mass and recomputed Akinci volumes; 8 + 8 solver
+    iterations at 1% tolerance, XSPH 0.05, warm start, fixed dt."""
+    dx, rho0 = 0.05, 1000.0
+    h = 2.0 * dx
+    parts = Particles(DIM_3, rho0, mass_calibrated_to_rest(rho0, dx, h, DIM_3, CUBIC_SPLINE), h)
+    parts.fill_box((0.1, 0.1, 0.1), 4, 4, 4, dx)
+    parts.fill_box_boundary((0.0, 0.0, 0.0), (0.4, 0.4, 0.45), dx, 1)
+    parts.recomputed_akinci_psi(CUBIC_SPLINE)
+    params = DfsphParams(gravity=(0.0, 0.0, -STANDARD_GRAVITY), particle_diameter=dx, density_error_tol=0.01,
+                         divergence_error_tol=0.01, max_density_iters=8, max_divergence_iters=8,
+                         xsph_epsilon=0.05, adaptive_dt=False, warm_start=True)
+    return DfsphWorld(parts, params, config)
+
+
 def canonical_dfsph_hash() -> int:
-    raise NotImplementedError(_NOT_ON_PATH.format("DFSPH"))
+    """`dfsph_tank_hash` (scenarios.rs:119-125): the canonical DFSPH tank after
+    40 steps of 1/120 s, hashed; stepped on the GPU."""
+    w = dfsph_hash_world()
+    w.run(DFSPH_HASH_DT, DFSPH_HASH_STEPS)
+    h = w.hash64()
+    w.close()
+    return h
 
 
 def canonical_coupling_hash() -> int:
@@ -1096,7 +1368,22 @@ def fluid_pbf_tank_demo(n_side=4, steps=40, dt=1.0 / 120.0, dim="3"):
 
 
 def fluid_dfsph_tank_demo(n_side=4, steps=40, dt=1.0 / 120.0, dim="3"):
-    raise NotImplementedError(_NOT_ON_PATH.format("DFSPH"))
+    """Small DFSPH tank (python/src/fluid.rs:100-184): returns (fluid positions
+    [N, 3], fluid densities [N], mean density error)."""
+    d = _parse_dim(dim)
+    dx, rho0 = 0.05, 1000.0
+    h = 2.0 * dx
+    parts = _tank_parts(d, int(n_side), dx, h, mass_calibrated_to_rest(rho0, dx, h, d, CUBIC_SPLINE), rho0)
+    parts.recomputed_akinci_psi(CUBIC_SPLINE)
+    g = (0.0, -STANDARD_GRAVITY, 0.0) if d == DIM_2 else (0.0, 0.0, -STANDARD_GRAVITY)
+    w = DfsphWorld(parts, DfsphParams(gravity=g, particle_diameter=dx, adaptive_dt=False, max_density_iters=4,
+                                      max_divergence_iters=4, density_error_tol=0.01, divergence_error_tol=0.01))
+    w.run(float(dt), int(steps))
+    fluid = w.kinds() == FLUID
+    x, rho = w.positions(), w.densities()
+    err = _mean_density_error_diag(rho, w.kinds(), rho0)
+    w.close()
+    return x[fluid], rho[fluid], err
 
 
 def fluid_poly6_w0(h: float) -> float:
