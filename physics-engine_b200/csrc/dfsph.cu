@@ -4,11 +4,14 @@
 // Slot state: pos = (x, psi), vel = (v, rho), acc = (v*, warm-start kappa of
 // the density solver), nout = (n_out, warm-start kappa of the divergence
 // solver), bf = boundary reaction, p = the density solver's kappa (the
-// reference's pressure diagnostic). All of it moves with the re-sort. The
-// neighbour lists hold every candidate of the 27 (9) neighbour cells, as the
-// reference's do: the solver's neighbour count (dfsph.rs:281-296) and the
-// reaction weights (dfsph.rs:498-518) range over the whole candidate set, not
-// only the support.
+// reference's pressure diagnostic). All of it moves with the re-sort.
+//
+// Lists: a fluid slot's visit list holds its fluid neighbours in support and
+// every boundary candidate of the 27 (9) neighbour cells, as the reference's
+// lists do: the reaction weights (dfsph.rs:498-518) range over every boundary
+// candidate, in or out of the support. Fluid candidates out of the support add
+// +-0 and are left out; the solver's neighbour count (dfsph.rs:281-296), which
+// counts every candidate, takes them from the union size the list build records.
 //
 // Boundary reactions: the reference scatters, for fluid i in ascending index,
 // F_b(i) wt_ij / sum_j wt_ij onto each boundary candidate j. The neighbour
@@ -17,9 +20,15 @@
 // list), which is the reference's order of additions.
 //
 // The solvers' average errors are sequential sums in original index order
-// (dfsph.rs:552-569, 604-616): the per-particle terms are scattered to original
-// order and summed by one thread, so the convergence decision is the
-// reference's bit for bit. Compiled with --fmad=false.
+// (dfsph.rs:552-569, 604-616) of non-negative terms, and only their comparison
+// with the tolerance is used. Any summation order of n non-negative terms lies
+// within gamma_(n-1) = (n-1)u / (1 - (n-1)u) (relative) of the exact sum, so a
+// parallel sum S brackets the sequential one in S (1 +- 2 gamma / (1 - gamma)).
+// When the whole bracket, divided by the fluid count, falls on one side of the
+// tolerance, that is the reference's decision; otherwise the terms (scattered
+// to original order) are summed sequentially by one thread. Either way the
+// convergence decision is the reference's bit for bit. Compiled with
+// --fmad=false.
 #include <algorithm>
 #include <cmath>
 #include <limits>
@@ -185,6 +194,35 @@ __global__ void __launch_bounds__(kDfThreads) k_df_error(uint32_t n, DfsphConst 
     }
     kappa[i] = kap;
     err_orig[o] = e;
+}
+
+// Partial sums of v (any order: only bounds are taken from them).
+constexpr uint32_t kSumBlocks = 148, kSumThreads = 256;
+
+__global__ void __launch_bounds__(kSumThreads) k_df_partial_sums(uint32_t n, const double* __restrict__ v,
+                                                                double* __restrict__ part) {
+    __shared__ double red[kSumThreads];
+    double s = 0.0;
+    for (uint32_t i = blockIdx.x * kSumThreads + threadIdx.x; i < n; i += kSumBlocks * kSumThreads) s += v[i];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (uint32_t o = kSumThreads / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = red[0];
+}
+
+__global__ void __launch_bounds__(kSumThreads) k_df_final_sum(const double* __restrict__ part,
+                                                             double* __restrict__ out) {
+    __shared__ double red[kSumThreads];
+    red[threadIdx.x] = threadIdx.x < kSumBlocks ? part[threadIdx.x] : 0.0;
+    __syncthreads();
+    for (uint32_t o = kSumThreads / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out = red[0];
 }
 
 // Sequential sum in original index order (the reference's accumulation order).
@@ -378,12 +416,16 @@ __global__ void __launch_bounds__(kDfThreads) k_df_alpha(uint32_t n, DfsphConst 
     }
     const double4 xi = s.pos[i];
     double sx = 0.0, sy = 0.0, sz = 0.0, sq = 0.0;
-    uint32_t nn = 0;
+    uint32_t nb_all = 0, nb_kept = 0;
     for_each_loaded(
         list_ref(l, i, kListVisit), [&](uint32_t e) { return s.pos[e & kEntrySlotMask]; },
         [&](uint32_t e, const double4& xj) {
             const double mj = nmass(k, s, e, xj, xi);
-            if (mj == 0.0 && (e & kEntryBoundary)) return;
+            if (e & kEntryBoundary) {
+                ++nb_all;
+                if (mj == 0.0) return;
+                ++nb_kept;
+            }
             double gx, gy, gz;
             kfn_grad(k.kf, xj.x - xi.x, xj.y - xi.y, xj.z - xi.z, &gx, &gy, &gz);
             const double ax = gx * mj, ay = gy * mj, az = gz * mj;
@@ -391,8 +433,9 @@ __global__ void __launch_bounds__(kDfThreads) k_df_alpha(uint32_t n, DfsphConst 
             sy = sy + ay;
             sz = sz + az;
             sq += ax * ax + ay * ay + az * az;
-            ++nn;
         });
+    // every fluid candidate but i itself, and the boundary ones of non-zero mass
+    const uint32_t nn = (l.ncand[i] - 1u - nb_all) + nb_kept;
     if (nn < 2) {
         alpha[i] = 0.0;
         return;
@@ -448,7 +491,7 @@ DfsphSolver::DfsphSolver(const DfsphParams& prm, const WorldConfig& cfg, int dim
     wc.use_graph = 0;
     w_.reset(new World(wp, wc, dim, rest_density, mass, h, n, xs.data(), vs.data(), kind, psi, n_out, nullptr, 1,
                        kernel_support(prm.kernel, h)));
-    w_->list_all_candidates_ = true;
+    w_->list_keep_boundary_ = true;
     w_->refresh_step_const();
     const size_t N = std::max<uint64_t>(n, 1);
     alpha_ = w_->alloc<double>(N);
@@ -457,6 +500,7 @@ DfsphSolver::DfsphSolver(const DfsphParams& prm, const WorldConfig& cfg, int dim
     react_ = w_->alloc<double4>(N);
     err_orig_ = w_->alloc<double>(N);
     sum_ = w_->alloc<double>(1);
+    part_ = w_->alloc<double>(kSumBlocks);
     w_->check(cudaMallocHost(&sum_host_, sizeof(double)), "pinned");
     refresh_const();
     // dfsph.rs:177-179
@@ -604,12 +648,31 @@ double DfsphSolver::solve_error(double dt, bool divergence) {
     const uint32_t nb = blocks_for(n, kDfThreads);
     k_df_error<<<nb, kDfThreads, 0, w.st_>>>(n, kc_, divergence ? 1 : 0, dt, dt * dt, w.cur_, w.lists_, alpha_,
                                              kappa_, err_orig_);
-    k_df_serial_sum<<<1, 32, 0, w.st_>>>(n, err_orig_, sum_);
-    w.launches_ += 2;
-    // the pressure update is queued before the host reads the average
+    k_df_partial_sums<<<kSumBlocks, kSumThreads, 0, w.st_>>>(n, err_orig_, part_);
+    k_df_final_sum<<<1, kSumThreads, 0, w.st_>>>(part_, sum_);
+    w.launches_ += 3;
+    // the sequential sum's terms are kept until the decision is known: the
+    // pressure update does not touch them
     pressure_update(dt, divergence);
     w.check(cudaMemcpyAsync(sum_host_, sum_, sizeof(double), cudaMemcpyDeviceToHost, w.st_), "dfsph error");
     w.check(cudaStreamSynchronize(w.st_), "dfsph error");
+    const double tol = divergence ? prm_.divergence_error_tol : prm_.density_error_tol;
+    const double cnt = n_fluid_ > 0 ? (double)n_fluid_ : 1.0;
+    const double S = *sum_host_;
+    const double u = std::ldexp(1.0, -53);
+    const double nm1 = n > 1 ? (double)(n - 1) : 0.0;
+    const double gam = nm1 * u / (1.0 - nm1 * u);
+    // generous outward margin for the bracket's own roundings
+    const double delta = (2.0 * gam / (1.0 - gam)) * S * (1.0 + 1e-6) + 4.0 * std::numeric_limits<double>::denorm_min();
+    const double hi = (S + delta) / cnt, lo = std::fmax(S - delta, 0.0) / cnt;
+    if (std::isfinite(S) && hi <= tol) return S / cnt;            // the sequential average is <= tol too
+    if (std::isfinite(S) && lo > tol && lo == lo) return S / cnt;  // and > tol here
+    // within the bracket's width of the tolerance (or non-finite): the sequential sum decides
+    k_df_serial_sum<<<1, 32, 0, w.st_>>>(n, err_orig_, sum_);
+    w.launches_ += 1;
+    w.check(cudaMemcpyAsync(sum_host_, sum_, sizeof(double), cudaMemcpyDeviceToHost, w.st_), "dfsph error");
+    w.check(cudaStreamSynchronize(w.st_), "dfsph error");
+    ++serial_sums_;
     double avg = *sum_host_;
     if (n_fluid_ > 0) avg /= (double)n_fluid_;
     return avg;

@@ -63,6 +63,7 @@ class DfsphSolver {
     // the solvers' average errors of their last iteration
     double last_density_error() const { return err_density_; }
     double last_divergence_error() const { return err_divergence_; }
+    uint64_t serial_sums() const { return serial_sums_; }
     void get_alpha(double* out);          // original order
     // the public phase methods (dfsph.rs:201, 214, 252)
     void rebuild_neighbours();
@@ -97,6 +98,8 @@ class DfsphSolver {
     // per original index: a solver pass's error terms, summed in index order
     double* err_orig_ = nullptr;
     double* sum_ = nullptr;          // device scalar
+    double* part_ = nullptr;         // partial sums
+    uint64_t serial_sums_ = 0;       // decisions that needed the sequential sum
     double* sum_host_ = nullptr;     // pinned
 };
 

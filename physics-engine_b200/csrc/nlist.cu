@@ -170,6 +170,11 @@ __device__ __forceinline__ bool within(const float4& q, const float4& me, float 
     return dx * dx + dy * dy + dz * dz <= r2f;
 }
 
+// in-support, or a boundary candidate kept whatever its distance
+__device__ __forceinline__ bool keep_entry(const float4& q, const float4& me, float r2f, int keep_boundary) {
+    return within(q, me, r2f) || (keep_boundary && (__float_as_uint(q.w) & kStageBoundary));
+}
+
 __device__ __forceinline__ uint32_t rows_for(uint32_t n) { return (n + 3u) >> 2; }
 
 // Reserved block of one chunk: `rows_a + rows_b` rows of `stride` groups.
@@ -275,7 +280,8 @@ __global__ void __launch_bounds__(kNlThreads) k_nlist_visit(GridDesc g, Tanks tk
                             uint32_t m = 0;
 #pragma unroll
                             for (int bit = 0; bit < 32; ++bit)
-                                m |= within(s_pos[(w << 5) + bit], me, r2f) ? (1u << bit) : 0u;
+                                m |= keep_entry(s_pos[(w << 5) + bit], me, r2f, k.keep_boundary) ? (1u << bit)
+                                                                                                 : 0u;
                             if (w == W - 1u && (U & 31u)) m &= (1u << (U & 31u)) - 1u;
                             if (w == (myu >> 5)) m &= ~(1u << (myu & 31u));
                             s_mask[w * kChunk + lane] = m;
@@ -349,7 +355,8 @@ __global__ void __launch_bounds__(kNlThreads) k_nlist_visit(GridDesc g, Tanks tk
                                 if (slot == kslot) continue;
                                 uint8_t fl;
                                 uint32_t o;
-                                if (within(stage_entry<DIM>(s, slot, cu, &fl, &o), me, r2f)) ++nv;
+                                if (keep_entry(stage_entry<DIM>(s, slot, cu, &fl, &o), me, r2f, k.keep_boundary))
+                                    ++nv;
                             }
                         }
                     }
@@ -370,7 +377,7 @@ __global__ void __launch_bounds__(kNlThreads) k_nlist_visit(GridDesc g, Tanks tk
                                 uint8_t fl;
                                 uint32_t o;
                                 const float4 qp = stage_entry<DIM>(s, slot, cu, &fl, &o);
-                                if (!within(qp, me, r2f)) continue;
+                                if (!keep_entry(qp, me, r2f, k.keep_boundary)) continue;
                                 uint32_t e = slot | entry_flags(__float_as_uint(qp.w));
                                 if (LOWER_FLAGS && !(fl & kFlagBoundary) && o < myo) e |= kEntryLower;
                                 if (tv < nv) pv[(tv >> 2) * step + (tv & 3u)] = e;
@@ -507,7 +514,10 @@ __global__ void __launch_bounds__(kNlThreads) k_nlist_lower(GridDesc g, Tanks tk
                     // R = fluid union entries below this particle's index (all
                     // of them for a boundary particle)
                     R = nf;
-                    if (!(mw & kStageBoundary)) {
+                    const bool bcentre = mw & kStageBoundary;
+                    const float r2c = (bcentre && k.keep_boundary) ? __int_as_float(0x7f800000) : r2f;
+                    if (!bcentre && k.lower_boundary_only) R = 0;
+                    if (!bcentre && !k.lower_boundary_only) {
                         uint32_t lo = 0, hi = nf;
                         while (lo < hi) {
                             const uint32_t mid = (lo + hi) >> 1;
@@ -526,7 +536,7 @@ __global__ void __launch_bounds__(kNlThreads) k_nlist_lower(GridDesc g, Tanks tk
 #pragma unroll
                         for (int bit = 0; bit < 32; ++bit) {
                             const uint32_t i = (w << 5) + bit;
-                            m |= within(s_pos[s_sorted[i < nf ? i : 0u]], me, r2f) ? (1u << bit) : 0u;
+                            m |= within(s_pos[s_sorted[i < nf ? i : 0u]], me, r2c) ? (1u << bit) : 0u;
                         }
                         if (w == WR - 1u && (R & 31u)) m &= (1u << (R & 31u)) - 1u;
                         s_mask[w * kChunk + lane] = m;
@@ -581,17 +591,21 @@ __global__ void __launch_bounds__(kNlThreads) k_nlist_lower(GridDesc g, Tanks tk
                 float4 me = make_float4(0.f, 0.f, 0.f, 0.f);
                 bool fluidc = false;
                 uint32_t nl = 0;
+                float r2c = r2f;
                 if (active) {
                     me = stage_entry<DIM>(s, kslot, cu, &mfl, &myo);
                     fluidc = !(mfl & kFlagBoundary);
-                    for (int c = 0; c < NC; ++c) {
-                        const uint32_t q0 = s_cstart[c], q1 = q0 + (s_off[c + 1] - s_off[c]);
-                        for (uint32_t slot = q0; slot < q1; ++slot) {
-                            uint8_t fl;
-                            uint32_t o;
-                            const float4 qp = stage_entry<DIM>(s, slot, cu, &fl, &o);
-                            if ((fl & kFlagBoundary) || (fluidc && o >= myo)) continue;
-                            if (within(qp, me, r2f)) ++nl;
+                    if (!fluidc && k.keep_boundary) r2c = __int_as_float(0x7f800000);
+                    if (!(fluidc && k.lower_boundary_only)) {
+                        for (int c = 0; c < NC; ++c) {
+                            const uint32_t q0 = s_cstart[c], q1 = q0 + (s_off[c + 1] - s_off[c]);
+                            for (uint32_t slot = q0; slot < q1; ++slot) {
+                                uint8_t fl;
+                                uint32_t o;
+                                const float4 qp = stage_entry<DIM>(s, slot, cu, &fl, &o);
+                                if ((fl & kFlagBoundary) || (fluidc && o >= myo)) continue;
+                                if (within(qp, me, r2c)) ++nl;
+                            }
                         }
                     }
                 }
@@ -617,7 +631,7 @@ __global__ void __launch_bounds__(kNlThreads) k_nlist_lower(GridDesc g, Tanks tk
                                         continue;
                                     uint8_t fl;
                                     uint32_t oo;
-                                    if (within(stage_entry<DIM>(s, slot, cu, &fl, &oo), me, r2f)) {
+                                    if (within(stage_entry<DIM>(s, slot, cu, &fl, &oo), me, r2c)) {
                                         best = o;
                                         best_slot = slot;
                                     }

@@ -306,11 +306,6 @@ PbfSolver::PbfSolver(const PbfParams& prm, const WorldConfig& cfg, int dim, doub
     wc.use_graph = 0;
     w_.reset(new World(wp, wc, dim, rest_density, mass, h, n, x, v, kind, psi, n_out, nullptr, 1, support));
     const size_t N = std::max<uint64_t>(n, 1);
-    // pbf.rs:146-156: the lists hold every candidate of the neighbour cells,
-    // as the reference's, because the constraint iterations reuse them while
-    // the predictions move
-    w_->list_all_candidates_ = true;
-    w_->refresh_step_const();
     lambda_ = w_->alloc<double>(N);
     lambda_orig_ = w_->alloc<double>(N);
     dp_ = w_->alloc<double4>(N);
@@ -411,8 +406,14 @@ void PbfSolver::refresh_const() {
     k.gz = prm_.gravity[2];
 }
 
-void PbfSolver::lists() {
-    w_->ensure_lists(true);
+void PbfSolver::lists(bool all_candidates) {
+    World& w = *w_;
+    if (w.list_all_candidates_ != all_candidates) {
+        w.list_all_candidates_ = all_candidates;
+        w.refresh_step_const();
+        w.lists_valid_ = false;
+    }
+    w.ensure_lists(true);
 }
 
 void PbfSolver::step(double dt) {
@@ -428,7 +429,12 @@ void PbfSolver::step(double dt) {
     k_pbf_predict<<<nb, kPbfThreads, 0, st>>>(n, kc_, dt, w.cur_, w.pos_nx_);
     w.launches_ += 1;
     w.build_grid(w.pos_nx_, nullptr);
-    lists();
+    // pbf.rs:146-156: lists the constraint iterations reuse while the
+    // predictions move hold every candidate of the neighbour cells, as the
+    // reference's; lists used only at the positions they were built for keep
+    // the candidates in support (the others add +-0)
+    const bool reused = prm_.reuse_neighbours && prm_.iterations > 1;
+    lists(reused);
     // pbf.rs:403-411: constraint iterations
     for (uint64_t it = 0; it < prm_.iterations; ++it) {
         k_pbf_density<<<nb, kPbfThreads, 0, st>>>(n, kc_, w.cur_, w.lists_);
@@ -438,7 +444,7 @@ void PbfSolver::step(double dt) {
         w.launches_ += 4;
         if (!prm_.reuse_neighbours) {
             w.build_grid(nullptr, nullptr);
-            lists();
+            lists(false);
         }
     }
     // pbf.rs:413-426: velocities from the displacement, x = pred, grid and
@@ -446,7 +452,7 @@ void PbfSolver::step(double dt) {
     k_pbf_finalize<<<nb, kPbfThreads, 0, st>>>(n, dt, w.cur_);
     w.launches_ += 1;
     w.build_grid(nullptr, nullptr);
-    lists();
+    lists(false);
     k_pbf_density<<<nb, kPbfThreads, 0, st>>>(n, kc_, w.cur_, w.lists_);
     w.launches_ += 1;
     // pbf.rs:288-381: the grid on x equals the one just built

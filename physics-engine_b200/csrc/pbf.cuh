@@ -58,7 +58,7 @@ class PbfSolver {
 
    private:
     void refresh_const();
-    void lists();
+    void lists(bool all_candidates);
     std::unique_ptr<World> w_;
     PbfParams prm_;
     PbfConst kc_{};

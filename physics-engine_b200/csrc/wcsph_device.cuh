@@ -87,6 +87,11 @@ struct StepConst {
     double boundary_eps_h;     // 0.15 * h (particles.rs:132)
     int adapt_sound_speed;
     float r2_filter;           // conservative single-precision (2h)^2 bound
+    // List-build modes of the sibling solvers: visit lists keep every
+    // boundary candidate whatever its distance; lower lists are built for
+    // boundary slots only, holding every fluid candidate.
+    int keep_boundary;
+    int lower_boundary_only;
 };
 
 struct StateBufs {

@@ -448,6 +448,8 @@ void World::refresh_step_const() {
     k.r2_filter = list_all_candidates_
                       ? std::numeric_limits<float>::infinity()
                       : std::nextafter((float)(sup * sup * (1.0 + 1e-4)), std::numeric_limits<float>::infinity());
+    k.keep_boundary = list_keep_boundary_ ? 1 : 0;
+    k.lower_boundary_only = list_keep_boundary_ ? 1 : 0;
     kc_ = k;
 
     F32Const f{};

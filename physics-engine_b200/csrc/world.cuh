@@ -179,6 +179,10 @@ class World {
     // in support: solvers that reuse a list while particles move (PBF's
     // constraint iterations) need the reference's complete candidate set.
     bool list_all_candidates_ = false;
+    // Lists keep every boundary candidate (visit lists) and every fluid
+    // candidate of boundary slots (lower lists, built for boundary slots only):
+    // the DFSPH reaction weights range over those whole candidate sets.
+    bool list_keep_boundary_ = false;
     uint64_t n_;
     WorldParams prm_;
     WorldConfig cfg_;
