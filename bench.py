@@ -74,7 +74,7 @@ def _args():
                     help="learned form: seeded 64k-particle tanks rolled out for training")
     ap.add_argument("--train-steps", type=int, default=300, help="learned form: plain steps trained on")
     ap.add_argument("--rollout-steps", type=int, default=200, help="learned form: steps of the 1M rollout")
-    ap.add_argument("--form", choices=("plain", "f32", "batched", "learned"), default="plain",
+    ap.add_argument("--form", choices=("plain", "f32", "batched", "learned", "pbf", "dfsph"), default="plain",
                     help="plain: the f64 step (reference bits); f32: the single-precision "
                          "form, timed and compared with the f64 step after the same steps; "
                          "batched: 512 seeded tanks in one world against a loop of "
@@ -507,13 +507,150 @@ def run_learned_form(args, ws, rank, local, torch, pe):
         print(json.dumps(line), flush=True)
 
 
+SOLVER_DT = 1e-3  # PBF / DFSPH: 0.4 dx / (2 g H)^0.5 at dx 0.01 and a 1 m column
+SOLVER_DV_CAP = 0.5
+
+
+def solver_scene(pe, workload, form):
+    """The dam-break geometry for the sibling solvers (block two spacings off
+    the walls, as in the reference's canonical tanks), with the reference's own
+    solver setups: PBF as its canonical tank (scenarios.rs:28-61: poly6/spiky,
+    h = 2 dx, 4 iterations, no tensile correction), DFSPH as its canonical tank
+    (scenarios.rs:74-116: calibrated mass, recomputed Akinci volumes, 1%
+    tolerances, 8 + 8 iterations, XSPH 0.05, warm start) plus the reference's
+    cap on the per-iteration pressure velocity change (0.5 m/s): without it the
+    reference's DFSPH step diverges on lattice-start blocks of 24^3 and more."""
+    (nx, ny, nz), box = WORKLOADS[workload]
+    h = 2.0 * DX
+    if form == "pbf":
+        mass = pe.mass_from_spacing(1000.0, DX, 3)
+    else:
+        mass = pe.mass_calibrated_to_rest(1000.0, DX, h, 3)
+    p = pe.Particles(3, 1000.0, mass, h)
+    p.fill_box((2 * DX, 2 * DX, 2 * DX), nx, ny, nz, DX)
+    p.jitter_fluid(SEED, JITTER)
+    p.fill_box_boundary((0.0, 0.0, 0.0), box, DX, 1)
+    g = (0.0, 0.0, -9.81)
+    if form == "pbf":
+        prm = pe.PbfParams(gravity=g, iterations=4, art_pressure_k=0.0, vorticity_eps=0.0)
+    else:
+        p.recomputed_akinci_psi()
+        prm = pe.DfsphParams(gravity=g, particle_diameter=DX, density_error_tol=0.01, divergence_error_tol=0.01,
+                             max_density_iters=8, max_divergence_iters=8, xsph_epsilon=0.05, adaptive_dt=False,
+                             warm_start=True, max_velocity_correction=SOLVER_DV_CAP)
+    return p, prm, nx * ny * nz
+
+
+def solver_cpu_baseline(form, steps=2):
+    """The oracle's PBF / DFSPH step (CPU restatements pinned by the reference's
+    locked tank hashes), single thread, on the 32^3 dam break for `steps` steps."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    (nx, ny, nz), box = WORKLOADS["dam_break_32k"]
+    h = 2.0 * DX
+    mass = O.mass_from_spacing(1000.0, DX, 3) if form == "pbf" else O.mass_calibrated_to_rest(1000.0, DX, h, 3)
+    s = O.Scene(3, 1000.0, mass, h)
+    s.fill_box((2 * DX, 2 * DX, 2 * DX), nx, ny, nz, DX)
+    s.jitter_fluid(SEED, JITTER)
+    s.fill_box_boundary((0.0, 0.0, 0.0), box, DX, 1)
+    if form == "pbf":
+        q = O.pbf_default_params()
+        q.iterations, q.art_pressure_k, q.vorticity_eps = 4, 0.0, 0.0
+        q.gravity[:] = (0.0, 0.0, -9.81)
+        w = O.PbfWorld(s, q)
+    else:
+        s.recompute_psi()
+        q = O.dfsph_default_params()
+        q.particle_diameter, q.density_error_tol, q.divergence_error_tol = DX, 0.01, 0.01
+        q.max_density_iters, q.max_divergence_iters, q.xsph_epsilon, q.adaptive_dt = 8, 8, 0.05, 0
+        q.max_velocity_correction = SOLVER_DV_CAP
+        q.gravity[:] = (0.0, 0.0, -9.81)
+        w = O.DfsphWorld(s, q)
+    w.step(SOLVER_DT)
+    t0 = time.perf_counter()
+    w.run(SOLVER_DT, steps)
+    sec = time.perf_counter() - t0
+    nf = nx * ny * nz
+    name = "PbfWorld::step" if form == "pbf" else "DfsphWorld::step"
+    return {"value": nf * steps / sec, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"32^3 dam break (32,768 fluid), {steps} steps of the single-threaded C++ "
+                      f"restatement of {name}, -O2 -ffp-contract=off; {sec:.1f} s",
+            "host_cpus": os.cpu_count()}
+
+
+def run_solver_form(args, ws, rank, local, torch, pe):
+    """PBF or DFSPH on the dam break: the bit-exact GPU step (the reference's
+    solver path), timed with CUDA events on the world's stream."""
+    import numpy as np
+
+    form = args.form
+    ps, prm, nf = solver_scene(pe, args.workload, form)
+    nb = len(ps) - nf
+    cfg = pe.WcsphConfig(device=local)
+    w = pe.PbfWorld(ps, prm, cfg) if form == "pbf" else pe.DfsphWorld(ps, prm, cfg)
+    del ps
+    stream = torch.cuda.ExternalStream(w.stream_handle(), device=local)
+    w.run(SOLVER_DT, max(args.warmup, 3))
+    torch.cuda.synchronize()
+    iters = []
+    sampler = ClockSampler(local)
+    sampler.start()
+    w.kernel_launches(reset=True)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier = (lambda: torch.distributed.barrier()) if ws > 1 else (lambda: None)
+    barrier()
+    torch.cuda.synchronize()
+    a.record(stream)
+    for _ in range(args.steps):
+        w.step(SOLVER_DT)
+        if form == "dfsph":
+            iters.append(w.last_iterations())
+    b.record(stream)
+    b.synchronize()
+    torch.cuda.synchronize()
+    barrier()
+    ms = a.elapsed_time(b)
+    launches = w.kernel_launches()
+    clocks = sampler.stop()
+    status = w.status()
+    ms = max_over_ranks(ms, torch)
+    value = ws * nf * args.steps / (ms / 1e3)
+    fluid = w.kinds() == 0
+    rho = w.densities()[fluid]
+    v = w.velocities()[fluid]
+    line = {
+        "metric": f"SPH fluid particle-steps/s @1M ({form.upper()} step)", "value": value, "unit": UNIT,
+        "n_gpus": ws, "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "form": form,
+        "config": {"workload": args.workload, "fluid_particles": nf, "boundary_particles": nb, "dx": DX,
+                   "dt": SOLVER_DT, "h_over_dx": 2.0,
+                   "params": {k: getattr(prm, k) for k in type(prm)._FIELDS},
+                   "parallelism": f"{ws} independent tank(s), one per GPU",
+                   "l2": "state + neighbour lists exceed the 126 MB L2; no flush needed"},
+        "gpu_launches": int(launches), "status": int(status),
+        "state": {"mean_density_error": float(np.mean(np.abs(rho - 1000.0)) / 1000.0),
+                  "v_max": float(np.sqrt((v * v).sum(1).max()))},
+        "clocks": clocks,
+    }
+    if form == "dfsph":
+        it = np.array(iters)
+        line["solver_iterations_mean"] = {"density": float(it[:, 0].mean()), "divergence": float(it[:, 1].mean())}
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = solver_cpu_baseline(form)
+    w.close()
+    if rank == 0:
+        print(json.dumps(line, default=str), flush=True)
+
+
 def main():
     args = _args()
     ws, rank, local = _dist()
     if args.impl == "reference":
         run_reference(args, ws, rank)
         return
-    if args.form in ("f32", "batched", "learned"):
+    if args.form in ("f32", "batched", "learned", "pbf", "dfsph"):
         import torch
 
         torch.cuda.set_device(local)
@@ -523,7 +660,8 @@ def main():
             torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
         import physics_engine_rs as pe
 
-        {"f32": run_f32, "batched": run_batched, "learned": run_learned_form}[args.form](
+        {"f32": run_f32, "batched": run_batched, "learned": run_learned_form, "pbf": run_solver_form,
+         "dfsph": run_solver_form}[args.form](
             args, ws, rank, local, torch, pe)
         if ws > 1:
             torch.distributed.destroy_process_group()

@@ -220,6 +220,8 @@ int pe_fluid_pbf_mean_density_error(PePbf* w, double* out);
 int pe_fluid_pbf_v_max(PePbf* w, double* out);
 int pe_fluid_pbf_status(PePbf* w, uint32_t* status);
 int pe_fluid_pbf_kernel_launches(PePbf* w, uint64_t* out, int32_t reset);
+/* The CUDA stream (cudaStream_t) all of the world's work is issued on. */
+int pe_fluid_pbf_stream(PePbf* w, void** out);
 
 /* ---- Divergence-free SPH (crates/pe-fluid/src/dfsph.rs) ----
  * DfsphParams (dfsph.rs:33-80) without surface tension; the optional free-slip
@@ -287,6 +289,7 @@ int pe_fluid_dfsph_mean_density_error(PeDfsph* w, double* out);
 int pe_fluid_dfsph_v_max(PeDfsph* w, double* out);
 int pe_fluid_dfsph_status(PeDfsph* w, uint32_t* status);
 int pe_fluid_dfsph_kernel_launches(PeDfsph* w, uint64_t* out, int32_t reset);
+int pe_fluid_dfsph_stream(PeDfsph* w, void** out);
 
 /* Fluid side of CoupledWcsphWorld::step (coupling.rs:853-866). A coupler holds
  * the rigid samples of a world: sample k is world particle particle[k] (an

@@ -290,6 +290,12 @@ int pe_fluid_pbf_status(PePbf* w, uint32_t* status) {
     });
 }
 
+int pe_fluid_pbf_stream(PePbf* w, void** out) {
+    if (!w || !out) return PE_ERR_NULL;
+    *out = (void*)w->s->world().stream();
+    return PE_OK;
+}
+
 int pe_fluid_pbf_kernel_launches(PePbf* w, uint64_t* out, int32_t reset) {
     if (!w || !out) return PE_ERR_NULL;
     *out = w->s->world().kernel_launches();
@@ -502,6 +508,12 @@ int pe_fluid_dfsph_status(PeDfsph* w, uint32_t* status) {
         *status = w->s->world().status();
         return PE_OK;
     });
+}
+
+int pe_fluid_dfsph_stream(PeDfsph* w, void** out) {
+    if (!w || !out) return PE_ERR_NULL;
+    *out = (void*)w->s->world().stream();
+    return PE_OK;
 }
 
 int pe_fluid_dfsph_kernel_launches(PeDfsph* w, uint64_t* out, int32_t reset) {

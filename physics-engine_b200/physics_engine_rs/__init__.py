@@ -242,6 +242,7 @@ def load_library():
         "pe_fluid_pbf_v_max": (C.c_int, [vp, D3]),
         "pe_fluid_pbf_status": (C.c_int, [vp, C.POINTER(u32)]),
         "pe_fluid_pbf_kernel_launches": (C.c_int, [vp, C.POINTER(u64), i32]),
+        "pe_fluid_pbf_stream": (C.c_int, [vp, C.POINTER(vp)]),
         "pe_fluid_dfsph_params_default": (C.c_int, [C.POINTER(_DfsphParams)]),
         "pe_fluid_dfsph_create": (C.c_int, [vp, C.POINTER(_DfsphParams), C.POINTER(_Config), C.POINTER(vp)]),
         "pe_fluid_dfsph_destroy": (None, [vp]),
@@ -270,6 +271,7 @@ def load_library():
         "pe_fluid_dfsph_v_max": (C.c_int, [vp, D3]),
         "pe_fluid_dfsph_status": (C.c_int, [vp, C.POINTER(u32)]),
         "pe_fluid_dfsph_kernel_launches": (C.c_int, [vp, C.POINTER(u64), i32]),
+        "pe_fluid_dfsph_stream": (C.c_int, [vp, C.POINTER(vp)]),
         "pe_fluid_coupler_create": (C.c_int, [vp, u32, u64, vp, vp, vp, vp, C.POINTER(vp)]),
         "pe_fluid_coupler_destroy": (None, [vp]),
         "pe_fluid_coupler_sync": (C.c_int, [vp, vp, vp, vp, vp]),
@@ -899,6 +901,12 @@ class PbfWorld:
         _ok(_lib.pe_fluid_pbf_status(self._w, C.byref(s)), "pbf_status")
         return s.value
 
+    def stream_handle(self) -> int:
+        """The cudaStream_t (as an int) all of this world's kernels run on."""
+        h = C.c_void_p()
+        _ok(_lib.pe_fluid_pbf_stream(self._w, C.byref(h)), "stream")
+        return h.value or 0
+
     def kernel_launches(self, reset=False) -> int:
         c = C.c_uint64()
         _ok(_lib.pe_fluid_pbf_kernel_launches(self._w, C.byref(c), 1 if reset else 0), "pbf_launches")
@@ -1111,6 +1119,12 @@ class DfsphWorld:
         s = C.c_uint32()
         _ok(_lib.pe_fluid_dfsph_status(self._w, C.byref(s)), "dfsph_status")
         return s.value
+
+    def stream_handle(self) -> int:
+        """The cudaStream_t (as an int) all of this world's kernels run on."""
+        h = C.c_void_p()
+        _ok(_lib.pe_fluid_dfsph_stream(self._w, C.byref(h)), "stream")
+        return h.value or 0
 
     def kernel_launches(self, reset=False) -> int:
         c = C.c_uint64()
