@@ -67,8 +67,8 @@ extern "C" {
 
 /* WcsphParams (crates/pe-fluid/src/wcsph.rs:24-39) flattened:
  * TaitEos (eos.rs:32), MonaghanViscosity (viscosity.rs:30), Xsph
- * (viscosity.rs:77), gravity, adapt_sound_speed, surface tension sigma
- * (must be 0: the surface-tension branch, wcsph.rs:262, is not provided). */
+ * (viscosity.rs:77), gravity, adapt_sound_speed, and SurfaceTensionParams
+ * (surface_tension.rs:38-46; the branch of wcsph.rs:261-278, f64 only). */
 typedef struct PeWcsphParams {
     int32_t density_kernel;
     double eos_rest_density;
@@ -80,8 +80,15 @@ typedef struct PeWcsphParams {
     double xsph_epsilon;
     double gravity[3];
     int32_t adapt_sound_speed;
-    double surface_tension_sigma;
+    double surface_tension_sigma;          /* SurfaceTensionParams.sigma; 0 = off */
+    int32_t surface_tension_model;         /* PE_SURFACE_TENSION_* */
+    double surface_tension_colour_gamma;   /* SurfaceTensionParams.colour_gamma */
 } PeWcsphParams;
+
+/* SurfaceTensionModel (crates/pe-fluid/src/surface_tension.rs:27-34). */
+#define PE_SURFACE_TENSION_NONE 0
+#define PE_SURFACE_TENSION_AKINCI 1
+#define PE_SURFACE_TENSION_COLOUR_FIELD 2
 
 /* GPU placement and capacities (no reference counterpart; zeros = defaults). */
 typedef struct PeWcsphConfig {

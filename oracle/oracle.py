@@ -37,6 +37,9 @@ class OParams(C.Structure):
         ("gravity", C.c_double * 3),
         ("adapt_sound_speed", C.c_int32),
         ("materialize_neigh_lists", C.c_int32),
+        ("st_model", C.c_int32),
+        ("st_sigma", C.c_double),
+        ("st_colour_gamma", C.c_double),
     ]
 
 

@@ -488,7 +488,20 @@ struct WParams {
     double gravity[3];         // wcsph.rs:34
     int32_t adapt_sound_speed; // wcsph.rs:36
     int32_t materialize_neigh_lists;  // wcsph.rs:102-113 (1 = as the reference)
+    // SurfaceTensionParams (surface_tension.rs:38-46): model 0 None,
+    // 1 Akinci2013, 2 ColourField
+    int32_t st_model;
+    double st_sigma, st_colour_gamma;
 };
+
+// surface_tension.rs:78-103 cohesion kernels (support h)
+static double cohesion_kernel(double r, double h, Dim dim) {
+    if (r <= 0.0 || r >= h || h <= 0.0) return 0.0;
+    double q = r / h;
+    double t = 1.0 - q;
+    if (dim == D2) return 16.0 / (PI * h * h) * t * t * t * q * q * q;
+    return 32.0 / (PI * oracle_pow(h, 3.0)) * t * t * t * q * q * q;
+}
 
 struct World {
     Particles parts;
@@ -499,6 +512,7 @@ struct World {
     std::vector<std::vector<size_t>> neigh_lists;
     std::vector<V3> xsph_dv;
     std::vector<V3> boundary_force;
+    std::vector<V3> st_normals, st_a;
 
     KernelKind kk() const { return (KernelKind)prm.kernel; }
 
@@ -624,6 +638,79 @@ struct World {
                 }
             }
             parts.a[i] += g;
+        }
+        // wcsph.rs:261-278 optional surface tension
+        if (prm.st_sigma != 0.0) {
+            surface_tension_accel(st_normals, st_a);
+            for (size_t i = 0; i < n; ++i)
+                if (parts.kind[i] == FLUID) parts.a[i] += st_a[i];
+        }
+    }
+    // surface_tension.rs:112-220 surface_tension_accel over the grid's lists
+    void surface_tension_accel(std::vector<V3>& normals, std::vector<V3>& out) {
+        const size_t n = parts.len();
+        normals.assign(n, zero3());
+        out.assign(n, zero3());
+        if (prm.st_model == 0 || prm.st_sigma == 0.0) return;
+        const double h = parts.h, mass = parts.mass;
+        const Dim dim = parts.dim;
+        for (size_t i = 0; i < n; ++i) {
+            if (parts.kind[i] != FLUID) continue;
+            neigh.clear();
+            grid.neighbours(i, neigh);
+            V3 xi = parts.x[i];
+            V3 ni = zero3();
+            for (size_t j : neigh) {
+                if (j == i || parts.kind[j] != FLUID) continue;
+                V3 gw = grad_w(kk(), parts.x[j] - xi, h, dim);
+                ni += gw * (mass / std::fmax(parts.rho[j], 1e-12));
+            }
+            normals[i] = ni * h;
+        }
+        if (prm.st_model == 1) {
+            const double dim_scale = dim == D2 ? 1.0 / 20.0 : 1.0;
+            const double sigma_eff = prm.st_sigma * dim_scale;
+            for (size_t i = 0; i < n; ++i) {
+                if (parts.kind[i] != FLUID) continue;
+                neigh.clear();
+                grid.neighbours(i, neigh);
+                V3 xi = parts.x[i];
+                V3 f = zero3();
+                for (size_t j : neigh) {
+                    if (j == i || parts.kind[j] != FLUID) continue;
+                    V3 rij = parts.x[j] - xi;
+                    double r = norm(rij);
+                    if (r < 1e-12) continue;
+                    V3 r_hat{rij.x / r, rij.y / r, rij.z / r};
+                    double c = cohesion_kernel(r, h, dim);
+                    f += r_hat * (sigma_eff * mass * mass * c);
+                    f += (normals[i] - normals[j]) * (-sigma_eff * mass);
+                }
+                out[i] = V3{f.x / mass, f.y / mass, f.z / mass};
+            }
+        } else if (prm.st_model == 2) {
+            const double gamma = prm.st_colour_gamma;
+            for (size_t i = 0; i < n; ++i) {
+                if (parts.kind[i] != FLUID) continue;
+                V3 ni = normals[i];
+                double n_len = norm(ni);
+                if (n_len < 1e-8) continue;
+                V3 n_hat{ni.x / n_len, ni.y / n_len, ni.z / n_len};
+                neigh.clear();
+                grid.neighbours(i, neigh);
+                V3 xi = parts.x[i];
+                double div_n = 0.0;
+                for (size_t j : neigh) {
+                    if (j == i || parts.kind[j] != FLUID) continue;
+                    V3 gw = grad_w(kk(), parts.x[j] - xi, h, dim);
+                    V3 nj = normals[j];
+                    double nj_len = norm(nj);
+                    V3 nj_hat = nj_len > 1e-8 ? V3{nj.x / nj_len, nj.y / nj_len, nj.z / nj_len} : zero3();
+                    div_n += (mass / std::fmax(parts.rho[j], 1e-12)) * dot(nj_hat - n_hat, gw);
+                }
+                double kappa = -div_n;
+                out[i] = n_hat * (-gamma * kappa / std::fmax(parts.rho[i], 1e-12));
+            }
         }
     }
     // wcsph.rs:283 apply_xsph

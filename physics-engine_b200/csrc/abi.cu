@@ -74,6 +74,8 @@ pe::WorldParams to_world(const PeWcsphParams& p) {
     for (int i = 0; i < 3; ++i) w.gravity[i] = p.gravity[i];
     w.adapt_sound_speed = p.adapt_sound_speed;
     w.surface_tension_sigma = p.surface_tension_sigma;
+    w.surface_tension_model = p.surface_tension_model;
+    w.surface_tension_colour_gamma = p.surface_tension_colour_gamma;
     return w;
 }
 
@@ -90,13 +92,18 @@ PeWcsphParams from_world(const pe::WorldParams& w) {
     for (int i = 0; i < 3; ++i) p.gravity[i] = w.gravity[i];
     p.adapt_sound_speed = w.adapt_sound_speed;
     p.surface_tension_sigma = w.surface_tension_sigma;
+    p.surface_tension_model = w.surface_tension_model;
+    p.surface_tension_colour_gamma = w.surface_tension_colour_gamma;
     return p;
 }
 
 int check_params(const PeWcsphParams* p) {
     if (!p) return PE_ERR_NULL;
     if (p->density_kernel != PE_KERNEL_CUBIC_SPLINE) return PE_ERR_UNSUPPORTED;
-    if (p->surface_tension_sigma != 0.0) return PE_ERR_UNSUPPORTED;
+    if (!std::isfinite(p->surface_tension_sigma) || !std::isfinite(p->surface_tension_colour_gamma))
+        return PE_ERR_ARG;
+    if (p->surface_tension_model < PE_SURFACE_TENSION_NONE || p->surface_tension_model > PE_SURFACE_TENSION_COLOUR_FIELD)
+        return PE_ERR_ARG;
     const double v[] = {p->eos_rest_density, p->eos_sound_speed, p->eos_gamma, p->visc_alpha,
                         p->visc_beta,        p->visc_eps,        p->xsph_epsilon};
     for (double d : v)
@@ -389,7 +396,9 @@ int pe_fluid_wcsph_params_water(double rest_density, double sound_speed, const d
     p.xsph_epsilon = 0.25;             // viscosity.rs:82-86
     for (int i = 0; i < 3; ++i) p.gravity[i] = gravity[i];
     p.adapt_sound_speed = 1;           // wcsph.rs:50
-    p.surface_tension_sigma = 0.0;     // wcsph.rs:51
+    p.surface_tension_sigma = 0.0;     // wcsph.rs:51 SurfaceTensionParams::disabled()
+    p.surface_tension_model = PE_SURFACE_TENSION_NONE;
+    p.surface_tension_colour_gamma = 0.0;
     *out = p;
     return PE_OK;
 }
@@ -420,6 +429,8 @@ int pe_fluid_wcsph_create_batch(const PeWcsphParams* params, int32_t dim, double
     *out = nullptr;
     int rc = check_params(params);
     if (rc != PE_OK) return rc;
+    if (cfg && cfg->precision == PE_PRECISION_F32 && params->surface_tension_sigma != 0.0)
+        return PE_ERR_UNSUPPORTED;  // the surface-tension branch runs in the f64 step only
     if (!valid_dim(dim)) return PE_ERR_ARG;
     if (!(std::isfinite(rest_density) && rest_density > 0.0 && std::isfinite(mass) && mass > 0.0 &&
           std::isfinite(h) && h > 0.0))
@@ -578,6 +589,7 @@ int pe_fluid_wcsph_set_params(PeWcsph* w, const PeWcsphParams* params) {
     if (!w) return PE_ERR_NULL;
     int rc = check_params(params);
     if (rc != PE_OK) return rc;
+    if (w->world->single_precision() && params->surface_tension_sigma != 0.0) return PE_ERR_UNSUPPORTED;
     return guard([&] {
         w->world->set_params(to_world(*params));
         return PE_OK;

@@ -1,4 +1,4 @@
-// Neighbour-list build: CTAs per occupied cell, two kernels.
+// Neighbour-list build: CTAs per occupied cell.
 //
 // Replaces the per-particle `UniformGrid::neighbours` gathers
 // (crates/pe-fluid/src/grid.rs:122-140) that the reference repeats six times
@@ -13,16 +13,17 @@
 // candidates are harmless: the f64 passes evaluate q exactly and such pairs
 // contribute an exact +-0.
 //
-// k_nlist_visit writes, for fluid particles, the "visit" list (in-support
+// k_nlist_both writes, for fluid particles, the "visit" list (in-support
 // candidates, self excluded, in visiting order, each flagged boundary /
 // oriented / lower; the force pass reads its unflagged entries as the
-// reference's j > i and boundary pairs). k_nlist_lower writes the "lower"
-// list: for fluid particles
-// the fluid neighbours with a smaller original index, for boundary particles
-// all fluid neighbours, both in ascending original index; the order comes
-// from a shared-memory radix sort of the union's fluid entries per cell.
+// reference's j > i and boundary pairs) and the "lower" list: for fluid
+// particles the fluid neighbours with a smaller original index, for boundary
+// particles all fluid neighbours, both in ascending original index; the order
+// comes from a shared-memory radix sort of the union's fluid entries per
+// cell. k_nlist_visit writes the visit list alone (the passes that need no
+// ascending-index order).
 //
-// Both kernels work on chunks of up to 64 centre particles with four threads
+// The kernels work on chunks of up to 64 centre particles with four threads
 // per particle, each taking a quarter of the candidates (union words, or
 // sorted positions). A first pass keeps the in-support bit masks in shared
 // memory and counts; the chunk's longest lists size one block of the list
@@ -217,6 +218,201 @@ __device__ __forceinline__ ChunkBlock reserve_chunk(const ListBufs& l, DeviceSca
     return *s_blk;
 }
 
+// LSD radix sort of a union's fluid positions (s_sorted[0..nf)) by original
+// index, on 4-bit digits of (orig - omin); keys are read through the staged
+// positions. The keys are unique, so the result does not depend on the
+// staging order. Ends with a block barrier.
+__device__ __forceinline__ void radix_sort_by_orig(const float4* s_pos, uint16_t* s_sorted, uint16_t* s_tmp,
+                                                   uint16_t* s_cnt, uint32_t nf, uint32_t omin, uint32_t omax) {
+    const uint32_t tid = threadIdx.x;
+    const uint32_t span = nf ? omax - omin : 0u;
+    const int npass = span ? (32 - __clz(span) + 3) / 4 : 0;
+    const uint32_t chunk = (nf + kNlThreads - 1) / kNlThreads;
+    const uint32_t e0 = min(nf, tid * chunk), e1 = min(nf, e0 + chunk);
+    uint16_t *src = s_sorted, *dst = s_tmp;
+    for (int pass = 0; pass < npass; ++pass) {
+        const int shift = 4 * pass;
+#pragma unroll
+        for (int d = 0; d < 16; ++d) s_cnt[d * kNlThreads + tid] = 0;
+        for (uint32_t e = e0; e < e1; ++e) {
+            const uint32_t o = __float_as_uint(s_pos[src[e]].w) & kStageOrigMask;
+            ++s_cnt[(((o - omin) >> shift) & 15u) * kNlThreads + tid];
+        }
+        __syncthreads();
+        {
+            uint32_t v[16], sum = 0;
+#pragma unroll
+            for (int d = 0; d < 16; ++d) {
+                v[d] = s_cnt[tid * 16 + d];
+                sum += v[d];
+            }
+            uint32_t ex, tot;
+            block_exclusive_scan(sum, &ex, &tot);
+#pragma unroll
+            for (int d = 0; d < 16; ++d) {
+                s_cnt[tid * 16 + d] = (uint16_t)ex;
+                ex += v[d];
+            }
+        }
+        __syncthreads();
+        for (uint32_t e = e0; e < e1; ++e) {
+            const uint16_t pu = src[e];
+            const uint32_t o = __float_as_uint(s_pos[pu].w) & kStageOrigMask;
+            dst[s_cnt[(((o - omin) >> shift) & 15u) * kNlThreads + tid]++] = pu;
+        }
+        __syncthreads();
+        uint16_t* t = src;
+        src = dst;
+        dst = t;
+    }
+    if (src != s_sorted) {
+        for (uint32_t i = tid; i < nf; i += blockDim.x) s_sorted[i] = src[i];
+    }
+    __syncthreads();
+}
+
+// Slow path of the visit list for a union larger than the stage.
+template <int DIM, bool LOWER_FLAGS>
+__device__ __forceinline__ void visit_slow(const StepConst& k, float r2f, const CellUnion& cu, uint32_t U,
+                                           const StateBufs& s, const ListBufs& l, DeviceScalars* sc,
+                                           const uint32_t* s_cstart, const uint32_t* s_off, uint32_t (*s_red)[2],
+                                           ChunkBlock* s_blk, bool* s_overflow) {
+    constexpr int NC = DIM == 3 ? 27 : 9;
+    const uint32_t tid = threadIdx.x;
+    // Slow path: a union larger than the stage, straight from global
+    // memory, one thread per centre particle: count, reserve, write.
+    if (tid == 0) atomicOr(&sc->status, kStatusSlowUnion);
+    for (uint32_t c0 = 0; c0 < cu.ncenter; c0 += kNlThreads) {
+        const uint32_t nc = min((uint32_t)kNlThreads, cu.ncenter - c0);
+        const bool active = tid < nc;
+        const uint32_t kslot = cu.cs + c0 + tid;
+        uint8_t mfl = 0;
+        uint32_t myo = 0;
+        float4 me = make_float4(0.f, 0.f, 0.f, 0.f);
+        uint32_t nv = 0;
+        bool fluidc = false;
+        if (active) {
+            me = stage_entry<DIM>(s, kslot, cu, &mfl, &myo);
+            fluidc = !(mfl & kFlagBoundary);
+            if (fluidc) {
+                for (int c = 0; c < NC; ++c) {
+                    const uint32_t q0 = s_cstart[c], q1 = q0 + (s_off[c + 1] - s_off[c]);
+                    for (uint32_t slot = q0; slot < q1; ++slot) {
+                        if (slot == kslot) continue;
+                        uint8_t fl;
+                        uint32_t o;
+                        if (keep_entry(stage_entry<DIM>(s, slot, cu, &fl, &o), me, r2f, k.keep_boundary))
+                            ++nv;
+                    }
+                }
+            }
+        }
+        const ChunkBlock blk = reserve_chunk(l, sc, nc, nv, 0u, s_red, s_blk, s_overflow);
+        if (active) {
+            const uint32_t gv = (uint32_t)blk.base + tid;
+            l.desc[kslot] = blk.ok ? make_uint4(gv, nc, nv, 0u) : make_uint4(0u, 0u, 0u, 0u);
+            l.ncand[kslot] = fluidc ? U : 0u;
+            if (blk.ok && fluidc) {
+                const size_t step = 4u * nc;
+                uint32_t* pv = l.pool + 4 * (size_t)gv;
+                uint32_t tv = 0;
+                for (int c = 0; c < NC; ++c) {
+                    const uint32_t q0 = s_cstart[c], q1 = q0 + (s_off[c + 1] - s_off[c]);
+                    for (uint32_t slot = q0; slot < q1; ++slot) {
+                        if (slot == kslot) continue;
+                        uint8_t fl;
+                        uint32_t o;
+                        const float4 qp = stage_entry<DIM>(s, slot, cu, &fl, &o);
+                        if (!keep_entry(qp, me, r2f, k.keep_boundary)) continue;
+                        uint32_t e = slot | entry_flags(__float_as_uint(qp.w));
+                        if (LOWER_FLAGS && !(fl & kFlagBoundary) && o < myo) e |= kEntryLower;
+                        if (tv < nv) pv[(tv >> 2) * step + (tv & 3u)] = e;
+                        ++tv;
+                    }
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Slow path of the lower list for a union larger than the stage.
+template <int DIM>
+__device__ __forceinline__ void lower_slow(const StepConst& k, float r2f, const CellUnion& cu, const StateBufs& s,
+                                           const ListBufs& l, DeviceScalars* sc, const uint32_t* s_cstart,
+                                           const uint32_t* s_off, uint32_t (*s_red)[2], ChunkBlock* s_blk,
+                                           bool* s_overflow) {
+    constexpr int NC = DIM == 3 ? 27 : 9;
+    const uint32_t tid = threadIdx.x;
+    // Slow path: ascending original index by repeated selection, one
+    // thread per centre particle: count, reserve, write.
+    if (tid == 0) atomicOr(&sc->status, kStatusSlowUnion);
+    for (uint32_t c0 = 0; c0 < cu.ncenter; c0 += kNlThreads) {
+        const uint32_t nc = min((uint32_t)kNlThreads, cu.ncenter - c0);
+        const bool active = tid < nc;
+        const uint32_t kslot = cu.cs + c0 + tid;
+        uint8_t mfl = 0;
+        uint32_t myo = 0;
+        float4 me = make_float4(0.f, 0.f, 0.f, 0.f);
+        bool fluidc = false;
+        uint32_t nl = 0;
+        float r2c = r2f;
+        if (active) {
+            me = stage_entry<DIM>(s, kslot, cu, &mfl, &myo);
+            fluidc = !(mfl & kFlagBoundary);
+            if (!fluidc && k.keep_boundary) r2c = __int_as_float(0x7f800000);
+            if (!(fluidc && k.lower_boundary_only)) {
+                for (int c = 0; c < NC; ++c) {
+                    const uint32_t q0 = s_cstart[c], q1 = q0 + (s_off[c + 1] - s_off[c]);
+                    for (uint32_t slot = q0; slot < q1; ++slot) {
+                        uint8_t fl;
+                        uint32_t o;
+                        const float4 qp = stage_entry<DIM>(s, slot, cu, &fl, &o);
+                        if ((fl & kFlagBoundary) || (fluidc && o >= myo)) continue;
+                        if (within(qp, me, r2c)) ++nl;
+                    }
+                }
+            }
+        }
+        const ChunkBlock blk = reserve_chunk(l, sc, nc, nl, 0u, s_red, s_blk, s_overflow);
+        if (active) {
+            const uint32_t gl = (uint32_t)blk.base + tid;
+            l.ldesc[kslot] = blk.ok ? make_uint2(gl, nl | (nc << 16)) : make_uint2(0u, 0u);
+            if (blk.ok) {
+                const size_t step = 4u * nc;
+                uint32_t* pl = l.pool + 4 * (size_t)gl;
+                uint32_t tl = 0;
+                long long last = -1;
+                while (tl < nl) {
+                    unsigned long long best = ULLONG_MAX;
+                    uint32_t best_slot = 0;
+                    for (int c = 0; c < NC; ++c) {
+                        const uint32_t q0 = s_cstart[c], q1 = q0 + (s_off[c + 1] - s_off[c]);
+                        for (uint32_t slot = q0; slot < q1; ++slot) {
+                            if (s.flags[slot] & kFlagBoundary) continue;
+                            const uint32_t o = s.orig[slot];
+                            if ((long long)o <= last || (fluidc && o >= myo) ||
+                                (unsigned long long)o >= best)
+                                continue;
+                            uint8_t fl;
+                            uint32_t oo;
+                            if (within(stage_entry<DIM>(s, slot, cu, &fl, &oo), me, r2c)) {
+                                best = o;
+                                best_slot = slot;
+                            }
+                        }
+                    }
+                    if (best == ULLONG_MAX) break;
+                    pl[(tl >> 2) * step + (tl & 3u)] = best_slot;
+                    ++tl;
+                    last = (long long)best;
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
 // ----------------------------------------------------------------- visit
 // Dynamic shared memory (ucap a multiple of kStageStep): float4 s_pos[ucap];
 // uint32 s_ent[ucap]; uint32 s_mask[(ucap / 32) * kChunk] (word w of chunk
@@ -234,7 +430,7 @@ __global__ void __launch_bounds__(kNlThreads) k_nlist_visit(GridDesc g, Tanks tk
     uint32_t* s_mask = s_ent + ucap;
     __shared__ uint32_t s_cstart[NC];
     __shared__ uint32_t s_off[NC + 1];
-    __shared__ uint32_t s_cv[kWays][kChunk], s_cu[kWays][kChunk];
+    __shared__ uint32_t s_cv[kWays][kChunk];
     __shared__ uint32_t s_red[kWarps][2];
     __shared__ ChunkBlock s_blk;
     __shared__ bool s_overflow;
@@ -333,61 +529,7 @@ __global__ void __launch_bounds__(kNlThreads) k_nlist_visit(GridDesc g, Tanks tk
                 __syncthreads();  // masks and counts are reused by the next chunk
             }
         } else {
-            // Slow path: a union larger than the stage, straight from global
-            // memory, one thread per centre particle: count, reserve, write.
-            if (tid == 0) atomicOr(&sc->status, kStatusSlowUnion);
-            for (uint32_t c0 = 0; c0 < cu.ncenter; c0 += kNlThreads) {
-                const uint32_t nc = min((uint32_t)kNlThreads, cu.ncenter - c0);
-                const bool active = tid < nc;
-                const uint32_t kslot = cu.cs + c0 + tid;
-                uint8_t mfl = 0;
-                uint32_t myo = 0;
-                float4 me = make_float4(0.f, 0.f, 0.f, 0.f);
-                uint32_t nv = 0;
-                bool fluidc = false;
-                if (active) {
-                    me = stage_entry<DIM>(s, kslot, cu, &mfl, &myo);
-                    fluidc = !(mfl & kFlagBoundary);
-                    if (fluidc) {
-                        for (int c = 0; c < NC; ++c) {
-                            const uint32_t q0 = s_cstart[c], q1 = q0 + (s_off[c + 1] - s_off[c]);
-                            for (uint32_t slot = q0; slot < q1; ++slot) {
-                                if (slot == kslot) continue;
-                                uint8_t fl;
-                                uint32_t o;
-                                if (keep_entry(stage_entry<DIM>(s, slot, cu, &fl, &o), me, r2f, k.keep_boundary))
-                                    ++nv;
-                            }
-                        }
-                    }
-                }
-                const ChunkBlock blk = reserve_chunk(l, sc, nc, nv, 0u, s_red, &s_blk, &s_overflow);
-                if (active) {
-                    const uint32_t gv = (uint32_t)blk.base + tid;
-                    l.desc[kslot] = blk.ok ? make_uint4(gv, nc, nv, 0u) : make_uint4(0u, 0u, 0u, 0u);
-                    l.ncand[kslot] = fluidc ? U : 0u;
-                    if (blk.ok && fluidc) {
-                        const size_t step = 4u * nc;
-                        uint32_t* pv = l.pool + 4 * (size_t)gv;
-                        uint32_t tv = 0;
-                        for (int c = 0; c < NC; ++c) {
-                            const uint32_t q0 = s_cstart[c], q1 = q0 + (s_off[c + 1] - s_off[c]);
-                            for (uint32_t slot = q0; slot < q1; ++slot) {
-                                if (slot == kslot) continue;
-                                uint8_t fl;
-                                uint32_t o;
-                                const float4 qp = stage_entry<DIM>(s, slot, cu, &fl, &o);
-                                if (!keep_entry(qp, me, r2f, k.keep_boundary)) continue;
-                                uint32_t e = slot | entry_flags(__float_as_uint(qp.w));
-                                if (LOWER_FLAGS && !(fl & kFlagBoundary) && o < myo) e |= kEntryLower;
-                                if (tv < nv) pv[(tv >> 2) * step + (tv & 3u)] = e;
-                                ++tv;
-                            }
-                        }
-                    }
-                }
-                __syncthreads();
-            }
+            visit_slow<DIM, LOWER_FLAGS>(k, r2f, cu, U, s, l, sc, s_cstart, s_off, s_red, &s_blk, &s_overflow);
         }
         __syncthreads();  // shared memory is reused by the next cell
     }
@@ -395,29 +537,34 @@ __global__ void __launch_bounds__(kNlThreads) k_nlist_visit(GridDesc g, Tanks tk
     if (tid == 0 && max_union) atomicMax(&sc->max_union, max_union);
 }
 
-// ----------------------------------------------------------------- lower
-// Dynamic shared memory: float4 s_pos[ucap]; uint32 s_ent[ucap] (slot);
-// uint16 s_sorted[ucap]; then a region used first by the radix sort
-// (uint16 s_tmp[ucap], uint16 s_cnt[16 * kNlThreads]) and then by the
-// in-support masks over sorted positions (uint32 s_mask[(ucap / 32) * kChunk]).
+// ----------------------------------------------------------------- both
+// One pass per occupied cell for both lists: the union is staged once, the
+// visit masks of a chunk's fluid centres are computed once, and a fluid
+// centre's lower list is read out of its own visit mask in ascending original
+// index (through the radix-sorted fluid positions); boundary centres test the
+// sorted fluid positions directly. One reservation per chunk holds both lists
+// (visit rows first). Dynamic shared memory: float4 s_pos[ucap]; uint32
+// s_ent[ucap] (slot | flags); uint32 s_vmask[(ucap / 32) * kChunk]; uint16
+// s_sorted[ucap]; then a region used first by the radix sort and then by the
+// lower masks over sorted positions.
 template <int DIM>
-__global__ void __launch_bounds__(kNlThreads) k_nlist_lower(GridDesc g, Tanks tk, StepConst k, uint32_t ucap,
-                                                            const uint32_t* __restrict__ occ,
-                                                            const uint32_t* __restrict__ cell_start,
-                                                            StateBufs s, ListBufs l,
-                                                            DeviceScalars* sc) {
+__global__ void __launch_bounds__(kNlThreads) k_nlist_both(GridDesc g, Tanks tk, StepConst k, uint32_t ucap,
+                                                           const uint32_t* __restrict__ occ,
+                                                           const uint32_t* __restrict__ cell_start,
+                                                           StateBufs s, ListBufs l, DeviceScalars* sc) {
     constexpr int NC = DIM == 3 ? 27 : 9;
     extern __shared__ __align__(16) unsigned char smem[];
     float4* s_pos = reinterpret_cast<float4*>(smem);
     uint32_t* s_ent = reinterpret_cast<uint32_t*>(s_pos + ucap);
-    uint16_t* s_sorted = reinterpret_cast<uint16_t*>(s_ent + ucap);
-    uint32_t* s_mask = reinterpret_cast<uint32_t*>(s_sorted + ucap);
-    uint16_t* s_tmp = reinterpret_cast<uint16_t*>(s_mask);
+    uint32_t* s_vmask = s_ent + ucap;
+    uint16_t* s_sorted = reinterpret_cast<uint16_t*>(s_vmask + (ucap / 32) * kChunk);
+    uint32_t* s_lmask = reinterpret_cast<uint32_t*>(s_sorted + ucap);
+    uint16_t* s_tmp = reinterpret_cast<uint16_t*>(s_lmask);
     uint16_t* s_cnt = s_tmp + ucap;
     __shared__ uint32_t s_cstart[NC];
     __shared__ uint32_t s_off[NC + 1];
     __shared__ uint32_t s_nf, s_omin, s_omax;
-    __shared__ uint32_t s_cl[kWays][kChunk];
+    __shared__ uint32_t s_cv[kWays][kChunk], s_cl[kWays][kChunk];
     __shared__ uint32_t s_red[kWarps][2];
     __shared__ ChunkBlock s_blk;
     __shared__ bool s_overflow;
@@ -426,6 +573,7 @@ __global__ void __launch_bounds__(kNlThreads) k_nlist_lower(GridDesc g, Tanks tk
     const uint32_t nocc = sc->nocc;
     const uint32_t tid = threadIdx.x;
     const uint32_t lane = tid % kChunk, q = tid / kChunk;
+    uint32_t max_union = 0;
     if (tid == 0) s_overflow = false;
 
     for (uint32_t it = blockIdx.x; it < nocc; it += gridDim.x) {
@@ -436,13 +584,15 @@ __global__ void __launch_bounds__(kNlThreads) k_nlist_lower(GridDesc g, Tanks tk
         }
         const CellUnion cu = cell_union<DIM>(g, tk, occ[it], cell_start, s_cstart, s_off);
         const uint32_t U = cu.U;
+        max_union = max(max_union, U);
         if (U <= ucap) {
             for (uint32_t u = tid; u < U; u += blockDim.x) {
                 const uint32_t slot = slot_of_union<NC>(s_off, s_cstart, u);
                 uint8_t fl;
                 uint32_t o;
-                s_pos[u] = stage_entry<DIM>(s, slot, cu, &fl, &o);
-                s_ent[u] = slot;
+                const float4 p = stage_entry<DIM>(s, slot, cu, &fl, &o);
+                s_pos[u] = p;
+                s_ent[u] = slot | entry_flags(__float_as_uint(p.w));
                 if (!(fl & kFlagBoundary)) {
                     const uint32_t idx = atomicAdd(&s_nf, 1u);
                     s_sorted[idx] = (uint16_t)u;
@@ -451,73 +601,43 @@ __global__ void __launch_bounds__(kNlThreads) k_nlist_lower(GridDesc g, Tanks tk
                 }
             }
             __syncthreads();
-            // LSD radix sort of the fluid positions on 4-bit digits of
-            // (orig - min); keys are read through the positions. The keys are
-            // unique, so the result does not depend on the staging order.
             const uint32_t nf = s_nf;
-            {
-                const uint32_t omin = s_omin;
-                const uint32_t span = nf ? s_omax - omin : 0u;
-                const int npass = span ? (32 - __clz(span) + 3) / 4 : 0;
-                const uint32_t chunk = (nf + kNlThreads - 1) / kNlThreads;
-                const uint32_t e0 = min(nf, tid * chunk), e1 = min(nf, e0 + chunk);
-                uint16_t *src = s_sorted, *dst = s_tmp;
-                for (int pass = 0; pass < npass; ++pass) {
-                    const int shift = 4 * pass;
-#pragma unroll
-                    for (int d = 0; d < 16; ++d) s_cnt[d * kNlThreads + tid] = 0;
-                    for (uint32_t e = e0; e < e1; ++e) {
-                        const uint32_t o = __float_as_uint(s_pos[src[e]].w) & kStageOrigMask;
-                        ++s_cnt[(((o - omin) >> shift) & 15u) * kNlThreads + tid];
-                    }
-                    __syncthreads();
-                    {
-                        uint32_t v[16], sum = 0;
-#pragma unroll
-                        for (int d = 0; d < 16; ++d) {
-                            v[d] = s_cnt[tid * 16 + d];
-                            sum += v[d];
-                        }
-                        uint32_t ex, tot;
-                        block_exclusive_scan(sum, &ex, &tot);
-#pragma unroll
-                        for (int d = 0; d < 16; ++d) {
-                            s_cnt[tid * 16 + d] = (uint16_t)ex;
-                            ex += v[d];
-                        }
-                    }
-                    __syncthreads();
-                    for (uint32_t e = e0; e < e1; ++e) {
-                        const uint16_t pu = src[e];
-                        const uint32_t o = __float_as_uint(s_pos[pu].w) & kStageOrigMask;
-                        dst[s_cnt[(((o - omin) >> shift) & 15u) * kNlThreads + tid]++] = pu;
-                    }
-                    __syncthreads();
-                    uint16_t* t = src;
-                    src = dst;
-                    dst = t;
-                }
-                if (src != s_sorted) {
-                    for (uint32_t i = tid; i < nf; i += blockDim.x) s_sorted[i] = src[i];
-                }
-                __syncthreads();
-            }
+            radix_sort_by_orig(s_pos, s_sorted, s_tmp, s_cnt, nf, s_omin, s_omax);
+            const uint32_t W = (U + 31u) >> 5;
+            const uint32_t wb = W * q / kWays, we = W * (q + 1) / kWays;
             for (uint32_t c0 = 0; c0 < cu.ncenter; c0 += kChunk) {
                 const uint32_t nc = min(kChunk, cu.ncenter - c0);
                 const bool active = lane < nc;
-                uint32_t wb = 0, we = 0, R = 0;
-                // ---- pass 1: in-support masks over this quarter's sorted words
+                const uint32_t myu = cu.center_off + c0 + lane;
+                bool fluidc = false;
+                uint32_t myo = 0, R = 0;
+                float4 me = make_float4(0.f, 0.f, 0.f, 0.f);
+                // ---- pass 1a: visit masks of this quarter's union words (fluid centres)
                 if (active) {
-                    const float4 me = s_pos[cu.center_off + c0 + lane];
+                    me = s_pos[myu];
                     const uint32_t mw = __float_as_uint(me.w);
-                    const uint32_t myo = mw & kStageOrigMask;
-                    // R = fluid union entries below this particle's index (all
-                    // of them for a boundary particle)
-                    R = nf;
-                    const bool bcentre = mw & kStageBoundary;
-                    const float r2c = (bcentre && k.keep_boundary) ? __int_as_float(0x7f800000) : r2f;
-                    if (!bcentre && k.lower_boundary_only) R = 0;
-                    if (!bcentre && !k.lower_boundary_only) {
+                    fluidc = !(mw & kStageBoundary);
+                    myo = mw & kStageOrigMask;
+                    uint32_t cv = 0;
+                    if (fluidc) {
+                        for (uint32_t w = wb; w < we; ++w) {
+                            uint32_t m = 0;
+#pragma unroll
+                            for (int bit = 0; bit < 32; ++bit)
+                                m |= keep_entry(s_pos[(w << 5) + bit], me, r2f, k.keep_boundary) ? (1u << bit)
+                                                                                                 : 0u;
+                            if (w == W - 1u && (U & 31u)) m &= (1u << (U & 31u)) - 1u;
+                            if (w == (myu >> 5)) m &= ~(1u << (myu & 31u));
+                            s_vmask[w * kChunk + lane] = m;
+                            cv += __popc(m);
+                        }
+                    }
+                    s_cv[q][lane] = cv;
+                    // R = sorted fluid positions below this particle's index
+                    // (all of them for a boundary particle)
+                    if (!fluidc) {
+                        R = nf;
+                    } else if (!k.lower_boundary_only) {
                         uint32_t lo = 0, hi = nf;
                         while (lo < hi) {
                             const uint32_t mid = (lo + hi) >> 1;
@@ -527,50 +647,88 @@ __global__ void __launch_bounds__(kNlThreads) k_nlist_lower(GridDesc g, Tanks tk
                         }
                         R = lo;
                     }
-                    const uint32_t WR = (R + 31u) >> 5;
-                    wb = WR * q / kWays;
-                    we = WR * (q + 1) / kWays;
+                }
+                __syncthreads();  // every quarter's visit words are in place
+                // ---- pass 1b: lower masks of this quarter's sorted words
+                const uint32_t WR = (R + 31u) >> 5;
+                const uint32_t lb = WR * q / kWays, le = WR * (q + 1) / kWays;
+                if (active) {
+                    const float r2c = (!fluidc && k.keep_boundary) ? __int_as_float(0x7f800000) : r2f;
                     uint32_t cl = 0;
-                    for (uint32_t w = wb; w < we; ++w) {
+                    for (uint32_t w = lb; w < le; ++w) {
                         uint32_t m = 0;
+                        if (fluidc) {
+#pragma unroll 8
+                            for (int bit = 0; bit < 32; ++bit) {
+                                const uint32_t i = (w << 5) + bit;
+                                const uint32_t u = s_sorted[i < nf ? i : 0u];
+                                m |= ((s_vmask[(u >> 5) * kChunk + lane] >> (u & 31u)) & 1u) << bit;
+                            }
+                        } else {
 #pragma unroll
-                        for (int bit = 0; bit < 32; ++bit) {
-                            const uint32_t i = (w << 5) + bit;
-                            m |= within(s_pos[s_sorted[i < nf ? i : 0u]], me, r2c) ? (1u << bit) : 0u;
+                            for (int bit = 0; bit < 32; ++bit) {
+                                const uint32_t i = (w << 5) + bit;
+                                m |= within(s_pos[s_sorted[i < nf ? i : 0u]], me, r2c) ? (1u << bit) : 0u;
+                            }
                         }
                         if (w == WR - 1u && (R & 31u)) m &= (1u << (R & 31u)) - 1u;
-                        s_mask[w * kChunk + lane] = m;
+                        s_lmask[w * kChunk + lane] = m;
                         cl += __popc(m);
                     }
                     s_cl[q][lane] = cl;
                 }
                 __syncthreads();
-                // ---- list length, this quarter's offset, the chunk's block
-                uint32_t nl = 0, ol = 0;
+                // ---- list lengths, this quarter's offsets, the chunk's block
+                uint32_t nv = 0, ov = 0, nl = 0, ol = 0;
                 if (active) {
 #pragma unroll
                     for (uint32_t r = 0; r < kWays; ++r) {
-                        const uint32_t a = s_cl[r][lane];
-                        if (r < q) ol += a;
-                        nl += a;
+                        const uint32_t a = s_cv[r][lane], b = s_cl[r][lane];
+                        if (r < q) {
+                            ov += a;
+                            ol += b;
+                        }
+                        nv += a;
+                        nl += b;
                     }
                 }
-                const ChunkBlock blk = reserve_chunk(l, sc, nc, nl, 0u, s_red, &s_blk, &s_overflow);
-                // ---- pass 2: descriptor and entries
+                const ChunkBlock blk = reserve_chunk(l, sc, nc, nv, nl, s_red, &s_blk, &s_overflow);
+                // ---- pass 2: descriptors and entries
                 if (active) {
                     const uint32_t kslot = cu.cs + c0 + lane;
-                    const uint32_t gl = (uint32_t)blk.base + lane;
-                    if (q == 0) l.ldesc[kslot] = blk.ok ? make_uint2(gl, nl | (nc << 16)) : make_uint2(0u, 0u);
+                    const uint32_t gv = (uint32_t)blk.base + lane;  // < pool_groups < 2^32 when ok
+                    const uint32_t gl = (uint32_t)(blk.base + (unsigned long long)blk.rows_a * nc) + lane;
+                    if (q == 0) {
+                        l.desc[kslot] = blk.ok ? make_uint4(gv, nc, nv, 0u) : make_uint4(0u, 0u, 0u, 0u);
+                        l.ncand[kslot] = fluidc ? U : 0u;
+                        l.ldesc[kslot] = blk.ok ? make_uint2(gl, nl | (nc << 16)) : make_uint2(0u, 0u);
+                    }
                     if (blk.ok) {
                         const size_t step = 4u * nc;
+                        if (fluidc) {
+                            uint32_t* pv = l.pool + 4 * (size_t)gv;
+                            uint32_t tv = ov;
+                            for (uint32_t w = wb; w < we; ++w) {
+                                uint32_t m = s_vmask[w * kChunk + lane];
+                                while (m) {
+                                    const uint32_t u = (w << 5) + (__ffs(m) - 1);
+                                    m &= m - 1u;
+                                    uint32_t e = s_ent[u];
+                                    const uint32_t ow = __float_as_uint(s_pos[u].w);
+                                    if (!(ow & kStageBoundary) && (ow & kStageOrigMask) < myo) e |= kEntryLower;
+                                    pv[(tv >> 2) * step + (tv & 3u)] = e;
+                                    ++tv;
+                                }
+                            }
+                        }
                         uint32_t* pl = l.pool + 4 * (size_t)gl;
                         uint32_t tl = ol;
-                        for (uint32_t w = wb; w < we; ++w) {
-                            uint32_t m = s_mask[w * kChunk + lane];
+                        for (uint32_t w = lb; w < le; ++w) {
+                            uint32_t m = s_lmask[w * kChunk + lane];
                             while (m) {
                                 const uint32_t i = (w << 5) + (__ffs(m) - 1);
                                 m &= m - 1u;
-                                pl[(tl >> 2) * step + (tl & 3u)] = s_ent[s_sorted[i]];
+                                pl[(tl >> 2) * step + (tl & 3u)] = s_ent[s_sorted[i]] & kEntrySlotMask;
                                 ++tl;
                             }
                         }
@@ -579,87 +737,23 @@ __global__ void __launch_bounds__(kNlThreads) k_nlist_lower(GridDesc g, Tanks tk
                 __syncthreads();  // masks and counts are reused by the next chunk
             }
         } else {
-            // Slow path: ascending original index by repeated selection, one
-            // thread per centre particle: count, reserve, write.
-            if (tid == 0) atomicOr(&sc->status, kStatusSlowUnion);
-            for (uint32_t c0 = 0; c0 < cu.ncenter; c0 += kNlThreads) {
-                const uint32_t nc = min((uint32_t)kNlThreads, cu.ncenter - c0);
-                const bool active = tid < nc;
-                const uint32_t kslot = cu.cs + c0 + tid;
-                uint8_t mfl = 0;
-                uint32_t myo = 0;
-                float4 me = make_float4(0.f, 0.f, 0.f, 0.f);
-                bool fluidc = false;
-                uint32_t nl = 0;
-                float r2c = r2f;
-                if (active) {
-                    me = stage_entry<DIM>(s, kslot, cu, &mfl, &myo);
-                    fluidc = !(mfl & kFlagBoundary);
-                    if (!fluidc && k.keep_boundary) r2c = __int_as_float(0x7f800000);
-                    if (!(fluidc && k.lower_boundary_only)) {
-                        for (int c = 0; c < NC; ++c) {
-                            const uint32_t q0 = s_cstart[c], q1 = q0 + (s_off[c + 1] - s_off[c]);
-                            for (uint32_t slot = q0; slot < q1; ++slot) {
-                                uint8_t fl;
-                                uint32_t o;
-                                const float4 qp = stage_entry<DIM>(s, slot, cu, &fl, &o);
-                                if ((fl & kFlagBoundary) || (fluidc && o >= myo)) continue;
-                                if (within(qp, me, r2c)) ++nl;
-                            }
-                        }
-                    }
-                }
-                const ChunkBlock blk = reserve_chunk(l, sc, nc, nl, 0u, s_red, &s_blk, &s_overflow);
-                if (active) {
-                    const uint32_t gl = (uint32_t)blk.base + tid;
-                    l.ldesc[kslot] = blk.ok ? make_uint2(gl, nl | (nc << 16)) : make_uint2(0u, 0u);
-                    if (blk.ok) {
-                        const size_t step = 4u * nc;
-                        uint32_t* pl = l.pool + 4 * (size_t)gl;
-                        uint32_t tl = 0;
-                        long long last = -1;
-                        while (tl < nl) {
-                            unsigned long long best = ULLONG_MAX;
-                            uint32_t best_slot = 0;
-                            for (int c = 0; c < NC; ++c) {
-                                const uint32_t q0 = s_cstart[c], q1 = q0 + (s_off[c + 1] - s_off[c]);
-                                for (uint32_t slot = q0; slot < q1; ++slot) {
-                                    if (s.flags[slot] & kFlagBoundary) continue;
-                                    const uint32_t o = s.orig[slot];
-                                    if ((long long)o <= last || (fluidc && o >= myo) ||
-                                        (unsigned long long)o >= best)
-                                        continue;
-                                    uint8_t fl;
-                                    uint32_t oo;
-                                    if (within(stage_entry<DIM>(s, slot, cu, &fl, &oo), me, r2c)) {
-                                        best = o;
-                                        best_slot = slot;
-                                    }
-                                }
-                            }
-                            if (best == ULLONG_MAX) break;
-                            pl[(tl >> 2) * step + (tl & 3u)] = best_slot;
-                            ++tl;
-                            last = (long long)best;
-                        }
-                    }
-                }
-                __syncthreads();
-            }
+            visit_slow<DIM, true>(k, r2f, cu, U, s, l, sc, s_cstart, s_off, s_red, &s_blk, &s_overflow);
+            lower_slow<DIM>(k, r2f, cu, s, l, sc, s_cstart, s_off, s_red, &s_blk, &s_overflow);
         }
         __syncthreads();  // shared memory is reused by the next cell
     }
     if (tid == 0 && s_overflow) atomicOr(&sc->status, kStatusListOverflow);
+    if (tid == 0 && max_union) atomicMax(&sc->max_union, max_union);
+}
+
+size_t both_smem_bytes(uint32_t ucap) {
+    const size_t sort = (size_t)ucap * sizeof(uint16_t) + 16 * kNlThreads * sizeof(uint16_t);
+    const size_t mask = (size_t)(ucap / 32) * kChunk * sizeof(uint32_t);
+    return (size_t)ucap * (sizeof(float4) + sizeof(uint32_t) + sizeof(uint16_t)) + mask + (sort > mask ? sort : mask);
 }
 
 size_t visit_smem_bytes(uint32_t ucap) {
     return (size_t)ucap * (sizeof(float4) + sizeof(uint32_t)) + (size_t)(ucap / 32) * kChunk * sizeof(uint32_t);
-}
-
-size_t lower_smem_bytes(uint32_t ucap) {
-    const size_t sort = (size_t)ucap * sizeof(uint16_t) + 16 * kNlThreads * sizeof(uint16_t);
-    const size_t mask = (size_t)(ucap / 32) * kChunk * sizeof(uint32_t);
-    return (size_t)ucap * (sizeof(float4) + sizeof(uint32_t) + sizeof(uint16_t)) + (sort > mask ? sort : mask);
 }
 
 }  // namespace
@@ -675,27 +769,25 @@ uint32_t nlist_union_capacity(uint32_t max_union) {
 }
 
 size_t nlist_smem_bytes(uint32_t ucap) {
-    const size_t a = visit_smem_bytes(ucap), b = lower_smem_bytes(ucap);
+    const size_t a = visit_smem_bytes(ucap), b = both_smem_bytes(ucap);
     return a > b ? a : b;
 }
 
 uint32_t nlist_prepare(int dim, uint32_t ucap) {
-    const int sv = (int)visit_smem_bytes(ucap), sl = (int)lower_smem_bytes(ucap);
-    int bv = 0, bl = 0;
+    const int sv = (int)visit_smem_bytes(ucap), sb = (int)both_smem_bytes(ucap);
+    int bv = 0, bb = 0;
     if (dim == 3) {
-        cudaFuncSetAttribute(k_nlist_visit<3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sv);
         cudaFuncSetAttribute(k_nlist_visit<3, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sv);
-        cudaFuncSetAttribute(k_nlist_lower<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, sl);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bv, k_nlist_visit<3, true>, kNlThreads, sv);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bl, k_nlist_lower<3>, kNlThreads, sl);
+        cudaFuncSetAttribute(k_nlist_both<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bv, k_nlist_visit<3, false>, kNlThreads, sv);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bb, k_nlist_both<3>, kNlThreads, sb);
     } else {
-        cudaFuncSetAttribute(k_nlist_visit<2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sv);
         cudaFuncSetAttribute(k_nlist_visit<2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sv);
-        cudaFuncSetAttribute(k_nlist_lower<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sl);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bv, k_nlist_visit<2, true>, kNlThreads, sv);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bl, k_nlist_lower<2>, kNlThreads, sl);
+        cudaFuncSetAttribute(k_nlist_both<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bv, k_nlist_visit<2, false>, kNlThreads, sv);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bb, k_nlist_both<2>, kNlThreads, sb);
     }
-    const int b = bv > bl ? bv : bl;
+    const int b = bv > bb ? bv : bb;
     return b > 0 ? (uint32_t)b : 1u;
 }
 
@@ -703,21 +795,17 @@ void launch_nlist(const GridDesc& g, const Tanks& tk, const StepConst& k, uint32
                   uint32_t nblocks, const uint32_t* occ, const uint32_t* cell_start,
                   const StateBufs& s, const ListBufs& l, DeviceScalars* sc, cudaStream_t st,
                   bool visit_only) {
-    const size_t sv = visit_smem_bytes(ucap), sl = lower_smem_bytes(ucap);
+    const size_t sv = visit_smem_bytes(ucap), sb = both_smem_bytes(ucap);
     if (g.dim == 3) {
-        if (visit_only) {
+        if (visit_only)
             k_nlist_visit<3, false><<<nblocks, kNlThreads, sv, st>>>(g, tk, k, ucap, occ, cell_start, s, l, sc);
-        } else {
-            k_nlist_visit<3, true><<<nblocks, kNlThreads, sv, st>>>(g, tk, k, ucap, occ, cell_start, s, l, sc);
-            k_nlist_lower<3><<<nblocks, kNlThreads, sl, st>>>(g, tk, k, ucap, occ, cell_start, s, l, sc);
-        }
+        else
+            k_nlist_both<3><<<nblocks, kNlThreads, sb, st>>>(g, tk, k, ucap, occ, cell_start, s, l, sc);
     } else {
-        if (visit_only) {
+        if (visit_only)
             k_nlist_visit<2, false><<<nblocks, kNlThreads, sv, st>>>(g, tk, k, ucap, occ, cell_start, s, l, sc);
-        } else {
-            k_nlist_visit<2, true><<<nblocks, kNlThreads, sv, st>>>(g, tk, k, ucap, occ, cell_start, s, l, sc);
-            k_nlist_lower<2><<<nblocks, kNlThreads, sl, st>>>(g, tk, k, ucap, occ, cell_start, s, l, sc);
-        }
+        else
+            k_nlist_both<2><<<nblocks, kNlThreads, sb, st>>>(g, tk, k, ucap, occ, cell_start, s, l, sc);
     }
 }
 

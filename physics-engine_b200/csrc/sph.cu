@@ -179,7 +179,8 @@ template <bool INTEGRATE, int DIM>
 __global__ void __launch_bounds__(kMaxPassThreads) k_forces(uint32_t n, StepConst kc, Tanks tk,
                                                             StateBufs s, ListBufs l, double dt,
                                                             double4* __restrict__ pos_next,
-                                                            double4* __restrict__ vel_next) {
+                                                            double4* __restrict__ vel_next,
+                                                            const double4* __restrict__ st_a) {
     uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     if (s.flags[k] & kFlagBoundary) return;
@@ -213,6 +214,12 @@ __global__ void __launch_bounds__(kMaxPassThreads) k_forces(uint32_t n, StepCons
     ax += kc.gx;
     ay += kc.gy;
     az += kc.gz;
+    if (st_a) {  // wcsph.rs:273-277 a += surface-tension acceleration
+        const double4 t = st_a[k];
+        ax += t.x;
+        ay += t.y;
+        az += t.z;
+    }
     s.acc[k] = make_double4(ax, ay, az, 0.0);
     if (INTEGRATE) {
         // wcsph.rs:336-341 symplectic Euler
@@ -332,15 +339,15 @@ void launch_pressure(uint32_t n, const StepConst& k, const Tanks& tk, const Stat
 
 void launch_forces(uint32_t n, uint32_t threads, const StepConst& k, const Tanks& tk,
                    const StateBufs& s, const ListBufs& l, bool integrate, double dt,
-                   double4* pos_next, double4* vel_next, cudaStream_t st) {
+                   double4* pos_next, double4* vel_next, const double4* st_a, cudaStream_t st) {
     if (!n) return;
     const uint32_t b = blocks_for(n, threads);
     if (k.dim == 3) {
-        if (integrate) k_forces<true, 3><<<b, threads, 0, st>>>(n, k, tk, s, l, dt, pos_next, vel_next);
-        else k_forces<false, 3><<<b, threads, 0, st>>>(n, k, tk, s, l, dt, pos_next, vel_next);
+        if (integrate) k_forces<true, 3><<<b, threads, 0, st>>>(n, k, tk, s, l, dt, pos_next, vel_next, st_a);
+        else k_forces<false, 3><<<b, threads, 0, st>>>(n, k, tk, s, l, dt, pos_next, vel_next, st_a);
     } else {
-        if (integrate) k_forces<true, 2><<<b, threads, 0, st>>>(n, k, tk, s, l, dt, pos_next, vel_next);
-        else k_forces<false, 2><<<b, threads, 0, st>>>(n, k, tk, s, l, dt, pos_next, vel_next);
+        if (integrate) k_forces<true, 2><<<b, threads, 0, st>>>(n, k, tk, s, l, dt, pos_next, vel_next, st_a);
+        else k_forces<false, 2><<<b, threads, 0, st>>>(n, k, tk, s, l, dt, pos_next, vel_next, st_a);
     }
 }
 

@@ -94,6 +94,16 @@ struct StepConst {
     int lower_boundary_only;
 };
 
+// Surface-tension constants (surface_tension.rs:112-220), evaluated on the host
+// in the reference's operand order.
+struct SurfConst {
+    int model;     // 1 Akinci 2013, 2 colour field
+    double sm2;    // (sigma_eff * m) * m
+    double nsm;    // (-sigma_eff) * m
+    double coh;    // cohesion normalisation: 32 / (pi h^3) (3-D), 16 / (pi h h) (2-D)
+    double gamma;  // colour_gamma
+};
+
 struct StateBufs {
     double4* pos;
     double4* vel;
@@ -213,6 +223,8 @@ void launch_gather(uint32_t n, const uint32_t* perm, const StateBufs& src, const
 // ----- neighbour lists -----
 uint32_t nlist_union_capacity(uint32_t max_union);
 size_t nlist_smem_bytes(uint32_t ucap);
+void launch_surface_tension(uint32_t n, const StepConst& k, const SurfConst& c, const StateBufs& s,
+                            const ListBufs& l, double4* normals, double4* out, cudaStream_t st);
 // Sets the dynamic shared-memory limit of the list kernel for this stage size
 // and returns how many of its CTAs fit on one SM.
 uint32_t nlist_prepare(int dim, uint32_t ucap);
@@ -229,7 +241,7 @@ void launch_pressure(uint32_t n, const StepConst& k, const Tanks& tk, const Stat
                      cudaStream_t st);
 void launch_forces(uint32_t n, uint32_t threads, const StepConst& k, const Tanks& tk,
                    const StateBufs& s, const ListBufs& l, bool integrate, double dt,
-                   double4* pos_next, double4* vel_next, cudaStream_t st);
+                   double4* pos_next, double4* vel_next, const double4* st_a, cudaStream_t st);
 void launch_boundary_force(uint32_t n, const StepConst& k, const StateBufs& s, const ListBufs& l,
                            cudaStream_t st);
 void launch_xsph(uint32_t n, uint32_t threads, const StepConst& k, const StateBufs& s,

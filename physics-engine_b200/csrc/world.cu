@@ -192,7 +192,10 @@ World::World(const WorldParams& prm, const WorldConfig& cfg, int dim, double res
         g_.dim = dim_;
 
         f32_ = cfg_.precision == 1;
+        if (f32_ && prm_.surface_tension_sigma != 0.0)
+            throw std::invalid_argument("surface tension needs the f64 step");
         refresh_step_const();
+        configure_surface_tension();
 
         // ---- union stage capacity from the largest initial neighbour-cell union ----
         std::vector<uint32_t> cnt(g_.ncell, 0);
@@ -488,9 +491,12 @@ void World::refresh_f32() {
 }
 
 void World::set_params(const WorldParams& p) {
+    if (f32_ && p.surface_tension_sigma != 0.0)
+        throw std::invalid_argument("surface tension needs the f64 step");
     bool c_changed = p.eos_sound_speed != prm_.eos_sound_speed;
     prm_ = p;
     refresh_step_const();
+    configure_surface_tension();
     if (c_changed) set_sound_speed(p.eos_sound_speed);
 }
 
@@ -554,7 +560,7 @@ void World::ensure_lists(bool visit_only) {
             launch_nlist(g_, tanks_, kc_, ucap_, nl_blocks_, occ_, cell_start_, cur_, lists_, sc_, st_,
                          build_visit_only);
             prof_end();
-            launches_ += build_visit_only ? 1 : 2;
+            launches_ += 1;
             check(cudaGetLastError(), "neighbour lists");
             if (lists_checked_) break;
             // First build for these positions: size the pool from what the
@@ -634,9 +640,11 @@ void World::run_forces(bool integrate, double dt) {
         prof_end();
         launches_ += 2;
     } else {
+        const bool surf = prm_.surface_tension_sigma != 0.0;  // wcsph.rs:262
+        if (surf) run_surface_tension();
         prof_begin(kForces);
         launch_forces((uint32_t)n_, shape_.forces, kc_, tanks_, cur_, lists_, integrate, dt, pos_nx_,
-                      vel_nx_, st_);
+                      vel_nx_, surf ? st_a_ : nullptr, st_);
         prof_end();
         prof_begin(kBoundaryForce);
         launch_boundary_force((uint32_t)n_, kc_, cur_, lists_, st_);
@@ -644,6 +652,45 @@ void World::run_forces(bool integrate, double dt) {
         launches_ += 2;
     }
     check(cudaGetLastError(), "forces");
+}
+
+// surface_tension.rs:112-220 into st_a_ (model none: zeros, which wcsph.rs:274
+// still adds)
+void World::run_surface_tension() {
+    configure_surface_tension();
+    const uint32_t n = (uint32_t)n_;
+    if (prm_.surface_tension_model == 0) return;  // st_a_ holds zeros
+    SurfConst c{};
+    c.model = prm_.surface_tension_model;
+    const double pi = 3.14159265358979311599796346854;  // f64::consts::PI
+    const double sigma_eff = prm_.surface_tension_sigma * (dim_ == 2 ? 1.0 / 20.0 : 1.0);
+    c.sm2 = sigma_eff * mass_ * mass_;
+    c.nsm = -sigma_eff * mass_;
+    c.coh = dim_ == 2 ? 16.0 / (pi * h_ * h_) : 32.0 / (pi * pow_int_dd(h_, 3));
+    c.gamma = prm_.surface_tension_colour_gamma;
+    launch_surface_tension(n, kc_, c, cur_, lists_, st_normals_, st_a_, st_);
+    launches_ += 2;
+    check(cudaGetLastError(), "surface tension");
+}
+
+// Buffers and list mode of the surface-tension branch: the Akinci curvature
+// term sums over every fluid candidate of the neighbour cells, so that model
+// needs lists holding all of them.
+void World::configure_surface_tension() {
+    const bool on = prm_.surface_tension_sigma != 0.0;
+    if (on && !st_a_) {
+        const size_t N = std::max<uint64_t>(n_, 1);
+        st_normals_ = alloc<double4>(N);
+        st_a_ = alloc<double4>(N);  // zeroed
+    }
+    const bool all = on && prm_.surface_tension_model == 1;
+    if (all != list_all_candidates_) {
+        list_all_candidates_ = all;
+        refresh_step_const();
+        lists_valid_ = false;
+        lists_checked_ = false;
+        invalidate_graph();
+    }
 }
 
 void World::run_xsph() {
@@ -864,7 +911,8 @@ World::Shapes World::autotune() {
     });
     pick(shape_.forces, [&] {
         if (f32_) launch_forces_f32(n, shape_.forces, kf_, tanks_, cur_, fb_, lists_, 0.f, pos_nx_, vel_nx_, nullptr, st_);
-        else launch_forces(n, shape_.forces, kc_, tanks_, cur_, lists_, true, 0.0, pos_nx_, vel_nx_, st_);
+        else launch_forces(n, shape_.forces, kc_, tanks_, cur_, lists_, true, 0.0, pos_nx_, vel_nx_,
+                           prm_.surface_tension_sigma != 0.0 ? st_a_ : nullptr, st_);
     });
     if (!f32_ && prm_.xsph_epsilon != 0.0)
         pick(shape_.xsph, [&] { launch_xsph(n, shape_.xsph, kc_, cur_, lists_, vel_nx_, st_); });

@@ -23,6 +23,8 @@ struct WorldParams {
     double gravity[3];
     int adapt_sound_speed;
     double surface_tension_sigma;
+    int surface_tension_model;  // 0 none, 1 Akinci 2013, 2 colour field
+    double surface_tension_colour_gamma;
 };
 
 struct WorldConfig {
@@ -80,6 +82,7 @@ class World {
     double mass() const { return mass_; }
     double rest_density() const { return rho0_; }
     double smoothing_length() const { return h_; }
+    bool single_precision() const { return f32_; }
 
     // Host-buffer access in original particle order.
     void get_vec(int which, double* out);         // 0 x, 1 v, 2 a, 3 boundary force
@@ -160,6 +163,10 @@ class World {
     void run_pressure();
     void run_forces(bool integrate, double dt);
     void run_xsph();
+    void run_surface_tension();
+    void configure_surface_tension();
+    double4* st_normals_ = nullptr;  // colour-field normals (surface tension)
+    double4* st_a_ = nullptr;        // surface-tension accelerations
     void refresh_step_const();
     void refresh_f32();
     void configure_lists();

@@ -38,6 +38,7 @@ STATUS_DOMAIN, STATUS_NEIGHBOUR_OVERFLOW, STATUS_NONFINITE, STATUS_SLOW_UNION = 
 FLUID, BOUNDARY = 0, 1
 CUBIC_SPLINE, WENDLAND_C2, POLY6, SPIKY = 0, 1, 2, 3
 DIM_2, DIM_3 = 2, 3
+SURFACE_TENSION_NONE, SURFACE_TENSION_AKINCI, SURFACE_TENSION_COLOUR_FIELD = 0, 1, 2
 STANDARD_GRAVITY = 9.80665  # pe-math units.rs:7
 
 _ERRNAMES = {1: "PE_ERR_NULL", 2: "PE_ERR_BOUNDS", 3: "PE_ERR_ARG", 4: "PE_ERR_PANIC",
@@ -72,6 +73,8 @@ class _Params(C.Structure):
         ("gravity", C.c_double * 3),
         ("adapt_sound_speed", C.c_int32),
         ("surface_tension_sigma", C.c_double),
+        ("surface_tension_model", C.c_int32),
+        ("surface_tension_colour_gamma", C.c_double),
     ]
 
 
@@ -407,7 +410,7 @@ class WcsphParams:
 
     _FIELDS = ("density_kernel", "eos_rest_density", "eos_sound_speed", "eos_gamma", "visc_alpha",
                "visc_beta", "visc_eps", "xsph_epsilon", "gravity", "adapt_sound_speed",
-               "surface_tension_sigma")
+               "surface_tension_sigma", "surface_tension_model", "surface_tension_colour_gamma")
 
     def __init__(self, **kw):
         self.density_kernel = CUBIC_SPLINE
@@ -419,6 +422,8 @@ class WcsphParams:
         self.gravity = (0.0, 0.0, -STANDARD_GRAVITY)
         self.adapt_sound_speed = True
         self.surface_tension_sigma = 0.0
+        self.surface_tension_model = SURFACE_TENSION_NONE
+        self.surface_tension_colour_gamma = 0.0
         for k, v in kw.items():
             if k not in self._FIELDS:
                 raise TypeError(f"unknown WcsphParams field {k!r}")
@@ -442,6 +447,8 @@ class WcsphParams:
         c.gravity[:] = [float(g) for g in self.gravity]
         c.adapt_sound_speed = 1 if self.adapt_sound_speed else 0
         c.surface_tension_sigma = float(self.surface_tension_sigma)
+        c.surface_tension_model = int(self.surface_tension_model)
+        c.surface_tension_colour_gamma = float(self.surface_tension_colour_gamma)
         return c
 
     @classmethod
@@ -450,7 +457,8 @@ class WcsphParams:
                    eos_sound_speed=c.eos_sound_speed, eos_gamma=c.eos_gamma, visc_alpha=c.visc_alpha,
                    visc_beta=c.visc_beta, visc_eps=c.visc_eps, xsph_epsilon=c.xsph_epsilon,
                    gravity=tuple(c.gravity), adapt_sound_speed=bool(c.adapt_sound_speed),
-                   surface_tension_sigma=c.surface_tension_sigma)
+                   surface_tension_sigma=c.surface_tension_sigma, surface_tension_model=c.surface_tension_model,
+                   surface_tension_colour_gamma=c.surface_tension_colour_gamma)
 
     def __repr__(self):
         return "WcsphParams(" + ", ".join(f"{k}={getattr(self, k)!r}" for k in self._FIELDS) + ")"

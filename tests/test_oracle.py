@@ -238,3 +238,27 @@ def test_neigh_list_materialisation_does_not_change_results(materialize):
     w0 = O.World(s0, O.dam_break_params(materialize=False))
     w0.run(1e-4, 3)
     assert w.hash64() == w0.hash64()
+
+
+def test_surface_tension_conserves_momentum():
+    """surface_tension.rs:152-184: the Akinci cohesion and curvature terms are
+    antisymmetric over the (symmetric) cell-grid neighbour relation, so the
+    surface-tension accelerations of equal masses sum to zero up to rounding."""
+    s0 = O.Scene(3, 1000.0, 1e-3, 0.02)
+    s0.fill_box((0.01, 0.01, 0.01), 8, 7, 6, 0.01)
+    s0.jitter_fluid(3, 1e-4)
+
+    def accel(model):
+        p = O.water_params(1000.0, 20.0, (0.0, 0.0, 0.0), materialize=False)
+        p.st_model, p.st_sigma, p.st_colour_gamma = model, 0.5, 0.5
+        w = O.World(s0, p)
+        w.rebuild_grid()
+        w.compute_density()
+        w.compute_pressure()
+        w.compute_forces()
+        return w.a()
+
+    d = accel(1) - accel(0)
+    scale = np.abs(d).max()
+    assert scale > 0.0
+    assert np.abs(d.sum(axis=0)).max() < 1e-9 * scale * len(d)
