@@ -31,6 +31,7 @@ namespace pe {
 namespace {
 
 constexpr int kThreads = 128;
+constexpr uint32_t kCompact = 32;  // visit entries compacted per chunk in the force pass
 
 inline uint32_t blocks_for(uint64_t n, uint32_t t) { return (uint32_t)((n + t - 1) / t); }
 
@@ -202,15 +203,41 @@ __global__ void __launch_bounds__(kMaxPassThreads) k_forces(uint32_t n, StepCons
         fluid_pair(kc, nac, xk, vk, d.x, d.v, ax, ay, az);
     });
     // fluid j > k and boundary j, visiting order: the visit list without the
-    // entries flagged lower (those came from the lower list, in index order)
-    for_each_loaded(list_ref(l, k, kListVisit), load, [&](uint32_t e, const PosVel& d) {
-        if (e & kEntryLower) return;
-        if (e & kEntryBoundary) {
-            boundary_pair(kc, xk, d.x, (e & kEntryOriented) != 0u, s.nout, e & kEntrySlotMask, ax, ay, az);
-        } else {
-            fluid_pair(kc, nac, xk, vk, d.x, d.v, ax, ay, az);
+    // entries flagged lower (those came from the lower list, in index order).
+    // The list is taken in chunks of kCompact entries whose kept entries are
+    // first compacted into this thread's column of shared memory, so the pair
+    // loop of a warp runs over kept entries only (the flagged ones are about
+    // half and fall at different positions in each thread's list).
+    extern __shared__ uint32_t s_keep[];  // kCompact x blockDim.x, column per thread
+    const uint32_t tid = threadIdx.x, bd = blockDim.x;
+    const ListRef vr = list_ref(l, k, kListVisit);
+    for (uint32_t t0 = 0; t0 < vr.n; t0 += kCompact) {
+        const uint32_t t1 = min(vr.n, t0 + kCompact);
+        uint32_t c = 0;
+        for (uint32_t t = t0; t < t1; t += 4) {
+            const uint4 g4 = __ldg(reinterpret_cast<const uint4*>(vr.p + (size_t)(t >> 2) * vr.step));
+            const uint32_t ge[4] = {g4.x, g4.y, g4.z, g4.w};
+#pragma unroll
+            for (uint32_t q = 0; q < 4; ++q)
+                if (t + q < t1 && !(ge[q] & kEntryLower)) s_keep[(c++) * bd + tid] = ge[q];
         }
-    });
+        if (c == 0) continue;
+        uint32_t e = s_keep[tid];
+        PosVel d = load(e);
+        for (uint32_t u = 0; u < c; ++u) {
+            const uint32_t ec = e;
+            const PosVel dc = d;
+            if (u + 1 < c) {
+                e = s_keep[(u + 1) * bd + tid];
+                d = load(e);
+            }
+            if (ec & kEntryBoundary) {
+                boundary_pair(kc, xk, dc.x, (ec & kEntryOriented) != 0u, s.nout, ec & kEntrySlotMask, ax, ay, az);
+            } else {
+                fluid_pair(kc, nac, xk, vk, dc.x, dc.v, ax, ay, az);
+            }
+        }
+    }
     ax += kc.gx;
     ay += kc.gy;
     az += kc.gz;
@@ -342,12 +369,13 @@ void launch_forces(uint32_t n, uint32_t threads, const StepConst& k, const Tanks
                    double4* pos_next, double4* vel_next, const double4* st_a, cudaStream_t st) {
     if (!n) return;
     const uint32_t b = blocks_for(n, threads);
+    const size_t sm = (size_t)kCompact * threads * sizeof(uint32_t);
     if (k.dim == 3) {
-        if (integrate) k_forces<true, 3><<<b, threads, 0, st>>>(n, k, tk, s, l, dt, pos_next, vel_next, st_a);
-        else k_forces<false, 3><<<b, threads, 0, st>>>(n, k, tk, s, l, dt, pos_next, vel_next, st_a);
+        if (integrate) k_forces<true, 3><<<b, threads, sm, st>>>(n, k, tk, s, l, dt, pos_next, vel_next, st_a);
+        else k_forces<false, 3><<<b, threads, sm, st>>>(n, k, tk, s, l, dt, pos_next, vel_next, st_a);
     } else {
-        if (integrate) k_forces<true, 2><<<b, threads, 0, st>>>(n, k, tk, s, l, dt, pos_next, vel_next, st_a);
-        else k_forces<false, 2><<<b, threads, 0, st>>>(n, k, tk, s, l, dt, pos_next, vel_next, st_a);
+        if (integrate) k_forces<true, 2><<<b, threads, sm, st>>>(n, k, tk, s, l, dt, pos_next, vel_next, st_a);
+        else k_forces<false, 2><<<b, threads, sm, st>>>(n, k, tk, s, l, dt, pos_next, vel_next, st_a);
     }
 }
 
