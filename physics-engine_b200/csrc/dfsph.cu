@@ -57,6 +57,14 @@ __device__ __forceinline__ bool sees(const DfsphConst& k, const double4& xb, con
     return d > -eps;
 }
 
+// A candidate beyond the kernel's support adds an exact +-0 to the gradient
+// and kernel sums (W and grad W vanish there); those sums skip it. The margin
+// on far2 keeps the test conservative under rounding.
+__device__ __forceinline__ bool far_pair(const DfsphConst& k, const double4& xi, const double4& xj) {
+    const double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
+    return dx * dx + dy * dy + dz * dz > k.far2;
+}
+
 // dfsph.rs:309-323 neighbour_mass_for
 __device__ __forceinline__ double nmass(const DfsphConst& k, const StateBufs& s, uint32_t e, const double4& xj,
                                         const double4& xi) {
@@ -105,7 +113,9 @@ __global__ void __launch_bounds__(kDfThreads) k_df_xsph(uint32_t n, DfsphConst k
     for_each_entry(list_ref(l, i, kListVisit), [&](uint32_t e) {
         if (e & kEntryBoundary) return;
         const uint32_t j = e & kEntrySlotMask;
-        const double4 xj = s.pos[j], vj = s.acc[j];
+        const double4 xj = s.pos[j];
+        if (far_pair(k, xi, xj)) return;
+        const double4 vj = s.acc[j];
         const double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
         const double wij = kfn_w(k.kf, sqrt(dx * dx + dy * dy + dz * dz));
         const double rho_bar = 0.5 * (rho_i + s.vel[j].w);
@@ -129,10 +139,13 @@ __global__ void k_df_xsph_apply(uint32_t n, StateBufs s, const double4* __restri
 }
 
 // kappa = the warm-start accumulator (which 0: density, acc.w; 1: divergence, nout.w)
-__global__ void k_df_warm_load(uint32_t n, int which, StateBufs s, double* __restrict__ kappa) {
+__global__ void k_df_warm_load(uint32_t n, DfsphConst k, int which, StateBufs s, double* __restrict__ kappa,
+                               double* __restrict__ kr) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    kappa[i] = which ? s.nout[i].w : s.acc[i].w;
+    const double kap = which ? s.nout[i].w : s.acc[i].w;
+    kappa[i] = kap;
+    kr[i] = is_boundary(s, i) ? 0.0 / k.rho0 : kap / fmax(s.vel[i].w, 1e-12);
 }
 
 __global__ void k_df_warm_zero(uint32_t n, int which, StateBufs s) {
@@ -150,6 +163,7 @@ __device__ __forceinline__ double density_rate(const DfsphConst& k, const StateB
     for_each_loaded(
         list_ref(l, i, kListVisit), [&](uint32_t e) { return s.pos[e & kEntrySlotMask]; },
         [&](uint32_t e, const double4& xj) {
+            if (far_pair(k, xi, xj)) return;
             const double mj = nmass(k, s, e, xj, xi);
             if (mj == 0.0) return;
             const uint32_t j = e & kEntrySlotMask;
@@ -168,12 +182,13 @@ __device__ __forceinline__ double density_rate(const DfsphConst& k, const StateB
 __global__ void __launch_bounds__(kDfThreads) k_df_error(uint32_t n, DfsphConst k, int divergence, double dt,
                                                         double dt2, StateBufs s, ListBufs l,
                                                         const double* __restrict__ alpha, double* __restrict__ kappa,
-                                                        double* __restrict__ err_orig) {
+                                                        double* __restrict__ kr, double* __restrict__ err_orig) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const uint32_t o = s.orig[i];
     if (is_boundary(s, i)) {
         kappa[i] = 0.0;
+        kr[i] = 0.0 / k.rho0;  // dfsph.rs:462-469: kj = 0, rho_j = rho0
         err_orig[o] = 0.0;
         return;
     }
@@ -193,6 +208,9 @@ __global__ void __launch_bounds__(kDfThreads) k_df_error(uint32_t n, DfsphConst 
         if (k.warm_start) s.nout[i].w = s.nout[i].w + kap;
     }
     kappa[i] = kap;
+    // dfsph.rs:436, 470: kappa / max(rho, 1e-12), the same quotient the
+    // reference forms for every pair, formed once
+    kr[i] = kap / fmax(s.vel[i].w, 1e-12);
     err_orig[o] = e;
 }
 
@@ -237,28 +255,26 @@ __global__ void k_df_serial_sum(uint32_t n, const double* __restrict__ v, double
 // weight sum, v* += dv.
 __global__ void __launch_bounds__(kDfThreads) k_df_pressure_fluid(uint32_t n, DfsphConst k, double dt,
                                                                  double inv_dt, StateBufs s, ListBufs l,
-                                                                 const double* __restrict__ kappa,
+                                                                 const double* __restrict__ kr,
                                                                  double4* __restrict__ react) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     if (is_boundary(s, i)) return;
     const double4 xi = s.pos[i];
-    const double rho_i = fmax(s.vel[i].w, 1e-12);
-    const double ki = kappa[i];
+    const double kri = kr[i];  // ki / rho_i
     double dx = 0.0, dy = 0.0, dz = 0.0, bx = 0.0, by = 0.0, bz = 0.0;
     const ListRef lr = list_ref(l, i, kListVisit);
     for_each_loaded(
         lr, [&](uint32_t e) { return s.pos[e & kEntrySlotMask]; },
         [&](uint32_t e, const double4& xj) {
+            if (far_pair(k, xi, xj)) return;
             const double mj = nmass(k, s, e, xj, xi);
             if (mj == 0.0) return;
             const uint32_t j = e & kEntrySlotMask;
             double gx, gy, gz;
             kfn_grad(k.kf, xj.x - xi.x, xj.y - xi.y, xj.z - xi.z, &gx, &gy, &gz);
             const bool bnd = e & kEntryBoundary;
-            const double kj = bnd ? 0.0 : kappa[j];
-            const double rho_j = bnd ? k.rho0 : fmax(s.vel[j].w, 1e-12);
-            const double coeff = mj * (ki / rho_i + kj / rho_j);
+            const double coeff = mj * (kri + kr[j]);  // mj (ki / rho_i + kj / rho_j)
             const double tx = gx * coeff, ty = gy * coeff, tz = gz * coeff;
             dx = dx + tx;
             dy = dy + ty;
@@ -391,6 +407,7 @@ __global__ void __launch_bounds__(kDfThreads) k_df_density(uint32_t n, DfsphCons
     for_each_loaded(
         list_ref(l, i, kListVisit), [&](uint32_t e) { return s.pos[e & kEntrySlotMask]; },
         [&](uint32_t e, const double4& xj) {
+            if (far_pair(k, xi, xj)) return;
             const double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
             const double wij = kfn_w(k.kf, sqrt(dx * dx + dy * dy + dz * dz));
             if (!(e & kEntryBoundary)) {
@@ -426,6 +443,7 @@ __global__ void __launch_bounds__(kDfThreads) k_df_alpha(uint32_t n, DfsphConst 
                 if (mj == 0.0) return;
                 ++nb_kept;
             }
+            if (far_pair(k, xi, xj)) return;
             double gx, gy, gz;
             kfn_grad(k.kf, xj.x - xi.x, xj.y - xi.y, xj.z - xi.z, &gx, &gy, &gz);
             const double ax = gx * mj, ay = gy * mj, az = gz * mj;
@@ -496,6 +514,7 @@ DfsphSolver::DfsphSolver(const DfsphParams& prm, const WorldConfig& cfg, int dim
     const size_t N = std::max<uint64_t>(n, 1);
     alpha_ = w_->alloc<double>(N);
     kappa_ = w_->alloc<double>(N);
+    kr_ = w_->alloc<double>(N);
     dv_ = w_->alloc<double4>(N);
     react_ = w_->alloc<double4>(N);
     err_orig_ = w_->alloc<double>(N);
@@ -610,6 +629,10 @@ void DfsphSolver::refresh_const() {
     k.omega = prm_.solver_omega;
     k.dv_cap = prm_.max_velocity_correction;
     k.warm_start = prm_.warm_start;
+    {
+        const double far = kernel_support(prm_.kernel, w.h_) * (1.0 + 1e-9);
+        k.far2 = far * far;
+    }
     for (int a = 0; a < 4; ++a) {
         k.has_slip[a] = prm_.has_slip[a];
         k.slip[a] = prm_.slip[a];
@@ -637,7 +660,7 @@ void DfsphSolver::pressure_update(double dt, bool /*divergence*/) {
     const uint32_t n = (uint32_t)w.n_;
     const uint32_t nb = blocks_for(n, kDfThreads);
     const double inv_dt = 1.0 / std::fmax(dt, 1e-12);
-    k_df_pressure_fluid<<<nb, kDfThreads, 0, w.st_>>>(n, kc_, dt, inv_dt, w.cur_, w.lists_, kappa_, react_);
+    k_df_pressure_fluid<<<nb, kDfThreads, 0, w.st_>>>(n, kc_, dt, inv_dt, w.cur_, w.lists_, kr_, react_);
     k_df_pressure_boundary<<<nb, kDfThreads, 0, w.st_>>>(n, kc_, w.cur_, w.lists_, react_);
     w.launches_ += 2;
 }
@@ -647,7 +670,7 @@ double DfsphSolver::solve_error(double dt, bool divergence) {
     const uint32_t n = (uint32_t)w.n_;
     const uint32_t nb = blocks_for(n, kDfThreads);
     k_df_error<<<nb, kDfThreads, 0, w.st_>>>(n, kc_, divergence ? 1 : 0, dt, dt * dt, w.cur_, w.lists_, alpha_,
-                                             kappa_, err_orig_);
+                                             kappa_, kr_, err_orig_);
     k_df_partial_sums<<<kSumBlocks, kSumThreads, 0, w.st_>>>(n, err_orig_, part_);
     k_df_final_sum<<<1, kSumThreads, 0, w.st_>>>(part_, sum_);
     w.launches_ += 3;
@@ -683,7 +706,7 @@ uint64_t DfsphSolver::correct_density_error(double dt) {
     const uint32_t n = (uint32_t)w.n_;
     const uint32_t nb = blocks_for(n, kDfThreads);
     if (prm_.warm_start) {
-        k_df_warm_load<<<nb, kDfThreads, 0, w.st_>>>(n, 0, w.cur_, kappa_);
+        k_df_warm_load<<<nb, kDfThreads, 0, w.st_>>>(n, kc_, 0, w.cur_, kappa_, kr_);
         w.launches_ += 1;
         pressure_update(dt, false);
     }
@@ -704,7 +727,7 @@ uint64_t DfsphSolver::correct_divergence_error(double dt) {
     const uint32_t n = (uint32_t)w.n_;
     const uint32_t nb = blocks_for(n, kDfThreads);
     if (prm_.warm_start) {
-        k_df_warm_load<<<nb, kDfThreads, 0, w.st_>>>(n, 1, w.cur_, kappa_);
+        k_df_warm_load<<<nb, kDfThreads, 0, w.st_>>>(n, kc_, 1, w.cur_, kappa_, kr_);
         w.launches_ += 1;
         pressure_update(dt, true);
     }

@@ -38,6 +38,7 @@ struct DfsphConst {
     int warm_start;
     int has_slip[4];
     double slip[4];
+    double far2;  // squared distance beyond the kernel's support (with a margin)
 };
 
 class DfsphSolver {
@@ -93,6 +94,7 @@ class DfsphSolver {
     // per slot (valid until the next re-sort)
     double* alpha_ = nullptr;
     double* kappa_ = nullptr;
+    double* kr_ = nullptr;           // kappa / max(rho, 1e-12) (boundary: 0 / rho0)
     double4* dv_ = nullptr;          // xsph scratch
     double4* react_ = nullptr;       // (F_b total, wsum) of a fluid particle's reaction
     // per original index: a solver pass's error terms, summed in index order

@@ -30,6 +30,14 @@ __device__ __forceinline__ double4 load_pos(const StateBufs& s, uint32_t e) {
     return s.pos[e & kEntrySlotMask];
 }
 
+// A candidate beyond both kernels' support contributes an exact +-0 to every
+// sum (W and grad W vanish there), which leaves the sums unchanged: it is
+// skipped. The margin on far2 keeps the test conservative under rounding.
+__device__ __forceinline__ bool far_pair(const PbfConst& k, const double4& xi, const double4& xj) {
+    const double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
+    return dx * dx + dy * dy + dz * dz > k.far2;
+}
+
 // pbf.rs:387-399: fluid v += g dt, pred = x + v dt (2-D: z = 0); the start
 // position goes to acc, the prediction to pred (the grid build's next positions).
 __global__ void k_pbf_predict(uint32_t n, PbfConst k, double dt, StateBufs s, double4* __restrict__ pred) {
@@ -66,6 +74,7 @@ __global__ void __launch_bounds__(kPbfThreads) k_pbf_density(uint32_t n, PbfCons
     for_each_loaded(
         list_ref(l, i, kListVisit), [&](uint32_t e) { return load_pos(s, e); },
         [&](uint32_t e, const double4& xj) {
+            if (far_pair(k, xi, xj)) return;
             const double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
             const double r = sqrt(dx * dx + dy * dy + dz * dz);
             const double wij = kfn_w(k.dk, r);
@@ -93,6 +102,7 @@ __global__ void __launch_bounds__(kPbfThreads) k_pbf_lambda(uint32_t n, PbfConst
     for_each_loaded(
         list_ref(l, i, kListVisit), [&](uint32_t e) { return load_pos(s, e); },
         [&](uint32_t e, const double4& xj) {
+            if (far_pair(k, xi, xj)) return;
             double wx, wy, wz;
             kfn_grad(k.gk, xj.x - xi.x, xj.y - xi.y, xj.z - xi.z, &wx, &wy, &wz);
             const bool fluid = !(e & kEntryBoundary);
@@ -133,6 +143,7 @@ __global__ void __launch_bounds__(kPbfThreads) k_pbf_delta_p(uint32_t n, PbfCons
     for_each_loaded(
         list_ref(l, i, kListVisit), [&](uint32_t e) { return load_pos(s, e); },
         [&](uint32_t e, const double4& xj) {
+            if (far_pair(k, xi, xj)) return;
             const double rx = xj.x - xi.x, ry = xj.y - xi.y, rz = xj.z - xi.z;
             const double r = sqrt(rx * rx + ry * ry + rz * rz);
             const double wij = kfn_w(k.dk, r);
@@ -200,7 +211,9 @@ __global__ void __launch_bounds__(kPbfThreads) k_pbf_viscosity(uint32_t n, PbfCo
     for_each_entry(list_ref(l, i, kListVisit), [&](uint32_t e) {
         if (e & kEntryBoundary) return;
         const uint32_t j = e & kEntrySlotMask;
-        const double4 xj = s.pos[j], vj = s.vel[j];
+        const double4 xj = s.pos[j];
+        if (far_pair(k, xi, xj)) return;
+        const double4 vj = s.vel[j];
         const double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
         const double r = sqrt(dx * dx + dy * dy + dz * dz);
         const double wij = kfn_w(k.dk, r);
@@ -244,7 +257,9 @@ __global__ void __launch_bounds__(kPbfThreads) k_pbf_omega(uint32_t n, PbfConst 
     for_each_entry(list_ref(l, i, kListVisit), [&](uint32_t e) {
         if (e & kEntryBoundary) return;
         const uint32_t j = e & kEntrySlotMask;
-        const double4 xj = s.pos[j], vj = s.vel[j];
+        const double4 xj = s.pos[j];
+        if (far_pair(k, xi, xj)) return;
+        const double4 vj = s.vel[j];
         D3 g;
         kfn_grad(k.gk, xj.x - xi.x, xj.y - xi.y, xj.z - xi.z, &g.x, &g.y, &g.z);
         const double rho_bar = 0.5 * (vi.w + vj.w);
@@ -268,7 +283,9 @@ __global__ void __launch_bounds__(kPbfThreads) k_pbf_confine(uint32_t n, PbfCons
     for_each_entry(list_ref(l, i, kListVisit), [&](uint32_t e) {
         if (e & kEntryBoundary) return;
         const uint32_t j = e & kEntrySlotMask;
-        const double4 xj = s.pos[j], oj = omega[j];
+        const double4 xj = s.pos[j];
+        if (far_pair(k, xi, xj)) return;
+        const double4 oj = omega[j];
         D3 g;
         kfn_grad(k.gk, xj.x - xi.x, xj.y - xi.y, xj.z - xi.z, &g.x, &g.y, &g.z);
         const double rho_bar = 0.5 * (rho_i + s.vel[j].w);
@@ -399,6 +416,11 @@ void PbfSolver::refresh_const() {
         k.w_dq = wd;
     }
     k.max_corr = 0.4 * w.h_;
+    {
+        const double sup = std::fmax(kernel_support(prm_.density_kernel, w.h_), kernel_support(prm_.grad_kernel, w.h_));
+        const double far = sup * (1.0 + 1e-9);
+        k.far2 = far * far;
+    }
     k.visc_eps = prm_.viscosity_eps;
     k.vort_eps = prm_.vorticity_eps;
     k.gx = prm_.gravity[0];

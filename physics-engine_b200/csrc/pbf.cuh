@@ -33,6 +33,7 @@ struct PbfConst {
     double max_corr;           // 0.4 h
     double visc_eps, vort_eps;
     double gx, gy, gz;
+    double far2;  // squared distance beyond both kernels' support (with a margin)
 };
 
 class PbfSolver {
