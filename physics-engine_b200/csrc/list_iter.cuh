@@ -44,4 +44,39 @@ __device__ __forceinline__ void for_each_loaded(const ListRef r, Load&& load, F&
     }
 }
 
+// Entries a chunk compacts at most (see for_each_kept).
+constexpr uint32_t kKeepChunk = 32;
+
+// Calls f(entry, data) in list order over the entries keep(entry, data)
+// accepts, data = load(entry). The list is taken in chunks of kKeepChunk; each
+// chunk's accepted entries are first compacted into this thread's column of
+// buf (kKeepChunk rows of blockDim.x entries, shared memory), so a warp runs
+// its f loop over accepted entries only instead of idling on the rejected ones
+// at each lane's own positions.
+template <class Load, class Keep, class F>
+__device__ __forceinline__ void for_each_kept(const ListRef r, uint32_t* buf, Load&& load, Keep&& keep, F&& f) {
+    const uint32_t n = r.n, tid = threadIdx.x, bd = blockDim.x;
+    auto at = [&](uint32_t t) { return __ldg(r.p + (size_t)(t >> 2) * r.step + (t & 3u)); };
+    for (uint32_t t0 = 0; t0 < n; t0 += kKeepChunk) {
+        const uint32_t t1 = min(n, t0 + kKeepChunk);
+        uint32_t c = 0;
+        for (uint32_t t = t0; t < t1; ++t) {
+            const uint32_t e = at(t);
+            if (keep(e, load(e))) buf[(c++) * bd + tid] = e;
+        }
+        if (c == 0) continue;
+        uint32_t e = buf[tid];
+        auto d = load(e);
+        for (uint32_t u = 0; u < c; ++u) {
+            const uint32_t ec = e;
+            const auto dc = d;
+            if (u + 1 < c) {
+                e = buf[(u + 1) * bd + tid];
+                d = load(e);
+            }
+            f(ec, dc);
+        }
+    }
+}
+
 }  // namespace pe

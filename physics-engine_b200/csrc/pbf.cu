@@ -19,6 +19,7 @@ namespace pe {
 namespace {
 
 constexpr uint32_t kPbfThreads = 128;
+constexpr size_t kKeepBytes = (size_t)kKeepChunk * kPbfThreads * sizeof(uint32_t);  // for_each_kept buffer
 
 inline uint32_t blocks_for(uint64_t n, uint32_t t) { return (uint32_t)((n + t - 1) / t); }
 
@@ -69,12 +70,13 @@ __global__ void __launch_bounds__(kPbfThreads) k_pbf_density(uint32_t n, PbfCons
         s.vel[i].w = k.rho0;
         return;
     }
+    extern __shared__ uint32_t s_keep[];
     const double4 xi = s.pos[i];
     double rho = k.rho_self;
-    for_each_loaded(
-        list_ref(l, i, kListVisit), [&](uint32_t e) { return load_pos(s, e); },
+    for_each_kept(
+        list_ref(l, i, kListVisit), s_keep, [&](uint32_t e) { return load_pos(s, e); },
+        [&](uint32_t, const double4& xj) { return !far_pair(k, xi, xj); },
         [&](uint32_t e, const double4& xj) {
-            if (far_pair(k, xi, xj)) return;
             const double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
             const double r = sqrt(dx * dx + dy * dy + dz * dz);
             const double wij = kfn_w(k.dk, r);
@@ -99,10 +101,11 @@ __global__ void __launch_bounds__(kPbfThreads) k_pbf_lambda(uint32_t n, PbfConst
     const double ci = s.vel[i].w / k.rho0 - 1.0;
     double sum_grad_sq = 0.0;
     double gx = 0.0, gy = 0.0, gz = 0.0;
-    for_each_loaded(
-        list_ref(l, i, kListVisit), [&](uint32_t e) { return load_pos(s, e); },
+    extern __shared__ uint32_t s_keep[];
+    for_each_kept(
+        list_ref(l, i, kListVisit), s_keep, [&](uint32_t e) { return load_pos(s, e); },
+        [&](uint32_t, const double4& xj) { return !far_pair(k, xi, xj); },
         [&](uint32_t e, const double4& xj) {
-            if (far_pair(k, xi, xj)) return;
             double wx, wy, wz;
             kfn_grad(k.gk, xj.x - xi.x, xj.y - xi.y, xj.z - xi.z, &wx, &wy, &wz);
             const bool fluid = !(e & kEntryBoundary);
@@ -140,10 +143,11 @@ __global__ void __launch_bounds__(kPbfThreads) k_pbf_delta_p(uint32_t n, PbfCons
     const double4 xi = s.pos[i];
     const double li = lambda[i];
     double cx = 0.0, cy = 0.0, cz = 0.0;
-    for_each_loaded(
-        list_ref(l, i, kListVisit), [&](uint32_t e) { return load_pos(s, e); },
+    extern __shared__ uint32_t s_keep[];
+    for_each_kept(
+        list_ref(l, i, kListVisit), s_keep, [&](uint32_t e) { return load_pos(s, e); },
+        [&](uint32_t, const double4& xj) { return !far_pair(k, xi, xj); },
         [&](uint32_t e, const double4& xj) {
-            if (far_pair(k, xi, xj)) return;
             const double rx = xj.x - xi.x, ry = xj.y - xi.y, rz = xj.z - xi.z;
             const double r = sqrt(rx * rx + ry * ry + rz * rz);
             const double wij = kfn_w(k.dk, r);
@@ -459,9 +463,9 @@ void PbfSolver::step(double dt) {
     lists(reused);
     // pbf.rs:403-411: constraint iterations
     for (uint64_t it = 0; it < prm_.iterations; ++it) {
-        k_pbf_density<<<nb, kPbfThreads, 0, st>>>(n, kc_, w.cur_, w.lists_);
-        k_pbf_lambda<<<nb, kPbfThreads, 0, st>>>(n, kc_, w.cur_, w.lists_, lambda_, lambda_orig_);
-        k_pbf_delta_p<<<nb, kPbfThreads, 0, st>>>(n, kc_, w.cur_, w.lists_, lambda_, dp_);
+        k_pbf_density<<<nb, kPbfThreads, kKeepBytes, st>>>(n, kc_, w.cur_, w.lists_);
+        k_pbf_lambda<<<nb, kPbfThreads, kKeepBytes, st>>>(n, kc_, w.cur_, w.lists_, lambda_, lambda_orig_);
+        k_pbf_delta_p<<<nb, kPbfThreads, kKeepBytes, st>>>(n, kc_, w.cur_, w.lists_, lambda_, dp_);
         k_pbf_apply_dp<<<nb, kPbfThreads, 0, st>>>(n, w.dim_, w.cur_, dp_);
         w.launches_ += 4;
         if (!prm_.reuse_neighbours) {
@@ -475,7 +479,7 @@ void PbfSolver::step(double dt) {
     w.launches_ += 1;
     w.build_grid(nullptr, nullptr);
     lists(false);
-    k_pbf_density<<<nb, kPbfThreads, 0, st>>>(n, kc_, w.cur_, w.lists_);
+    k_pbf_density<<<nb, kPbfThreads, kKeepBytes, st>>>(n, kc_, w.cur_, w.lists_);
     w.launches_ += 1;
     // pbf.rs:288-381: the grid on x equals the one just built
     if (prm_.viscosity_eps != 0.0) {

@@ -162,7 +162,7 @@ struct DeviceScalars {
     uint32_t status;
     uint32_t nocc;                  // occupied cells
     uint32_t max_union;             // largest neighbour-cell union seen by the list build
-    uint32_t pad_;
+    uint32_t pad_;                  // scratch flag (state import: a position changed)
     unsigned long long list_used;   // 16-byte groups the last list build asked for
 };
 

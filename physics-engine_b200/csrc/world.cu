@@ -37,17 +37,24 @@ __global__ void k_export_w(uint32_t n, const uint32_t* __restrict__ slot_of_orig
     out[i] = src4 ? src4[s].w : src1[s];
 }
 
+// changed (optional): set to 1 when any written component differs in its bits
+// from what the slot held
 __global__ void k_import_vec(uint32_t n, const uint32_t* __restrict__ slot_of_orig,
                              const double* __restrict__ in, double4* __restrict__ dst,
-                             const uint8_t* __restrict__ flags, int only_fluid) {
+                             const uint8_t* __restrict__ flags, int only_fluid, uint32_t* changed) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     uint32_t s = slot_of_orig[i];
     if (only_fluid && (flags[s] & kFlagBoundary)) return;
     double4 v = dst[s];
-    v.x = in[3 * (size_t)i];
-    v.y = in[3 * (size_t)i + 1];
-    v.z = in[3 * (size_t)i + 2];
+    const double x = in[3 * (size_t)i], y = in[3 * (size_t)i + 1], z = in[3 * (size_t)i + 2];
+    if (changed && (__double_as_longlong(x) != __double_as_longlong(v.x) ||
+                    __double_as_longlong(y) != __double_as_longlong(v.y) ||
+                    __double_as_longlong(z) != __double_as_longlong(v.z)))
+        *changed = 1u;
+    v.x = x;
+    v.y = y;
+    v.z = z;
     dst[s] = v;
 }
 
@@ -1002,13 +1009,20 @@ void World::set_vec(int which, const double* in) {
     uint32_t n = (uint32_t)n_;
     if (!n) return;
     check(cudaMemcpyAsync(xfer_, in, sizeof(double) * 3 * n_, cudaMemcpyHostToDevice, st_), "import");
+    // Positions that come back bit for bit as they were (a caller that reads
+    // the state out and writes it back) leave the grid, lists and densities
+    // valid: rebuilding them would reproduce the same bits.
+    uint32_t* changed = which == 0 ? &sc_->pad_ : nullptr;
+    if (changed) check(cudaMemsetAsync(changed, 0, sizeof(uint32_t), st_), "import");
     // Velocities of boundary samples are part of the state too (the reference
     // stores them; they never move), so both kinds are written.
     k_import_vec<<<blocks_for(n, 256), 256, 0, st_>>>(n, slot_of_orig_, xfer_,
-                                                      which == 0 ? cur_.pos : cur_.vel, cur_.flags, 0);
+                                                      which == 0 ? cur_.pos : cur_.vel, cur_.flags, 0, changed);
     refresh_f32();
+    uint32_t moved = 1;
+    if (changed) check(cudaMemcpyAsync(&moved, changed, sizeof(uint32_t), cudaMemcpyDeviceToHost, st_), "import");
     check(cudaStreamSynchronize(st_), "import");
-    if (which == 0) {
+    if (which == 0 && moved) {
         grid_current_ = false;
         rho_current_ = false;
         lists_valid_ = false;

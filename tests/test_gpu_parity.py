@@ -163,3 +163,25 @@ def test_c1_scene_two_steps_bit_exact():
     co, so = o.neighbour_counts()
     np.testing.assert_array_equal(cg.astype(np.int64), co)
     np.testing.assert_array_equal(sg.astype(np.int64), so)
+
+
+def test_state_write_back_bit_exact():
+    """Writing positions back unchanged keeps the grid, lists and densities
+    (they would be rebuilt to the same bits); writing changed positions
+    rebuilds them. Both continue bit for bit with the oracle."""
+    w, o = _pair(**SMALL)
+    w.run(1e-4, 3)
+    o.run(1e-4, 3)
+    w.set_positions(w.positions())
+    w.set_velocities(w.velocities())
+    w.step(1e-4)
+    o.step(1e-4)
+    _compare_state(w, o, "unchanged write-back")
+    x = w.positions()
+    x[5] += 1e-4
+    w.set_positions(x)
+    o.set_x(x)
+    w.run(1e-4, 2)
+    o.run(1e-4, 2)
+    _compare_state(w, o, "changed write-back")
+    w.close()
