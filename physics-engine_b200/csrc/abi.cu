@@ -641,23 +641,13 @@ int pe_fluid_wcsph_get_kinds(PeWcsph* w, uint8_t* out, uint64_t n) {
 int pe_fluid_wcsph_set_positions(PeWcsph* w, const double* in, uint64_t n) {
     if (!w || !in) return PE_ERR_NULL;
     if (n != w->world->len()) return PE_ERR_BOUNDS;
-    for (uint64_t i = 0; i < 3 * n; ++i)
-        if (!std::isfinite(in[i])) return PE_ERR_ARG;
-    return guard([&] {
-        w->world->set_vec(0, in);
-        return PE_OK;
-    });
+    return guard([&] { return w->world->set_vec(0, in) ? PE_OK : PE_ERR_ARG; });
 }
 
 int pe_fluid_wcsph_set_velocities(PeWcsph* w, const double* in, uint64_t n) {
     if (!w || !in) return PE_ERR_NULL;
     if (n != w->world->len()) return PE_ERR_BOUNDS;
-    for (uint64_t i = 0; i < 3 * n; ++i)
-        if (!std::isfinite(in[i])) return PE_ERR_ARG;
-    return guard([&] {
-        w->world->set_vec(1, in);
-        return PE_OK;
-    });
+    return guard([&] { return w->world->set_vec(1, in) ? PE_OK : PE_ERR_ARG; });
 }
 
 int pe_fluid_wcsph_set_densities(PeWcsph* w, const double* in, uint64_t n) {

@@ -255,11 +255,8 @@ PE_PBF_GET(get_lambdas, w->s->get_lambda(out))
     int pe_fluid_pbf_##name(PePbf* w, const double* in, uint64_t n) {     \
         if (!w || !in) return PE_ERR_NULL;                                \
         if (n != w->s->world().len()) return PE_ERR_BOUNDS;               \
-        for (uint64_t i = 0; i < 3 * n; ++i)                              \
-            if (!std::isfinite(in[i])) return PE_ERR_ARG;                 \
         return guard([&] {                                                \
-            w->s->world().set_vec(which, in);                             \
-            return PE_OK;                                                 \
+            return w->s->world().set_vec(which, in) ? PE_OK : PE_ERR_ARG; \
         });                                                               \
     }
 PE_PBF_SET(set_positions, 0)
@@ -468,11 +465,8 @@ PE_DF_GET(get_alphas, w->s->get_alpha(out))
     int pe_fluid_dfsph_##name(PeDfsph* w, const double* in, uint64_t n) { \
         if (!w || !in) return PE_ERR_NULL;                                \
         if (n != w->s->world().len()) return PE_ERR_BOUNDS;               \
-        for (uint64_t i = 0; i < 3 * n; ++i)                              \
-            if (!std::isfinite(in[i])) return PE_ERR_ARG;                 \
         return guard([&] {                                                \
-            w->s->world().set_vec(which, in);                             \
-            return PE_OK;                                                 \
+            return w->s->world().set_vec(which, in) ? PE_OK : PE_ERR_ARG; \
         });                                                               \
     }
 PE_DF_SET(set_positions, 0)

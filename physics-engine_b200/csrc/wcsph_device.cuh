@@ -164,6 +164,8 @@ struct DeviceScalars {
     uint32_t max_union;             // largest neighbour-cell union seen by the list build
     uint32_t pad_;                  // scratch flag (state import: a position changed)
     unsigned long long list_used;   // 16-byte groups the last list build asked for
+    uint32_t import_bad;            // state import: a non-finite value was found
+    uint32_t pad2_;
 };
 
 // Block size of the per-particle passes: a launch parameter, chosen by the

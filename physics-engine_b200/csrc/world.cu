@@ -37,13 +37,21 @@ __global__ void k_export_w(uint32_t n, const uint32_t* __restrict__ slot_of_orig
     out[i] = src4 ? src4[s].w : src1[s];
 }
 
+// bad = 1 when any of the m values is not finite
+__global__ void k_check_finite(uint64_t m, const double* __restrict__ in, uint32_t* bad) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (uint64_t)gridDim.x * blockDim.x)
+        if (!isfinite(in[i])) *bad = 1u;
+}
+
 // changed (optional): set to 1 when any written component differs in its bits
-// from what the slot held
+// from what the slot held. Nothing is written when *bad is set.
 __global__ void k_import_vec(uint32_t n, const uint32_t* __restrict__ slot_of_orig,
                              const double* __restrict__ in, double4* __restrict__ dst,
-                             const uint8_t* __restrict__ flags, int only_fluid, uint32_t* changed) {
+                             const uint8_t* __restrict__ flags, int only_fluid, uint32_t* changed,
+                             const uint32_t* bad = nullptr) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    if (bad && *bad) return;
     uint32_t s = slot_of_orig[i];
     if (only_fluid && (flags[s] & kFlagBoundary)) return;
     double4 v = dst[s];
@@ -1005,10 +1013,15 @@ void World::get_vec(int which, double* out) {
     gather_orig_vec(src, out);
 }
 
-void World::set_vec(int which, const double* in) {
+bool World::set_vec(int which, const double* in) {
     uint32_t n = (uint32_t)n_;
-    if (!n) return;
+    if (!n) return true;
     check(cudaMemcpyAsync(xfer_, in, sizeof(double) * 3 * n_, cudaMemcpyHostToDevice, st_), "import");
+    // The input is checked for non-finite values on the device (a host scan of
+    // the caller's buffer costs more than the copy); a rejected input leaves
+    // the state untouched.
+    check(cudaMemsetAsync(&sc_->import_bad, 0, sizeof(uint32_t), st_), "import");
+    k_check_finite<<<sms_ * 4, 256, 0, st_>>>(3 * n_, xfer_, &sc_->import_bad);
     // Positions that come back bit for bit as they were (a caller that reads
     // the state out and writes it back) leave the grid, lists and densities
     // valid: rebuilding them would reproduce the same bits.
@@ -1017,17 +1030,21 @@ void World::set_vec(int which, const double* in) {
     // Velocities of boundary samples are part of the state too (the reference
     // stores them; they never move), so both kinds are written.
     k_import_vec<<<blocks_for(n, 256), 256, 0, st_>>>(n, slot_of_orig_, xfer_,
-                                                      which == 0 ? cur_.pos : cur_.vel, cur_.flags, 0, changed);
-    refresh_f32();
-    uint32_t moved = 1;
-    if (changed) check(cudaMemcpyAsync(&moved, changed, sizeof(uint32_t), cudaMemcpyDeviceToHost, st_), "import");
+                                                      which == 0 ? cur_.pos : cur_.vel, cur_.flags, 0, changed,
+                                                      &sc_->import_bad);
+    uint32_t flags_h[2] = {0u, 1u};  // bad, moved
+    check(cudaMemcpyAsync(&flags_h[0], &sc_->import_bad, sizeof(uint32_t), cudaMemcpyDeviceToHost, st_), "import");
+    if (changed) check(cudaMemcpyAsync(&flags_h[1], changed, sizeof(uint32_t), cudaMemcpyDeviceToHost, st_), "import");
     check(cudaStreamSynchronize(st_), "import");
-    if (which == 0 && moved) {
+    if (flags_h[0]) return false;
+    refresh_f32();
+    if (which == 0 && flags_h[1]) {
         grid_current_ = false;
         rho_current_ = false;
         lists_valid_ = false;
         lists_checked_ = false;
     }
+    return true;
 }
 
 void World::get_scalar(int which, double* out) {

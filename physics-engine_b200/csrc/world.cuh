@@ -86,7 +86,8 @@ class World {
 
     // Host-buffer access in original particle order.
     void get_vec(int which, double* out);         // 0 x, 1 v, 2 a, 3 boundary force
-    void set_vec(int which, const double* in);    // 0 x, 1 v
+    // 0 x, 1 v; false (state untouched) when the input holds a non-finite value
+    bool set_vec(int which, const double* in);
     void get_scalar(int which, double* out);      // 0 rho, 1 p
     void set_scalar(int which, const double* in); // 0 rho, 1 p
     void get_kind(uint8_t* out);

@@ -185,3 +185,20 @@ def test_state_write_back_bit_exact():
     o.run(1e-4, 2)
     _compare_state(w, o, "changed write-back")
     w.close()
+
+
+def test_non_finite_state_rejected_untouched():
+    """Non-finite positions or velocities are refused (PE_ERR_ARG, the pe-ffi
+    rule) and leave the world's state as it was."""
+    w, _ = _pair(**SMALL)
+    w.run(1e-4, 2)
+    x0, v0 = w.positions(), w.velocities()
+    for setter, arr in ((w.set_positions, x0), (w.set_velocities, v0)):
+        bad = arr.copy()
+        bad[len(bad) // 2, 1] = np.nan
+        with pytest.raises(pe.PeError) as e:
+            setter(bad)
+        assert e.value.code == pe.PE_ERR_ARG
+    assert_bits_equal(w.positions(), x0, "x kept")
+    assert_bits_equal(w.velocities(), v0, "v kept")
+    w.close()
