@@ -411,7 +411,7 @@ int pe_fluid_wcsph_stream(PeWcsph* w, void** out);
 int pe_fluid_wcsph_kernel_launches(PeWcsph* w, uint64_t* out, int32_t reset);
 
 /* ---- stateless helpers ---- */
-/* kernels.rs:40 w and kernels.rs:56 grad_w (cubic spline), eos.rs:65 pressure. */
+/* kernels.rs:40 w and kernels.rs:56 grad_w (every PE_KERNEL_*), eos.rs:65 pressure. */
 double pe_fluid_kernel_w(int32_t kernel, double r, double h, int32_t dim);
 int pe_fluid_grad_w(int32_t kernel, const double rij[3], double h, int32_t dim, double out[3]);
 double pe_fluid_tait_pressure(double rest_density, double sound_speed, double gamma, double density);

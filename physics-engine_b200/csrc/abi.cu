@@ -12,6 +12,7 @@
 #include "../../include/pe_fluid_wcsph.h"
 #include "pe_math.cuh"
 #include "handles.cuh"
+#include "kernel_any.cuh"
 #include "coupling.cuh"
 #include "world.cuh"
 
@@ -799,25 +800,17 @@ int pe_fluid_wcsph_kernel_launches(PeWcsph* w, uint64_t* out, int32_t reset) {
 
 // ---------------------------------------------------------------- helpers
 double pe_fluid_kernel_w(int32_t kernel, double r, double h, int32_t dim) {
-    if (kernel != PE_KERNEL_CUBIC_SPLINE || !valid_dim(dim)) return NAN;
-    return pe::cubic_w(r, h, pe::cubic_alpha(h, dim));
+    if (kernel < PE_KERNEL_CUBIC_SPLINE || kernel > PE_KERNEL_SPIKY || !valid_dim(dim)) return NAN;
+    if (h <= 0.0) return 0.0;  // kernels.rs:41
+    return pe::kfn_w(pe::make_kernel_fn(kernel, h, dim), r);
 }
 
 int pe_fluid_grad_w(int32_t kernel, const double rij[3], double h, int32_t dim, double out[3]) {
     if (!rij || !out) return PE_ERR_NULL;
-    if (kernel != PE_KERNEL_CUBIC_SPLINE) return PE_ERR_UNSUPPORTED;
-    if (!valid_dim(dim)) return PE_ERR_ARG;
-    // kernels.rs:56-75
+    if (kernel < PE_KERNEL_CUBIC_SPLINE || kernel > PE_KERNEL_SPIKY || !valid_dim(dim)) return PE_ERR_ARG;
     out[0] = out[1] = out[2] = 0.0;
-    if (h <= 0.0) return PE_OK;
-    const double r2 = rij[0] * rij[0] + rij[1] * rij[1] + rij[2] * rij[2];
-    const double r = std::sqrt(r2);
-    const double dwdr = pe::cubic_dwdr(r, h, pe::cubic_alpha(h, dim));
-    if (r < 1e-30) return PE_OK;
-    const double s = -dwdr / r;
-    out[0] = rij[0] * s;
-    out[1] = rij[1] * s;
-    out[2] = rij[2] * s;
+    if (h <= 0.0) return PE_OK;  // kernels.rs:57
+    pe::kfn_grad(pe::make_kernel_fn(kernel, h, dim), rij[0], rij[1], rij[2], &out[0], &out[1], &out[2]);
     return PE_OK;
 }
 

@@ -39,15 +39,21 @@ inline KernelFn make_kernel_fn(int kind, double h, int dim) {
     return KernelFn{kind, h, 1.0 / h, kernel_alpha(kind, h, dim)};
 }
 
-__device__ __forceinline__ double kdiv_h(double a, const KernelFn& k) {
+// RN(a / h): on the device by one multiply and a Markstein correction, on the
+// host by the IEEE division (the same value)
+PE_HD double kdiv_h(double a, const KernelFn& k) {
+#ifdef __CUDA_ARCH__
     if (!(fabs(a) < 1e300) || fabs(a) < 1e-290) return a / k.h;
     const double q0 = a * k.inv_h;
     const double r = fma(-q0, k.h, a);
     return fma(r, k.inv_h, q0);
+#else
+    return a / k.h;
+#endif
 }
 
 // kernels.rs:40 w
-__device__ __forceinline__ double kfn_w(const KernelFn& k, double r) {
+PE_HD double kfn_w(const KernelFn& k, double r) {
     if (k.h <= 0.0 || r < 0.0) return 0.0;
     const double a = k.alpha;
     switch (k.kind) {
@@ -78,7 +84,7 @@ __device__ __forceinline__ double kfn_w(const KernelFn& k, double r) {
 }
 
 // dW/dr of each kind (kernels.rs:102, 139, 169, 197)
-__device__ __forceinline__ double kfn_dwdr(const KernelFn& k, double r) {
+PE_HD double kfn_dwdr(const KernelFn& k, double r) {
     const double a = k.alpha;
     switch (k.kind) {
         case kCubic: {
@@ -114,7 +120,7 @@ __device__ __forceinline__ double kfn_dwdr(const KernelFn& k, double r) {
 }
 
 // kernels.rs:56 grad_w at rij = rj - ri (returns grad_i W)
-__device__ __forceinline__ void kfn_grad(const KernelFn& k, double rx, double ry, double rz, double* gx,
+PE_HD void kfn_grad(const KernelFn& k, double rx, double ry, double rz, double* gx,
                                          double* gy, double* gz) {
     if (k.h <= 0.0) {
         *gx = *gy = *gz = 0.0;

@@ -131,6 +131,24 @@ def test_kernel_and_pair_helpers_match_oracle_bitwise():
         assert pe.suggested_dt(*args) == O.suggested_dt(*args)
 
 
+def test_all_kernel_kinds_match_oracle_bitwise():
+    """kernels.rs:40-215: cubic spline, Wendland C2, poly6 and spiky, W and
+    grad W in 2-D and 3-D, inside, across and beyond the support."""
+    rng = np.random.default_rng(11)
+    for kind in (pe.CUBIC_SPLINE, pe.WENDLAND_C2, pe.POLY6, pe.SPIKY):
+        for dim in (2, 3):
+            for _ in range(500):
+                h = float(rng.uniform(0.01, 0.2))
+                rij = rng.uniform(-2.5 * h, 2.5 * h, 3)
+                if dim == 2:
+                    rij[2] = 0.0
+                r = float(np.linalg.norm(rij))
+                assert pe.kernel_w(kind, r, h, dim) == O.kernel_w(kind, r, h, dim)
+                assert np.array_equal(pe.grad_w(kind, rij, h, dim), O.grad_w(kind, rij, h, dim))
+            assert pe.kernel_w(kind, 0.0, 0.1, dim) == O.kernel_w(kind, 0.0, 0.1, dim)
+            assert pe.kernel_w(kind, 0.05, -1.0, dim) == 0.0
+
+
 def test_params_water_defaults():
     """wcsph.rs:43-53, viscosity.rs:39-45,82-86, eos.rs:25."""
     p = pe.WcsphParams.water(1000.0, 20.0, (0.0, 0.0, -9.81))
