@@ -100,7 +100,7 @@ PeWcsphParams from_world(const pe::WorldParams& w) {
 
 int check_params(const PeWcsphParams* p) {
     if (!p) return PE_ERR_NULL;
-    if (p->density_kernel != PE_KERNEL_CUBIC_SPLINE) return PE_ERR_UNSUPPORTED;
+    if (p->density_kernel < PE_KERNEL_CUBIC_SPLINE || p->density_kernel > PE_KERNEL_SPIKY) return PE_ERR_ARG;
     if (!std::isfinite(p->surface_tension_sigma) || !std::isfinite(p->surface_tension_colour_gamma))
         return PE_ERR_ARG;
     if (p->surface_tension_model < PE_SURFACE_TENSION_NONE || p->surface_tension_model > PE_SURFACE_TENSION_COLOUR_FIELD)
@@ -430,8 +430,9 @@ int pe_fluid_wcsph_create_batch(const PeWcsphParams* params, int32_t dim, double
     *out = nullptr;
     int rc = check_params(params);
     if (rc != PE_OK) return rc;
-    if (cfg && cfg->precision == PE_PRECISION_F32 && params->surface_tension_sigma != 0.0)
-        return PE_ERR_UNSUPPORTED;  // the surface-tension branch runs in the f64 step only
+    if (cfg && cfg->precision == PE_PRECISION_F32 &&
+        (params->surface_tension_sigma != 0.0 || params->density_kernel != PE_KERNEL_CUBIC_SPLINE))
+        return PE_ERR_UNSUPPORTED;  // the single-precision form: cubic spline, no surface tension
     if (!valid_dim(dim)) return PE_ERR_ARG;
     if (!(std::isfinite(rest_density) && rest_density > 0.0 && std::isfinite(mass) && mass > 0.0 &&
           std::isfinite(h) && h > 0.0))
@@ -590,7 +591,9 @@ int pe_fluid_wcsph_set_params(PeWcsph* w, const PeWcsphParams* params) {
     if (!w) return PE_ERR_NULL;
     int rc = check_params(params);
     if (rc != PE_OK) return rc;
-    if (w->world->single_precision() && params->surface_tension_sigma != 0.0) return PE_ERR_UNSUPPORTED;
+    if (w->world->single_precision() &&
+        (params->surface_tension_sigma != 0.0 || params->density_kernel != PE_KERNEL_CUBIC_SPLINE))
+        return PE_ERR_UNSUPPORTED;
     return guard([&] {
         w->world->set_params(to_world(*params));
         return PE_OK;

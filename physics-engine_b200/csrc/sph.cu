@@ -39,6 +39,7 @@ struct PosVel {
     double4 x, v;
 };
 
+template <bool CUBIC>
 __global__ void __launch_bounds__(kMaxPassThreads) k_density(uint32_t n, StepConst k, StateBufs s,
                                                       ListBufs l) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -55,7 +56,7 @@ __global__ void __launch_bounds__(kMaxPassThreads) k_density(uint32_t n, StepCon
         const uint32_t j = e & kEntrySlotMask;
         const double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
         const double r = sqrt(dx * dx + dy * dy + dz * dz);
-        const double wij = kern_w(r, k);
+        const double wij = kw<CUBIC>(r, k);
         if ((e & kEntryOriented) && !sees_fluid(k, xj, s.nout[j], xi.x, xi.y, xi.z)) return;
         // fluid: mass * W; boundary: (rho0 * psi_j) * W (wcsph.rs:143-148)
         const double f = (e & kEntryBoundary) ? k.rho0 * xj.w : k.mass;
@@ -129,6 +130,7 @@ __global__ void k_pressure(uint32_t n, StepConst k, Tanks tk, StateBufs s) {
 
 // Pressure + Monaghan viscosity force of fluid pair (k, j), seen from k:
 // rx = x_j - x_k (wcsph.rs:219), pi_ij(x_k, x_j, v_k, v_j, rho_k, rho_j).
+template <bool CUBIC>
 __device__ __forceinline__ void fluid_pair(const StepConst& kc, double nac, double4 xk, double4 vk,
                                            double4 xj, double4 vj, double& ax, double& ay,
                                            double& az) {
@@ -136,7 +138,7 @@ __device__ __forceinline__ void fluid_pair(const StepConst& kc, double nac, doub
     const double r2 = rx * rx + ry * ry + rz * rz;
     const double r = sqrt(r2);
     if (r < 1e-30) return;
-    const double dwdr = kern_dwdr(r, kc);
+    const double dwdr = kdwdr<CUBIC>(r, kc);
     const double sc = -dwdr / r;
     const double gx = rx * sc, gy = ry * sc, gz = rz * sc;
     const double press = xk.w + xj.w;  // p_k/rho_k^2 + p_j/rho_j^2
@@ -159,6 +161,7 @@ __device__ __forceinline__ void fluid_pair(const StepConst& kc, double nac, doub
 }
 
 // Akinci boundary pressure of fluid k against boundary sample j (wcsph.rs:244-255).
+template <bool CUBIC>
 __device__ __forceinline__ void boundary_pair(const StepConst& kc, double4 xk, double4 xj,
                                               bool oriented, const double4* nout, uint32_t j,
                                               double& ax, double& ay, double& az) {
@@ -167,7 +170,7 @@ __device__ __forceinline__ void boundary_pair(const StepConst& kc, double4 xk, d
     double r = sqrt(r2);
     if (r < 1e-30) return;
     if (oriented && !sees_fluid(kc, xj, nout[j], xk.x, xk.y, xk.z)) return;
-    double dwdr = kern_dwdr(r, kc);
+    double dwdr = kdwdr<CUBIC>(r, kc);
     double sc = -dwdr / r;
     double gx = rx * sc, gy = ry * sc, gz = rz * sc;
     double m = -(kc.rho0 * xj.w) * xk.w;  // -(rho0 psi_j) * p_k/rho_k^2
@@ -176,7 +179,7 @@ __device__ __forceinline__ void boundary_pair(const StepConst& kc, double4 xk, d
     az += gz * m;
 }
 
-template <bool INTEGRATE, int DIM>
+template <bool INTEGRATE, int DIM, bool CUBIC>
 __global__ void __launch_bounds__(kMaxPassThreads) k_forces(uint32_t n, StepConst kc, Tanks tk,
                                                             StateBufs s, ListBufs l, double dt,
                                                             double4* __restrict__ pos_next,
@@ -200,7 +203,7 @@ __global__ void __launch_bounds__(kMaxPassThreads) k_forces(uint32_t n, StepCons
         return d;
     };
     for_each_loaded(list_ref(l, k, kListLower), load, [&](uint32_t, const PosVel& d) {
-        fluid_pair(kc, nac, xk, vk, d.x, d.v, ax, ay, az);
+        fluid_pair<CUBIC>(kc, nac, xk, vk, d.x, d.v, ax, ay, az);
     });
     // fluid j > k and boundary j, visiting order: the visit list without the
     // entries flagged lower (those came from the lower list, in index order).
@@ -232,9 +235,9 @@ __global__ void __launch_bounds__(kMaxPassThreads) k_forces(uint32_t n, StepCons
                 d = load(e);
             }
             if (ec & kEntryBoundary) {
-                boundary_pair(kc, xk, dc.x, (ec & kEntryOriented) != 0u, s.nout, ec & kEntrySlotMask, ax, ay, az);
+                boundary_pair<CUBIC>(kc, xk, dc.x, (ec & kEntryOriented) != 0u, s.nout, ec & kEntrySlotMask, ax, ay, az);
             } else {
-                fluid_pair(kc, nac, xk, vk, dc.x, dc.v, ax, ay, az);
+                fluid_pair<CUBIC>(kc, nac, xk, vk, dc.x, dc.v, ax, ay, az);
             }
         }
     }
@@ -263,6 +266,7 @@ __global__ void __launch_bounds__(kMaxPassThreads) k_forces(uint32_t n, StepCons
 
 // boundary_force[j] (wcsph.rs:254): sum over fluid i in ascending index of
 // f(i,j) * (-m) with f = gradW(x_j - x_i) * (-(rho0 psi_j) * p_i/rho_i^2).
+template <bool CUBIC>
 __global__ void __launch_bounds__(kThreads) k_boundary_force(uint32_t n, StepConst kc, StateBufs s,
                                                              ListBufs l) {
     uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
@@ -281,7 +285,7 @@ __global__ void __launch_bounds__(kThreads) k_boundary_force(uint32_t n, StepCon
         double r = sqrt(r2);
         if (r < 1e-30) return;
         if (oriented && !sees_fluid(kc, xb, nb, xi.x, xi.y, xi.z)) return;
-        double dwdr = kern_dwdr(r, kc);
+        double dwdr = kdwdr<CUBIC>(r, kc);
         double sc = -dwdr / r;
         double m = mpsi * xi.w;
         double ffx = (rx * sc) * m, ffy = (ry * sc) * m, ffz = (rz * sc) * m;
@@ -292,6 +296,7 @@ __global__ void __launch_bounds__(kThreads) k_boundary_force(uint32_t n, StepCon
     s.bf[b] = make_double4(fx, fy, fz, 0.0);
 }
 
+template <bool CUBIC>
 __global__ void __launch_bounds__(kMaxPassThreads) k_xsph(uint32_t n, StepConst kc, StateBufs s,
                                                    ListBufs l, double4* __restrict__ vel_out) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -318,7 +323,7 @@ __global__ void __launch_bounds__(kMaxPassThreads) k_xsph(uint32_t n, StepConst 
         const double4 xj = d.x;
         const double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
         const double r = sqrt(dx * dx + dy * dy + dz * dz);
-        const double wij = kern_w(r, kc);
+        const double wij = kw<CUBIC>(r, kc);
         const double4 vj = d.v;
         const double rho_bar = 0.5 * (vi.w + vj.w);
         const double f = kc.mass / rho_bar * wij;
@@ -343,7 +348,7 @@ __global__ void k_in_support(uint32_t n, StepConst kc, StateBufs s, ListBufs l, 
         const double4 xj = s.pos[e & kEntrySlotMask];
         const double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
         const double r = sqrt(dx * dx + dy * dy + dz * dz);
-        c += div_h(r, kc) < 2.0;
+        c += in_support(r, kc);
     });
     out[i] = c;
 }
@@ -352,7 +357,9 @@ __global__ void k_in_support(uint32_t n, StepConst kc, StateBufs s, ListBufs l, 
 
 void launch_density(uint32_t n, uint32_t threads, const StepConst& k, const StateBufs& s,
                     const ListBufs& l, cudaStream_t st) {
-    if (n) k_density<<<blocks_for(n, threads), threads, 0, st>>>(n, k, s, l);
+    if (!n) return;
+    if (k.kernel == 0) k_density<true><<<blocks_for(n, threads), threads, 0, st>>>(n, k, s, l);
+    else k_density<false><<<blocks_for(n, threads), threads, 0, st>>>(n, k, s, l);
 }
 
 void launch_vmax(uint32_t n, const Tanks& tk, const StateBufs& s, cudaStream_t st) {
@@ -370,23 +377,40 @@ void launch_forces(uint32_t n, uint32_t threads, const StepConst& k, const Tanks
     if (!n) return;
     const uint32_t b = blocks_for(n, threads);
     const size_t sm = (size_t)kCompact * threads * sizeof(uint32_t);
+    const bool cubic = k.kernel == 0;
+#define PE_FORCES(I, D, C) k_forces<I, D, C><<<b, threads, sm, st>>>(n, k, tk, s, l, dt, pos_next, vel_next, st_a)
     if (k.dim == 3) {
-        if (integrate) k_forces<true, 3><<<b, threads, sm, st>>>(n, k, tk, s, l, dt, pos_next, vel_next, st_a);
-        else k_forces<false, 3><<<b, threads, sm, st>>>(n, k, tk, s, l, dt, pos_next, vel_next, st_a);
+        if (cubic) {
+            if (integrate) PE_FORCES(true, 3, true);
+            else PE_FORCES(false, 3, true);
+        } else {
+            if (integrate) PE_FORCES(true, 3, false);
+            else PE_FORCES(false, 3, false);
+        }
     } else {
-        if (integrate) k_forces<true, 2><<<b, threads, sm, st>>>(n, k, tk, s, l, dt, pos_next, vel_next, st_a);
-        else k_forces<false, 2><<<b, threads, sm, st>>>(n, k, tk, s, l, dt, pos_next, vel_next, st_a);
+        if (cubic) {
+            if (integrate) PE_FORCES(true, 2, true);
+            else PE_FORCES(false, 2, true);
+        } else {
+            if (integrate) PE_FORCES(true, 2, false);
+            else PE_FORCES(false, 2, false);
+        }
     }
+#undef PE_FORCES
 }
 
 void launch_boundary_force(uint32_t n, const StepConst& k, const StateBufs& s, const ListBufs& l,
                            cudaStream_t st) {
-    if (n) k_boundary_force<<<blocks_for(n, kThreads), kThreads, 0, st>>>(n, k, s, l);
+    if (!n) return;
+    if (k.kernel == 0) k_boundary_force<true><<<blocks_for(n, kThreads), kThreads, 0, st>>>(n, k, s, l);
+    else k_boundary_force<false><<<blocks_for(n, kThreads), kThreads, 0, st>>>(n, k, s, l);
 }
 
 void launch_xsph(uint32_t n, uint32_t threads, const StepConst& k, const StateBufs& s,
                  const ListBufs& l, double4* vel_out, cudaStream_t st) {
-    if (n) k_xsph<<<blocks_for(n, threads), threads, 0, st>>>(n, k, s, l, vel_out);
+    if (!n) return;
+    if (k.kernel == 0) k_xsph<true><<<blocks_for(n, threads), threads, 0, st>>>(n, k, s, l, vel_out);
+    else k_xsph<false><<<blocks_for(n, threads), threads, 0, st>>>(n, k, s, l, vel_out);
 }
 
 void launch_in_support_counts(uint32_t n, const StepConst& k, const StateBufs& s,

@@ -75,9 +75,10 @@ struct Tanks {
 
 struct StepConst {
     int dim;
+    int kernel;                // KernelKind (kernels.rs:19); 0 = cubic spline
     double h, mass, rho0;      // particles.h, .mass, .rest_density
     double inv_h;              // RN(1 / h), for the exact division by h
-    double alpha;              // cubic_alpha(h, dim)
+    double alpha;              // the kernel's normalisation for (h, dim)
     double rho_self;           // 0.0 + mass * W(0)
     double visc_alpha, visc_beta, eps_h2;  // eps_h2 = visc.eps * h * h
     double eos_rho0, eos_gamma;

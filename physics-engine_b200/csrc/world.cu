@@ -5,6 +5,7 @@
 #include <cstring>
 #include <limits>
 
+#include "kernel_any.cuh"
 #include "pe_math.cuh"
 #include "world.cuh"
 
@@ -132,7 +133,8 @@ World::World(const WorldParams& prm, const WorldConfig& cfg, int dim, double res
              double mass, double h, uint64_t n, const double* x, const double* v,
              const uint8_t* kind, const double* psi, const double* n_out,
              const uint64_t* tank_offsets, uint32_t n_tanks, double support)
-    : dim_(dim), rho0_(rest_density), mass_(mass), h_(h), support_(support > 0.0 ? support : 2.0 * h),
+    : dim_(dim), rho0_(rest_density), mass_(mass), h_(h),
+      support_(support > 0.0 ? support : kernel_support(prm.kernel, h)),
       n_(n), prm_(prm), cfg_(cfg) {
     if (cfg_.device >= 0) check(cudaSetDevice(cfg_.device), "cudaSetDevice");
     check(cudaGetDevice(&device_), "cudaGetDevice");
@@ -209,6 +211,7 @@ World::World(const WorldParams& prm, const WorldConfig& cfg, int dim, double res
         f32_ = cfg_.precision == 1;
         if (f32_ && prm_.surface_tension_sigma != 0.0)
             throw std::invalid_argument("surface tension needs the f64 step");
+        if (f32_ && prm_.kernel != 0) throw std::invalid_argument("the single-precision form is cubic-spline only");
         refresh_step_const();
         configure_surface_tension();
 
@@ -445,9 +448,11 @@ void World::refresh_step_const() {
     k.inv_h = 1.0 / h_;
     k.mass = mass_;
     k.rho0 = rho0_;
-    k.alpha = cubic_alpha(h_, dim_);
+    k.kernel = prm_.kernel;
+    const KernelFn kf = make_kernel_fn(prm_.kernel, h_, dim_);
+    k.alpha = kf.alpha;
     // wcsph.rs:133-135: rho = 0.0; rho += mass * w(kern, 0.0, h, dim)
-    k.rho_self = 0.0 + mass_ * cubic_w(0.0, h_, k.alpha);
+    k.rho_self = 0.0 + mass_ * kfn_w(kf, 0.0);
     k.visc_alpha = prm_.visc_alpha;
     k.visc_beta = prm_.visc_beta;
     k.eps_h2 = prm_.visc_eps * h_ * h_;  // viscosity.rs:63
@@ -508,6 +513,9 @@ void World::refresh_f32() {
 void World::set_params(const WorldParams& p) {
     if (f32_ && p.surface_tension_sigma != 0.0)
         throw std::invalid_argument("surface tension needs the f64 step");
+    if (f32_ && p.kernel != 0) throw std::invalid_argument("the single-precision form is cubic-spline only");
+    if (kernel_support(p.kernel, h_) != kernel_support(prm_.kernel, h_))
+        throw std::invalid_argument("the kernel's support radius is fixed at creation");
     bool c_changed = p.eos_sound_speed != prm_.eos_sound_speed;
     prm_ = p;
     refresh_step_const();

@@ -202,3 +202,23 @@ def test_non_finite_state_rejected_untouched():
     assert_bits_equal(w.positions(), x0, "x kept")
     assert_bits_equal(w.velocities(), v0, "v kept")
     w.close()
+
+
+@pytest.mark.parametrize("kind", [pe.WENDLAND_C2, pe.POLY6, pe.SPIKY])
+def test_other_kernel_kinds_bit_exact(kind):
+    """WcsphParams.density_kernel (wcsph.rs:26) other than the cubic spline:
+    Wendland C2 (support 2h) and poly6 / spiky (support h, grid cell h)."""
+    ps = product_dam_break(SMALL["nx"], SMALL["ny"], SMALL["nz"], box=SMALL["box"])
+    os_ = oracle_dam_break(SMALL["nx"], SMALL["ny"], SMALL["nz"], box=SMALL["box"])
+    p = dam_break_params_pe()
+    p.density_kernel = kind
+    q = O.dam_break_params(materialize=False)
+    q.kernel = kind
+    w = pe.WcsphWorld(ps, p)
+    o = O.World(os_, q)
+    for s in range(4):
+        w.step(1e-4)
+        o.step(1e-4)
+    _compare_state(w, o, f"kernel {kind}")
+    _compare_grid(w, o)
+    w.close()
