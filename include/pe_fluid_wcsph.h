@@ -54,8 +54,9 @@ extern "C" {
 #define PE_DIM_2 2
 #define PE_DIM_3 3
 
-/* KernelKind (crates/pe-fluid/src/kernels.rs:19); the WCSPH path supports the
- * cubic spline, the reference's default (wcsph.rs:45). */
+/* KernelKind (crates/pe-fluid/src/kernels.rs:19). The f64 WCSPH step takes any
+ * kind (the cubic spline is the reference's default, wcsph.rs:45); the
+ * single-precision form takes the cubic spline only. */
 #define PE_KERNEL_CUBIC_SPLINE 0
 #define PE_KERNEL_WENDLAND_C2 1
 #define PE_KERNEL_POLY6 2
