@@ -24,11 +24,12 @@
 // ascending-index order).
 //
 // The kernels work on chunks of up to 64 centre particles with four threads
-// per particle, each taking a quarter of the candidates (union words, or
-// sorted positions). A first pass keeps the in-support bit masks in shared
+// per particle. A first pass, each thread taking a quarter of the candidates
+// (union words, or sorted positions), keeps the in-support bit masks in shared
 // memory and counts; the chunk's longest lists size one block of the list
-// pool, reserved with one atomic add; a second pass writes each quarter's
-// entries at its offset in the list.
+// pool, reserved with one atomic add; a second pass writes the entries, each
+// thread a quarter of the particle's list (a quarter of the words would leave
+// most of the kept candidates, which lie in the middle words, to two threads).
 #include <climits>
 
 #include "pe_math.cuh"
@@ -176,6 +177,19 @@ __device__ __forceinline__ bool keep_entry(const float4& q, const float4& me, fl
     return within(q, me, r2f) || (keep_boundary && (__float_as_uint(q.w) & kStageBoundary));
 }
 
+// Keep mask of the 32 staged entries at q (keep_entry per bit).
+template <bool KEEP_BOUNDARY>
+__device__ __forceinline__ uint32_t word_mask(const float4* q, const float4& me, float r2f) {
+    uint32_t m = 0;
+#pragma unroll
+    for (int bit = 0; bit < 32; ++bit) {
+        const float4 e = q[bit];
+        const bool keep = within(e, me, r2f) || (KEEP_BOUNDARY && (__float_as_uint(e.w) & kStageBoundary));
+        m |= keep ? (1u << bit) : 0u;
+    }
+    return m;
+}
+
 __device__ __forceinline__ uint32_t rows_for(uint32_t n) { return (n + 3u) >> 2; }
 
 // Reserved block of one chunk: `rows_a + rows_b` rows of `stride` groups.
@@ -183,6 +197,35 @@ struct ChunkBlock {
     unsigned long long base;  // group index of row 0, lane 0
     uint32_t rows_a, rows_b;
     bool ok;
+};
+
+// Cursor over the set bits of one centre's masks (word w at m[w * kChunk]),
+// in ascending bit order: entry t of the list is the t-th set bit.
+struct MaskCursor {
+    const uint32_t* m;
+    uint32_t w, bits;
+    // Positioned on entry t0, given this centre's per-way counts cnt[r] of the
+    // way word ranges [W r / kWays, W (r + 1) / kWays); t0 < the total count.
+    __device__ __forceinline__ MaskCursor(const uint32_t* masks, const uint32_t (*cnt)[kChunk], uint32_t lane,
+                                          uint32_t W, uint32_t t0)
+        : m(masks + lane) {
+        uint32_t r = 0, acc = 0;
+        while (r + 1u < kWays && acc + cnt[r][lane] <= t0) acc += cnt[r++][lane];
+        w = W * r / kWays;
+        bits = m[w * kChunk];
+        while (acc + (uint32_t)__popc(bits) <= t0) {
+            acc += __popc(bits);
+            bits = m[++w * kChunk];
+        }
+        for (; acc < t0; ++acc) bits &= bits - 1u;
+    }
+    // Position of the next set bit; the caller takes no more than the count.
+    __device__ __forceinline__ uint32_t next() {
+        while (!bits) bits = m[++w * kChunk];
+        const uint32_t u = (w << 5) + (__ffs(bits) - 1);
+        bits &= bits - 1u;
+        return u;
+    }
 };
 
 // Every thread passes its (a, b) list lengths; thread 0 reserves the block for
@@ -240,19 +283,26 @@ __device__ __forceinline__ void radix_sort_by_orig(const float4* s_pos, uint16_t
         }
         __syncthreads();
         {
-            uint32_t v[16], sum = 0;
+            // this thread's 16 consecutive counters as two 16-byte words
+            // (32-byte stride between lanes: two-way bank conflicts, not 8)
+            uint4* cw = reinterpret_cast<uint4*>(s_cnt + tid * 16);
+            const uint4 c0 = cw[0], c1 = cw[1];
+            const uint32_t pk[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
+            uint32_t sum = 0;
 #pragma unroll
-            for (int d = 0; d < 16; ++d) {
-                v[d] = s_cnt[tid * 16 + d];
-                sum += v[d];
-            }
+            for (int j = 0; j < 8; ++j) sum += (pk[j] & 0xffffu) + (pk[j] >> 16);
             uint32_t ex, tot;
             block_exclusive_scan(sum, &ex, &tot);
+            uint32_t out[8];
 #pragma unroll
-            for (int d = 0; d < 16; ++d) {
-                s_cnt[tid * 16 + d] = (uint16_t)ex;
-                ex += v[d];
+            for (int j = 0; j < 8; ++j) {
+                const uint32_t lo = ex;
+                ex += pk[j] & 0xffffu;
+                out[j] = lo | (ex << 16);
+                ex += pk[j] >> 16;
             }
+            cw[0] = make_uint4(out[0], out[1], out[2], out[3]);
+            cw[1] = make_uint4(out[4], out[5], out[6], out[7]);
         }
         __syncthreads();
         for (uint32_t e = e0; e < e1; ++e) {
@@ -473,11 +523,8 @@ __global__ void __launch_bounds__(kNlThreads) k_nlist_visit(GridDesc g, Tanks tk
                     uint32_t cv = 0;
                     if (fluidc) {
                         for (uint32_t w = wb; w < we; ++w) {
-                            uint32_t m = 0;
-#pragma unroll
-                            for (int bit = 0; bit < 32; ++bit)
-                                m |= keep_entry(s_pos[(w << 5) + bit], me, r2f, k.keep_boundary) ? (1u << bit)
-                                                                                                 : 0u;
+                            uint32_t m = k.keep_boundary ? word_mask<true>(s_pos + (w << 5), me, r2f)
+                                                         : word_mask<false>(s_pos + (w << 5), me, r2f);
                             if (w == W - 1u && (U & 31u)) m &= (1u << (U & 31u)) - 1u;
                             if (w == (myu >> 5)) m &= ~(1u << (myu & 31u));
                             s_mask[w * kChunk + lane] = m;
@@ -487,15 +534,11 @@ __global__ void __launch_bounds__(kNlThreads) k_nlist_visit(GridDesc g, Tanks tk
                     s_cv[q][lane] = cv;
                 }
                 __syncthreads();
-                // ---- list lengths, this quarter's offsets, the chunk's block
-                uint32_t nv = 0, ov = 0;
+                // ---- list lengths and the chunk's block
+                uint32_t nv = 0;
                 if (active) {
 #pragma unroll
-                    for (uint32_t r = 0; r < kWays; ++r) {
-                        const uint32_t a = s_cv[r][lane];
-                        if (r < q) ov += a;
-                        nv += a;
-                    }
+                    for (uint32_t r = 0; r < kWays; ++r) nv += s_cv[r][lane];
                 }
                 const ChunkBlock blk = reserve_chunk(l, sc, nc, nv, 0u, s_red, &s_blk, &s_overflow);
                 // ---- pass 2: descriptors and entries
@@ -506,23 +549,20 @@ __global__ void __launch_bounds__(kNlThreads) k_nlist_visit(GridDesc g, Tanks tk
                         l.desc[kslot] = blk.ok ? make_uint4(gv, nc, nv, 0u) : make_uint4(0u, 0u, 0u, 0u);
                         l.ncand[kslot] = fluidc ? U : 0u;
                     }
-                    if (blk.ok && fluidc) {
+                    // entries split evenly over the centre's threads
+                    const uint32_t v0 = nv * q / kWays, v1 = nv * (q + 1u) / kWays;
+                    if (blk.ok && fluidc && v0 < v1) {
                         const size_t step = 4u * nc;
                         uint32_t* pv = l.pool + 4 * (size_t)gv;
-                        uint32_t tv = ov;
-                        for (uint32_t w = wb; w < we; ++w) {
-                            uint32_t m = s_mask[w * kChunk + lane];
-                            while (m) {
-                                const uint32_t u = (w << 5) + (__ffs(m) - 1);
-                                m &= m - 1u;
-                                uint32_t e = s_ent[u];
-                                if (LOWER_FLAGS) {
-                                    const uint32_t ow = __float_as_uint(s_pos[u].w);
-                                    if (!(ow & kStageBoundary) && (ow & kStageOrigMask) < myo) e |= kEntryLower;
-                                }
-                                pv[(tv >> 2) * step + (tv & 3u)] = e;
-                                ++tv;
+                        MaskCursor cur(s_mask, s_cv, lane, W, v0);
+                        for (uint32_t t = v0; t < v1; ++t) {
+                            const uint32_t u = cur.next();
+                            uint32_t e = s_ent[u];
+                            if (LOWER_FLAGS) {
+                                const uint32_t ow = __float_as_uint(s_pos[u].w);
+                                if (!(ow & kStageBoundary) && (ow & kStageOrigMask) < myo) e |= kEntryLower;
                             }
+                            pv[(t >> 2) * step + (t & 3u)] = e;
                         }
                     }
                 }
@@ -548,7 +588,7 @@ __global__ void __launch_bounds__(kNlThreads) k_nlist_visit(GridDesc g, Tanks tk
 // s_sorted[ucap]; then a region used first by the radix sort and then by the
 // lower masks over sorted positions.
 template <int DIM>
-__global__ void __launch_bounds__(kNlThreads) k_nlist_both(GridDesc g, Tanks tk, StepConst k, uint32_t ucap,
+__global__ void __launch_bounds__(kNlThreads, 2) k_nlist_both(GridDesc g, Tanks tk, StepConst k, uint32_t ucap,
                                                            const uint32_t* __restrict__ occ,
                                                            const uint32_t* __restrict__ cell_start,
                                                            StateBufs s, ListBufs l, DeviceScalars* sc) {
@@ -586,19 +626,36 @@ __global__ void __launch_bounds__(kNlThreads) k_nlist_both(GridDesc g, Tanks tk,
         const uint32_t U = cu.U;
         max_union = max(max_union, U);
         if (U <= ucap) {
-            for (uint32_t u = tid; u < U; u += blockDim.x) {
-                const uint32_t slot = slot_of_union<NC>(s_off, s_cstart, u);
-                uint8_t fl;
-                uint32_t o;
-                const float4 p = stage_entry<DIM>(s, slot, cu, &fl, &o);
-                s_pos[u] = p;
-                s_ent[u] = slot | entry_flags(__float_as_uint(p.w));
-                if (!(fl & kFlagBoundary)) {
-                    const uint32_t idx = atomicAdd(&s_nf, 1u);
-                    s_sorted[idx] = (uint16_t)u;
-                    atomicMin(&s_omin, o);
-                    atomicMax(&s_omax, o);
+            // Stage the union; fluid entries are appended to s_sorted with one
+            // shared atomic per warp, their index range reduced per warp.
+            uint32_t tmin = 0xffffffffu, tmax = 0u;
+            for (uint32_t u0 = 0; u0 < U; u0 += blockDim.x) {
+                const uint32_t u = u0 + tid;
+                bool fluid = false;
+                if (u < U) {
+                    const uint32_t slot = slot_of_union<NC>(s_off, s_cstart, u);
+                    uint8_t fl;
+                    uint32_t o;
+                    const float4 p = stage_entry<DIM>(s, slot, cu, &fl, &o);
+                    s_pos[u] = p;
+                    s_ent[u] = slot | entry_flags(__float_as_uint(p.w));
+                    fluid = !(fl & kFlagBoundary);
+                    if (fluid) {
+                        tmin = min(tmin, o);
+                        tmax = max(tmax, o);
+                    }
                 }
+                const uint32_t fm = __ballot_sync(0xffffffffu, fluid);
+                uint32_t base = 0;
+                if ((tid & 31u) == 0 && fm) base = atomicAdd(&s_nf, (uint32_t)__popc(fm));
+                base = __shfl_sync(0xffffffffu, base, 0);
+                if (fluid) s_sorted[base + __popc(fm & ((1u << (tid & 31u)) - 1u))] = (uint16_t)u;
+            }
+            tmin = __reduce_min_sync(0xffffffffu, tmin);
+            tmax = __reduce_max_sync(0xffffffffu, tmax);
+            if ((tid & 31u) == 0 && tmin <= tmax) {
+                atomicMin(&s_omin, tmin);
+                atomicMax(&s_omax, tmax);
             }
             __syncthreads();
             const uint32_t nf = s_nf;
@@ -621,11 +678,8 @@ __global__ void __launch_bounds__(kNlThreads) k_nlist_both(GridDesc g, Tanks tk,
                     uint32_t cv = 0;
                     if (fluidc) {
                         for (uint32_t w = wb; w < we; ++w) {
-                            uint32_t m = 0;
-#pragma unroll
-                            for (int bit = 0; bit < 32; ++bit)
-                                m |= keep_entry(s_pos[(w << 5) + bit], me, r2f, k.keep_boundary) ? (1u << bit)
-                                                                                                 : 0u;
+                            uint32_t m = k.keep_boundary ? word_mask<true>(s_pos + (w << 5), me, r2f)
+                                                         : word_mask<false>(s_pos + (w << 5), me, r2f);
                             if (w == W - 1u && (U & 31u)) m &= (1u << (U & 31u)) - 1u;
                             if (w == (myu >> 5)) m &= ~(1u << (myu & 31u));
                             s_vmask[w * kChunk + lane] = m;
@@ -678,18 +732,13 @@ __global__ void __launch_bounds__(kNlThreads) k_nlist_both(GridDesc g, Tanks tk,
                     s_cl[q][lane] = cl;
                 }
                 __syncthreads();
-                // ---- list lengths, this quarter's offsets, the chunk's block
-                uint32_t nv = 0, ov = 0, nl = 0, ol = 0;
+                // ---- list lengths and the chunk's block
+                uint32_t nv = 0, nl = 0;
                 if (active) {
 #pragma unroll
                     for (uint32_t r = 0; r < kWays; ++r) {
-                        const uint32_t a = s_cv[r][lane], b = s_cl[r][lane];
-                        if (r < q) {
-                            ov += a;
-                            ol += b;
-                        }
-                        nv += a;
-                        nl += b;
+                        nv += s_cv[r][lane];
+                        nl += s_cl[r][lane];
                     }
                 }
                 const ChunkBlock blk = reserve_chunk(l, sc, nc, nv, nl, s_red, &s_blk, &s_overflow);
@@ -705,32 +754,27 @@ __global__ void __launch_bounds__(kNlThreads) k_nlist_both(GridDesc g, Tanks tk,
                     }
                     if (blk.ok) {
                         const size_t step = 4u * nc;
-                        if (fluidc) {
+                        // Entries are split evenly over the centre's threads
+                        // (split by words, the middle ways would hold most of
+                        // the kept candidates).
+                        const uint32_t v0 = nv * q / kWays, v1 = nv * (q + 1u) / kWays;
+                        if (fluidc && v0 < v1) {
                             uint32_t* pv = l.pool + 4 * (size_t)gv;
-                            uint32_t tv = ov;
-                            for (uint32_t w = wb; w < we; ++w) {
-                                uint32_t m = s_vmask[w * kChunk + lane];
-                                while (m) {
-                                    const uint32_t u = (w << 5) + (__ffs(m) - 1);
-                                    m &= m - 1u;
-                                    uint32_t e = s_ent[u];
-                                    const uint32_t ow = __float_as_uint(s_pos[u].w);
-                                    if (!(ow & kStageBoundary) && (ow & kStageOrigMask) < myo) e |= kEntryLower;
-                                    pv[(tv >> 2) * step + (tv & 3u)] = e;
-                                    ++tv;
-                                }
+                            MaskCursor cur(s_vmask, s_cv, lane, W, v0);
+                            for (uint32_t t = v0; t < v1; ++t) {
+                                const uint32_t u = cur.next();
+                                uint32_t e = s_ent[u];
+                                const uint32_t ow = __float_as_uint(s_pos[u].w);
+                                if (!(ow & kStageBoundary) && (ow & kStageOrigMask) < myo) e |= kEntryLower;
+                                pv[(t >> 2) * step + (t & 3u)] = e;
                             }
                         }
-                        uint32_t* pl = l.pool + 4 * (size_t)gl;
-                        uint32_t tl = ol;
-                        for (uint32_t w = lb; w < le; ++w) {
-                            uint32_t m = s_lmask[w * kChunk + lane];
-                            while (m) {
-                                const uint32_t i = (w << 5) + (__ffs(m) - 1);
-                                m &= m - 1u;
-                                pl[(tl >> 2) * step + (tl & 3u)] = s_ent[s_sorted[i]] & kEntrySlotMask;
-                                ++tl;
-                            }
+                        const uint32_t l0 = nl * q / kWays, l1 = nl * (q + 1u) / kWays;
+                        if (l0 < l1) {
+                            uint32_t* pl = l.pool + 4 * (size_t)gl;
+                            MaskCursor cur(s_lmask, s_cl, lane, WR, l0);
+                            for (uint32_t t = l0; t < l1; ++t)
+                                pl[(t >> 2) * step + (t & 3u)] = s_ent[s_sorted[cur.next()]] & kEntrySlotMask;
                         }
                     }
                 }
