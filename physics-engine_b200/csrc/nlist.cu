@@ -43,7 +43,12 @@ constexpr int kNlThreads = 256;
 constexpr uint32_t kChunk = 64;                    // centre particles per chunk
 constexpr uint32_t kWays = kNlThreads / kChunk;    // threads per centre particle
 constexpr uint32_t kWarps = kNlThreads / 32;
-constexpr uint32_t kMaxUnionStage = 8192;
+// Largest stage: the fused kernel's 38 dynamic bytes per staged entry (f32
+// position 16, slot 4, sort index 2, visit masks 8, lower masks or sort
+// scratch 8) plus its ~2.4 KB of static shared memory must fit the 227 KB a
+// CTA can opt in to on sm_100 (232,448 bytes).
+constexpr uint32_t kMaxUnionStage = 5888;
+static_assert(38u * kMaxUnionStage + 4096u <= 232448u, "list stage exceeds the shared-memory limit");
 constexpr uint32_t kStageStep = 256;               // stage capacities are multiples of this
 
 // Staged word w of a union entry: original index (29 bits) | kind flags.
