@@ -1,7 +1,8 @@
 """GPU edge cases of the plain WCSPH step against the oracle, bit for bit.
 
 The reference step (crates/pe-fluid/src/wcsph.rs:326-347) has no special
-cases for them, so neither does the oracle: a world of boundary samples only
+cases for them, so neither does the oracle: a world without particles, a
+world of boundary samples only
 (no fluid moves, every density is the boundary's own), a single fluid
 particle without neighbours in free fall inside the wall shell, and a
 neighbour-cell union larger than the list build's shared-memory stage (the
@@ -85,7 +86,7 @@ def test_single_fluid_particle_free_fall_bit_exact():
 def test_union_beyond_the_stage_takes_the_slow_path_bit_exact():
     # 22^3 boundary samples 0.002 m apart with h = 0.02: the block sits in
     # 2 x 2 x 2 cells of 0.04 m, so a cell's 27-cell union (10,648 + the fluid)
-    # exceeds the 8,192-entry shared-memory stage. Eight fluid particles sit
+    # exceeds the 5,888-entry shared-memory stage. Eight fluid particles sit
     # inside it, so the slow path's lists (built per particle from global
     # memory, the lower ones by repeated selection) stay short.
     h, s = 0.02, 0.002
@@ -131,4 +132,19 @@ def test_leaving_the_grid_domain_is_an_error():
         w.step(1e-3)  # 2 m in one step: far past the domain's margin
     assert e.value.code == PE_ERR_BOUNDS
     assert w.status() & pe.STATUS_DOMAIN
+    w.close()
+
+
+def test_empty_world_steps():
+    ps, os_ = _scenes(2 * DX, lambda s: None)
+    prm, op = _params()
+    w = pe.WcsphWorld(ps, prm)
+    o = O.World(os_, op)
+    w.step(1e-4)
+    w.run(1e-4, 7)
+    o.step(1e-4)
+    o.run(1e-4, 7)
+    assert w.t == o.t
+    assert w.positions().shape == (0, 3) and w.densities().shape == (0,)
+    assert w.status() == 0
     w.close()
