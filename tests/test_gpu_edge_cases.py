@@ -6,7 +6,9 @@ world of boundary samples only
 (no fluid moves, every density is the boundary's own), a single fluid
 particle without neighbours in free fall inside the wall shell, and a
 neighbour-cell union larger than the list build's shared-memory stage (the
-build's slow path, flagged by STATUS_SLOW_UNION). A particle that leaves the
+build's slow path, flagged by STATUS_SLOW_UNION; also through the PBF and
+DFSPH steps, whose list modes keep every candidate or every boundary
+candidate). A particle that leaves the
 dense grid domain makes the step return PE_ERR_BOUNDS with STATUS_DOMAIN set
 (the reference's sparse grid has no domain); a non-positive dt is PE_ERR_ARG.
 """
@@ -147,4 +149,74 @@ def test_empty_world_steps():
     assert w.t == o.t
     assert w.positions().shape == (0, 3) and w.densities().shape == (0,)
     assert w.status() == 0
+    w.close()
+
+
+def _dense_block(sc, s):
+    """22^3 boundary samples s apart around eight fluid particles."""
+    g = (0.1 + s * np.arange(22)).tolist()
+    for x in g:
+        for y in g:
+            for z in g:
+                sc.push_boundary((x, y, z), s ** 3)
+    for k in range(8):
+        sc.push_fluid((0.111 + 0.004 * (k & 1), 0.113 + 0.004 * ((k >> 1) & 1), 0.117 + 0.004 * (k >> 2)))
+
+
+def test_pbf_slow_path_bit_exact():
+    """PBF's lists (every candidate kept during the iterations) through the
+    slow path: poly6 support h = 0.02 m, so the block spans ~3^3 cells."""
+    h, s = 0.02, 0.002
+    mass = pe.mass_from_spacing(RHO0, s, 3)
+    ps, os_ = pe.Particles(3, RHO0, mass, h), O.Scene(3, RHO0, mass, h)
+    _dense_block(ps, s)
+    _dense_block(os_, s)
+    p = pe.PbfParams(iterations=2, art_pressure_k=0.0)
+    q = O.pbf_default_params()
+    for k in pe.PbfParams._FIELDS:
+        v = getattr(p, k)
+        if k == "gravity":
+            q.gravity[:] = v
+        else:
+            setattr(q, k, int(v) if isinstance(v, bool) else v)
+    w, o = pe.PbfWorld(ps, p), O.PbfWorld(os_, q)
+    w.step(1e-6)
+    o.step(1e-6)
+    assert_bits_equal(w.positions(), o.x(), "pbf slow path x")
+    assert_bits_equal(w.velocities(), o.v(), "pbf slow path v")
+    assert_bits_equal(w.densities(), o.rho(), "pbf slow path rho")
+    assert w.status() & pe.STATUS_SLOW_UNION
+    w.close()
+
+
+def test_dfsph_slow_path_bit_exact():
+    """DFSPH's visit lists (boundary candidates kept) and the boundary slots'
+    ascending fluid lists through the slow path."""
+    h, s = 0.02, 0.002
+    mass = pe.mass_from_spacing(RHO0, s, 3)
+    ps, os_ = pe.Particles(3, RHO0, mass, h), O.Scene(3, RHO0, mass, h)
+    _dense_block(ps, s)
+    _dense_block(os_, s)
+    p = pe.DfsphParams(adaptive_dt=False, particle_diameter=s, max_density_iters=3, max_divergence_iters=3)
+    q = O.dfsph_default_params()
+    q.kernel = p.kernel
+    q.max_density_iters, q.max_divergence_iters = p.max_density_iters, p.max_divergence_iters
+    q.density_error_tol, q.divergence_error_tol = p.density_error_tol, p.divergence_error_tol
+    q.gravity[:] = p.gravity
+    q.xsph_epsilon, q.particle_diameter, q.cfl_lambda = p.xsph_epsilon, p.particle_diameter, p.cfl_lambda
+    q.adaptive_dt, q.warm_start = int(p.adaptive_dt), int(p.warm_start)
+    for a, k in enumerate(pe.DfsphParams._SLIPS):
+        v = getattr(p, k)
+        q.has_slip[a] = 0 if v is None else 1
+        q.slip[a] = 0.0 if v is None else v
+    q.solver_omega, q.max_velocity_correction = p.solver_omega, p.max_velocity_correction
+    w, o = pe.DfsphWorld(ps, p), O.DfsphWorld(os_, q)
+    w.step(1e-6)
+    o.step(1e-6)
+    assert_bits_equal(w.positions(), o.x(), "dfsph slow path x")
+    assert_bits_equal(w.velocities(), o.v(), "dfsph slow path v")
+    assert_bits_equal(w.densities(), o.rho(), "dfsph slow path rho")
+    assert_bits_equal(w.boundary_forces(), o.boundary_force(), "dfsph slow path boundary force")
+    assert w.last_iterations() == o.iterations()
+    assert w.status() & pe.STATUS_SLOW_UNION
     w.close()
