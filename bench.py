@@ -55,6 +55,8 @@ FORCE_OPS_PER_PAIR = 65.0
 FORCE_TRAFFIC_PER_FLUID = (427.182848e6 + 20.532480e6) / 262144
 # sm__pipe_fp64_cycles_active of the force pass in the same capture
 FORCE_FP64_PIPE_ACTIVE = 0.550
+# smsp__issue_active of the list build (k_nlist_both) in the same capture
+LISTS_ISSUE_ACTIVE = 0.486
 # Whole step, per fluid / per boundary particle (cell key 28 + sort 8 +
 # density 32 + XSPH 80 + forces 104; boundary 28 + 8 + 3 x 24).
 STEP_BYTES_FLUID, STEP_BYTES_BOUNDARY = 252.0, 108.0
@@ -747,6 +749,9 @@ def main():
     hbm_peak, peak_kind = _peaks()
     f_ms, f_n = prof["forces"]
     achieved = FORCE_BYTES_PER_FLUID * nf * f_n / (f_ms / 1e3) / 1e9 if f_ms > 0 else 0.0
+    l_ms, l_n = prof["lists"]
+    # list pool groups used by one build (16 B each) + per-slot descriptors (uint4 + uint2 + u32)
+    list_bytes = cap["list_groups_used"] * 16 + (nf + nb) * (16 + 8 + 4)
     # FP64 axis: visited in-support pairs of the force pass against the
     # device's measured non-fused FP64 issue rate
     _, in_sup = world.neighbour_counts()
@@ -789,6 +794,18 @@ def main():
                           "ncu_fp64_pipe_active": FORCE_FP64_PIPE_ACTIVE,
                           "note": "pairs are visited (ordered) in-support pairs: the gather evaluates each "
                                   "fluid pair from both sides, the reference's scatter once"},
+        # The list build is the largest kernel by time but has no algorithmic
+        # work in the step's byte or FLOP model (its ~1,700 candidate tests per
+        # fluid particle are the builder's overhead); its DRAM traffic is
+        # about the lists it writes, and it is issue bound (no FP64).
+        "roofline_lists": {"bound": "issue", "kernel": "k_nlist_both (visit + lower lists)",
+                           "achieved": list_bytes / (l_ms / max(1, l_n) / 1e3) / 1e9 if l_ms > 0 else None,
+                           "peak": hbm_peak, "unit": "GB/s",
+                           "frac": (list_bytes / (l_ms / max(1, l_n) / 1e3) / 1e9 / hbm_peak) if l_ms > 0 else None,
+                           "peak_kind": peak_kind, "bytes_per_launch": list_bytes,
+                           "launch_ms": l_ms / max(1, l_n), "ncu_issue_active": LISTS_ISSUE_ACTIVE,
+                           "note": "bytes = the list entries and descriptors written per build; issue bound, "
+                                   "not HBM bound"},
         "step_roofline": {"algorithmic_bytes_per_step": step_bytes,
                           "achieved_gbs": step_bytes / (ms / args.steps / 1e3) / 1e9,
                           "profiled_ms_per_step": total_prof / max(1, args.steps)},
