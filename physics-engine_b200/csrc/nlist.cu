@@ -52,7 +52,7 @@ static_assert(38u * kMaxUnionStage + 4096u <= 232448u, "list stage exceeds the s
 constexpr uint32_t kStageStep = 256;               // stage capacities are multiples of this
 
 // Staged word w of a union entry: original index (29 bits) | kind flags.
-constexpr uint32_t kStageBoundary = 1u << 31;
+constexpr uint32_t kStageBoundary = 1u << 31;  // the sign bit (word_mask reads it so)
 constexpr uint32_t kStageOriented = 1u << 30;
 constexpr uint32_t kStageOrigMask = (1u << 29) - 1u;
 
@@ -182,15 +182,78 @@ __device__ __forceinline__ bool keep_entry(const float4& q, const float4& me, fl
     return within(q, me, r2f) || (keep_boundary && (__float_as_uint(q.w) & kStageBoundary));
 }
 
-// Keep mask of the 32 staged entries at q (keep_entry per bit).
+// The staged union in shared memory as four float arrays (cell-local x, y, z
+// and the staged word orig | kind flags), so that the candidates of a word can
+// be read four at a time per coordinate.
+struct Stage {
+    float *x, *y, *z, *w;
+    __device__ __forceinline__ Stage(float* base, uint32_t ucap)
+        : x(base), y(base + ucap), z(base + 2 * ucap), w(base + 3 * ucap) {}
+    __device__ __forceinline__ float4 get(uint32_t u) const { return make_float4(x[u], y[u], z[u], w[u]); }
+    __device__ __forceinline__ void put(uint32_t u, const float4& p) {
+        x[u] = p.x;
+        y[u] = p.y;
+        z[u] = p.z;
+        w[u] = p.w;
+    }
+    __device__ __forceinline__ uint32_t word(uint32_t u) const { return __float_as_uint(w[u]); }
+};
+
+// Packed single-precision pairs (two f32 in one 64-bit register) and the
+// sm_100 paired arithmetic on them, each half rounded to nearest like the
+// scalar instruction.
+__device__ __forceinline__ unsigned long long f2_pack(float lo, float hi) {
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ void f2_unpack(unsigned long long v, float& lo, float& hi) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ unsigned long long f2_sub(unsigned long long a, unsigned long long b) {
+    unsigned long long r;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ unsigned long long f2_mul(unsigned long long a, unsigned long long b) {
+    unsigned long long r;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ unsigned long long f2_fma(unsigned long long a, unsigned long long b,
+                                                     unsigned long long c) {
+    unsigned long long r;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+    return r;
+}
+
+// Keep mask of the 32 staged entries from position base (keep_entry per bit):
+// four candidates per 16-byte read of each coordinate, their squared
+// distances in two packed pairs (dx dx + dy dy + dz dz, as the scalar test).
 template <bool KEEP_BOUNDARY>
-__device__ __forceinline__ uint32_t word_mask(const float4* q, const float4& me, float r2f) {
+__device__ __forceinline__ uint32_t word_mask(const Stage& st, uint32_t base, const float4& me, float r2f) {
+    const unsigned long long mx = f2_pack(me.x, me.x), my = f2_pack(me.y, me.y), mz = f2_pack(me.z, me.z);
     uint32_t m = 0;
 #pragma unroll
-    for (int bit = 0; bit < 32; ++bit) {
-        const float4 e = q[bit];
-        const bool keep = within(e, me, r2f) || (KEEP_BOUNDARY && (__float_as_uint(e.w) & kStageBoundary));
-        m |= keep ? (1u << bit) : 0u;
+    for (int g = 0; g < 8; ++g) {
+        const float4 X = *reinterpret_cast<const float4*>(st.x + base + 4 * g);
+        const float4 Y = *reinterpret_cast<const float4*>(st.y + base + 4 * g);
+        const float4 Z = *reinterpret_cast<const float4*>(st.z + base + 4 * g);
+        const unsigned long long dx0 = f2_sub(f2_pack(X.x, X.y), mx), dx1 = f2_sub(f2_pack(X.z, X.w), mx);
+        const unsigned long long dy0 = f2_sub(f2_pack(Y.x, Y.y), my), dy1 = f2_sub(f2_pack(Y.z, Y.w), my);
+        const unsigned long long dz0 = f2_sub(f2_pack(Z.x, Z.y), mz), dz1 = f2_sub(f2_pack(Z.z, Z.w), mz);
+        const unsigned long long r0 = f2_fma(dz0, dz0, f2_fma(dy0, dy0, f2_mul(dx0, dx0)));
+        const unsigned long long r1 = f2_fma(dz1, dz1, f2_fma(dy1, dy1, f2_mul(dx1, dx1)));
+        float a, b, c, d;
+        f2_unpack(r0, a, b);
+        f2_unpack(r1, c, d);
+        uint32_t k4 = (a <= r2f ? 1u : 0u) | (b <= r2f ? 2u : 0u) | (c <= r2f ? 4u : 0u) | (d <= r2f ? 8u : 0u);
+        if (KEEP_BOUNDARY) {
+            const float4 W = *reinterpret_cast<const float4*>(st.w + base + 4 * g);
+            k4 |= ((__float_as_uint(W.x) >> 31) & 1u) | (((__float_as_uint(W.y) >> 31) & 1u) << 1) |
+                  (((__float_as_uint(W.z) >> 31) & 1u) << 2) | (((__float_as_uint(W.w) >> 31) & 1u) << 3);
+        }
+        m |= k4 << (4 * g);
     }
     return m;
 }
@@ -270,7 +333,7 @@ __device__ __forceinline__ ChunkBlock reserve_chunk(const ListBufs& l, DeviceSca
 // index, on 4-bit digits of (orig - omin); keys are read through the staged
 // positions. The keys are unique, so the result does not depend on the
 // staging order. Ends with a block barrier.
-__device__ __forceinline__ void radix_sort_by_orig(const float4* s_pos, uint16_t* s_sorted, uint16_t* s_tmp,
+__device__ __forceinline__ void radix_sort_by_orig(const float* s_w, uint16_t* s_sorted, uint16_t* s_tmp,
                                                    uint16_t* s_cnt, uint32_t nf, uint32_t omin, uint32_t omax) {
     const uint32_t tid = threadIdx.x;
     const uint32_t span = nf ? omax - omin : 0u;
@@ -283,7 +346,7 @@ __device__ __forceinline__ void radix_sort_by_orig(const float4* s_pos, uint16_t
 #pragma unroll
         for (int d = 0; d < 16; ++d) s_cnt[d * kNlThreads + tid] = 0;
         for (uint32_t e = e0; e < e1; ++e) {
-            const uint32_t o = __float_as_uint(s_pos[src[e]].w) & kStageOrigMask;
+            const uint32_t o = __float_as_uint(s_w[src[e]]) & kStageOrigMask;
             ++s_cnt[(((o - omin) >> shift) & 15u) * kNlThreads + tid];
         }
         __syncthreads();
@@ -312,7 +375,7 @@ __device__ __forceinline__ void radix_sort_by_orig(const float4* s_pos, uint16_t
         __syncthreads();
         for (uint32_t e = e0; e < e1; ++e) {
             const uint16_t pu = src[e];
-            const uint32_t o = __float_as_uint(s_pos[pu].w) & kStageOrigMask;
+            const uint32_t o = __float_as_uint(s_w[pu]) & kStageOrigMask;
             dst[s_cnt[(((o - omin) >> shift) & 15u) * kNlThreads + tid]++] = pu;
         }
         __syncthreads();
@@ -469,7 +532,7 @@ __device__ __forceinline__ void lower_slow(const StepConst& k, float r2f, const 
 }
 
 // ----------------------------------------------------------------- visit
-// Dynamic shared memory (ucap a multiple of kStageStep): float4 s_pos[ucap];
+// Dynamic shared memory (ucap a multiple of kStageStep): float x, y, z, w[ucap] (Stage);
 // uint32 s_ent[ucap]; uint32 s_mask[(ucap / 32) * kChunk] (word w of chunk
 // lane c at s_mask[w * kChunk + c]).
 template <int DIM, bool LOWER_FLAGS>
@@ -480,8 +543,8 @@ __global__ void __launch_bounds__(kNlThreads) k_nlist_visit(GridDesc g, Tanks tk
                                                             DeviceScalars* sc) {
     constexpr int NC = DIM == 3 ? 27 : 9;
     extern __shared__ __align__(16) unsigned char smem[];
-    float4* s_pos = reinterpret_cast<float4*>(smem);
-    uint32_t* s_ent = reinterpret_cast<uint32_t*>(s_pos + ucap);
+    Stage st(reinterpret_cast<float*>(smem), ucap);
+    uint32_t* s_ent = reinterpret_cast<uint32_t*>(smem) + 4 * (size_t)ucap;
     uint32_t* s_mask = s_ent + ucap;
     __shared__ uint32_t s_cstart[NC];
     __shared__ uint32_t s_off[NC + 1];
@@ -507,7 +570,7 @@ __global__ void __launch_bounds__(kNlThreads) k_nlist_visit(GridDesc g, Tanks tk
                 uint8_t fl;
                 uint32_t o;
                 const float4 p = stage_entry<DIM>(s, slot, cu, &fl, &o);
-                s_pos[u] = p;
+                st.put(u, p);
                 s_ent[u] = slot | entry_flags(__float_as_uint(p.w));
             }
             __syncthreads();
@@ -521,15 +584,15 @@ __global__ void __launch_bounds__(kNlThreads) k_nlist_visit(GridDesc g, Tanks tk
                 uint32_t myo = 0;
                 // ---- pass 1: in-support masks of this quarter's words, counts
                 if (active) {
-                    const float4 me = s_pos[myu];
+                    const float4 me = st.get(myu);
                     const uint32_t mw = __float_as_uint(me.w);
                     fluidc = !(mw & kStageBoundary);
                     myo = mw & kStageOrigMask;
                     uint32_t cv = 0;
                     if (fluidc) {
                         for (uint32_t w = wb; w < we; ++w) {
-                            uint32_t m = k.keep_boundary ? word_mask<true>(s_pos + (w << 5), me, r2f)
-                                                         : word_mask<false>(s_pos + (w << 5), me, r2f);
+                            uint32_t m = k.keep_boundary ? word_mask<true>(st, w << 5, me, r2f)
+                                                         : word_mask<false>(st, w << 5, me, r2f);
                             if (w == W - 1u && (U & 31u)) m &= (1u << (U & 31u)) - 1u;
                             if (w == (myu >> 5)) m &= ~(1u << (myu & 31u));
                             s_mask[w * kChunk + lane] = m;
@@ -564,7 +627,7 @@ __global__ void __launch_bounds__(kNlThreads) k_nlist_visit(GridDesc g, Tanks tk
                             const uint32_t u = cur.next();
                             uint32_t e = s_ent[u];
                             if (LOWER_FLAGS) {
-                                const uint32_t ow = __float_as_uint(s_pos[u].w);
+                                const uint32_t ow = st.word(u);
                                 if (!(ow & kStageBoundary) && (ow & kStageOrigMask) < myo) e |= kEntryLower;
                             }
                             pv[(t >> 2) * step + (t & 3u)] = e;
@@ -588,7 +651,7 @@ __global__ void __launch_bounds__(kNlThreads) k_nlist_visit(GridDesc g, Tanks tk
 // centre's lower list is read out of its own visit mask in ascending original
 // index (through the radix-sorted fluid positions); boundary centres test the
 // sorted fluid positions directly. One reservation per chunk holds both lists
-// (visit rows first). Dynamic shared memory: float4 s_pos[ucap]; uint32
+// (visit rows first). Dynamic shared memory: float x, y, z, w[ucap] (Stage); uint32
 // s_ent[ucap] (slot | flags); uint32 s_vmask[(ucap / 32) * kChunk]; uint16
 // s_sorted[ucap]; then a region used first by the radix sort and then by the
 // lower masks over sorted positions.
@@ -599,8 +662,8 @@ __global__ void __launch_bounds__(kNlThreads, 2) k_nlist_both(GridDesc g, Tanks 
                                                            StateBufs s, ListBufs l, DeviceScalars* sc) {
     constexpr int NC = DIM == 3 ? 27 : 9;
     extern __shared__ __align__(16) unsigned char smem[];
-    float4* s_pos = reinterpret_cast<float4*>(smem);
-    uint32_t* s_ent = reinterpret_cast<uint32_t*>(s_pos + ucap);
+    Stage st(reinterpret_cast<float*>(smem), ucap);
+    uint32_t* s_ent = reinterpret_cast<uint32_t*>(smem) + 4 * (size_t)ucap;
     uint32_t* s_vmask = s_ent + ucap;
     uint16_t* s_sorted = reinterpret_cast<uint16_t*>(s_vmask + (ucap / 32) * kChunk);
     uint32_t* s_lmask = reinterpret_cast<uint32_t*>(s_sorted + ucap);
@@ -642,7 +705,7 @@ __global__ void __launch_bounds__(kNlThreads, 2) k_nlist_both(GridDesc g, Tanks 
                     uint8_t fl;
                     uint32_t o;
                     const float4 p = stage_entry<DIM>(s, slot, cu, &fl, &o);
-                    s_pos[u] = p;
+                    st.put(u, p);
                     s_ent[u] = slot | entry_flags(__float_as_uint(p.w));
                     fluid = !(fl & kFlagBoundary);
                     if (fluid) {
@@ -664,7 +727,7 @@ __global__ void __launch_bounds__(kNlThreads, 2) k_nlist_both(GridDesc g, Tanks 
             }
             __syncthreads();
             const uint32_t nf = s_nf;
-            radix_sort_by_orig(s_pos, s_sorted, s_tmp, s_cnt, nf, s_omin, s_omax);
+            radix_sort_by_orig(st.w, s_sorted, s_tmp, s_cnt, nf, s_omin, s_omax);
             const uint32_t W = (U + 31u) >> 5;
             const uint32_t wb = W * q / kWays, we = W * (q + 1) / kWays;
             for (uint32_t c0 = 0; c0 < cu.ncenter; c0 += kChunk) {
@@ -676,15 +739,15 @@ __global__ void __launch_bounds__(kNlThreads, 2) k_nlist_both(GridDesc g, Tanks 
                 float4 me = make_float4(0.f, 0.f, 0.f, 0.f);
                 // ---- pass 1a: visit masks of this quarter's union words (fluid centres)
                 if (active) {
-                    me = s_pos[myu];
+                    me = st.get(myu);
                     const uint32_t mw = __float_as_uint(me.w);
                     fluidc = !(mw & kStageBoundary);
                     myo = mw & kStageOrigMask;
                     uint32_t cv = 0;
                     if (fluidc) {
                         for (uint32_t w = wb; w < we; ++w) {
-                            uint32_t m = k.keep_boundary ? word_mask<true>(s_pos + (w << 5), me, r2f)
-                                                         : word_mask<false>(s_pos + (w << 5), me, r2f);
+                            uint32_t m = k.keep_boundary ? word_mask<true>(st, w << 5, me, r2f)
+                                                         : word_mask<false>(st, w << 5, me, r2f);
                             if (w == W - 1u && (U & 31u)) m &= (1u << (U & 31u)) - 1u;
                             if (w == (myu >> 5)) m &= ~(1u << (myu & 31u));
                             s_vmask[w * kChunk + lane] = m;
@@ -700,7 +763,7 @@ __global__ void __launch_bounds__(kNlThreads, 2) k_nlist_both(GridDesc g, Tanks 
                         uint32_t lo = 0, hi = nf;
                         while (lo < hi) {
                             const uint32_t mid = (lo + hi) >> 1;
-                            const uint32_t o = __float_as_uint(s_pos[s_sorted[mid]].w) & kStageOrigMask;
+                            const uint32_t o = st.word(s_sorted[mid]) & kStageOrigMask;
                             if (o < myo) lo = mid + 1;
                             else hi = mid;
                         }
@@ -727,7 +790,7 @@ __global__ void __launch_bounds__(kNlThreads, 2) k_nlist_both(GridDesc g, Tanks 
 #pragma unroll
                             for (int bit = 0; bit < 32; ++bit) {
                                 const uint32_t i = (w << 5) + bit;
-                                m |= within(s_pos[s_sorted[i < nf ? i : 0u]], me, r2c) ? (1u << bit) : 0u;
+                                m |= within(st.get(s_sorted[i < nf ? i : 0u]), me, r2c) ? (1u << bit) : 0u;
                             }
                         }
                         if (w == WR - 1u && (R & 31u)) m &= (1u << (R & 31u)) - 1u;
@@ -769,7 +832,7 @@ __global__ void __launch_bounds__(kNlThreads, 2) k_nlist_both(GridDesc g, Tanks 
                             for (uint32_t t = v0; t < v1; ++t) {
                                 const uint32_t u = cur.next();
                                 uint32_t e = s_ent[u];
-                                const uint32_t ow = __float_as_uint(s_pos[u].w);
+                                const uint32_t ow = st.word(u);
                                 if (!(ow & kStageBoundary) && (ow & kStageOrigMask) < myo) e |= kEntryLower;
                                 pv[(t >> 2) * step + (t & 3u)] = e;
                             }
