@@ -728,6 +728,11 @@ __global__ void __launch_bounds__(kNlThreads, 2) k_nlist_both(GridDesc g, Tanks 
             __syncthreads();
             const uint32_t nf = s_nf;
             radix_sort_by_orig(st.w, s_sorted, s_tmp, s_cnt, nf, s_omin, s_omax);
+            // sorted positions past nf up to the next multiple of 32 read as
+            // union position 0: the lower-mask pass reads whole words (their
+            // bits past a centre's prefix are cleared)
+            for (uint32_t i = nf + tid; i < ((nf + 31u) & ~31u); i += blockDim.x) s_sorted[i] = 0;
+            __syncthreads();
             const uint32_t W = (U + 31u) >> 5;
             const uint32_t wb = W * q / kWays, we = W * (q + 1) / kWays;
             for (uint32_t c0 = 0; c0 < cu.ncenter; c0 += kChunk) {
@@ -780,17 +785,22 @@ __global__ void __launch_bounds__(kNlThreads, 2) k_nlist_both(GridDesc g, Tanks 
                     for (uint32_t w = lb; w < le; ++w) {
                         uint32_t m = 0;
                         if (fluidc) {
-#pragma unroll 8
-                            for (int bit = 0; bit < 32; ++bit) {
-                                const uint32_t i = (w << 5) + bit;
-                                const uint32_t u = s_sorted[i < nf ? i : 0u];
-                                m |= ((s_vmask[(u >> 5) * kChunk + lane] >> (u & 31u)) & 1u) << bit;
+                            const uint4* sw = reinterpret_cast<const uint4*>(s_sorted + (w << 5));
+#pragma unroll
+                            for (int v = 0; v < 4; ++v) {
+                                const uint4 x = sw[v];
+                                const uint32_t pr[4] = {x.x, x.y, x.z, x.w};
+#pragma unroll
+                                for (int h = 0; h < 8; ++h) {
+                                    const uint32_t u = (pr[h >> 1] >> ((h & 1) * 16)) & 0xffffu;
+                                    m |= ((s_vmask[(u >> 5) * kChunk + lane] >> (u & 31u)) & 1u) << (v * 8 + h);
+                                }
                             }
                         } else {
 #pragma unroll
                             for (int bit = 0; bit < 32; ++bit) {
                                 const uint32_t i = (w << 5) + bit;
-                                m |= within(st.get(s_sorted[i < nf ? i : 0u]), me, r2c) ? (1u << bit) : 0u;
+                                m |= within(st.get(s_sorted[i]), me, r2c) ? (1u << bit) : 0u;
                             }
                         }
                         if (w == WR - 1u && (R & 31u)) m &= (1u << (R & 31u)) - 1u;
