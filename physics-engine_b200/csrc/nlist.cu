@@ -628,7 +628,7 @@ __global__ void __launch_bounds__(kNlThreads) k_nlist_visit(GridDesc g, Tanks tk
                             uint32_t e = s_ent[u];
                             if (LOWER_FLAGS) {
                                 const uint32_t ow = st.word(u);
-                                if (!(ow & kStageBoundary) && (ow & kStageOrigMask) < myo) e |= kEntryLower;
+                                e |= ow < myo ? kEntryLower : 0u;  // a boundary word has bit 31 set
                             }
                             pv[(t >> 2) * step + (t & 3u)] = e;
                         }
@@ -843,7 +843,7 @@ __global__ void __launch_bounds__(kNlThreads, 2) k_nlist_both(GridDesc g, Tanks 
                                 const uint32_t u = cur.next();
                                 uint32_t e = s_ent[u];
                                 const uint32_t ow = st.word(u);
-                                if (!(ow & kStageBoundary) && (ow & kStageOrigMask) < myo) e |= kEntryLower;
+                                e |= ow < myo ? kEntryLower : 0u;  // a boundary word has bit 31 set
                                 pv[(t >> 2) * step + (t & 3u)] = e;
                             }
                         }
