@@ -330,24 +330,37 @@ __device__ __forceinline__ ChunkBlock reserve_chunk(const ListBufs& l, DeviceSca
 }
 
 // LSD radix sort of a union's fluid positions (s_sorted[0..nf)) by original
-// index, on 4-bit digits of (orig - omin); keys are read through the staged
-// positions. The keys are unique, so the result does not depend on the
-// staging order. Ends with a block barrier.
+// index, on 9-bit digits of (orig - omin) (two passes for spans below 2^18);
+// keys are read through the staged words. Warp w ranks the w-th contiguous
+// segment of the array, 32 entries at a time in order, grouping equal digits
+// with a match, so every pass is stable; counter (digit, warp) is
+// s_cnt[digit * kWarps + warp] and one exclusive scan over them in that order
+// gives each group its start. The keys are unique, so the result does not
+// depend on the staging order. Ends with a block barrier.
+constexpr int kRadixBits = 9;
+constexpr uint32_t kRadixDigits = 1u << kRadixBits;
+static_assert(kRadixDigits * kWarps == 16 * kNlThreads, "radix counters fill the scan's 16 per thread");
+
 __device__ __forceinline__ void radix_sort_by_orig(const float* s_w, uint16_t* s_sorted, uint16_t* s_tmp,
                                                    uint16_t* s_cnt, uint32_t nf, uint32_t omin, uint32_t omax) {
-    const uint32_t tid = threadIdx.x;
+    const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
     const uint32_t span = nf ? omax - omin : 0u;
-    const int npass = span ? (32 - __clz(span) + 3) / 4 : 0;
-    const uint32_t chunk = (nf + kNlThreads - 1) / kNlThreads;
-    const uint32_t e0 = min(nf, tid * chunk), e1 = min(nf, e0 + chunk);
+    const int npass = span ? (32 - __clz(span) + kRadixBits - 1) / kRadixBits : 0;
+    const uint32_t seg = ((nf + kWarps - 1) / kWarps + 31u) & ~31u;
+    const uint32_t e0 = min(nf, warp * seg), e1 = min(nf, e0 + seg);
     uint16_t *src = s_sorted, *dst = s_tmp;
     for (int pass = 0; pass < npass; ++pass) {
-        const int shift = 4 * pass;
-#pragma unroll
-        for (int d = 0; d < 16; ++d) s_cnt[d * kNlThreads + tid] = 0;
-        for (uint32_t e = e0; e < e1; ++e) {
-            const uint32_t o = __float_as_uint(s_w[src[e]]) & kStageOrigMask;
-            ++s_cnt[(((o - omin) >> shift) & 15u) * kNlThreads + tid];
+        const int shift = kRadixBits * pass;
+        for (uint32_t i = tid; i < kRadixDigits * kWarps; i += blockDim.x) s_cnt[i] = 0;
+        __syncthreads();
+        for (uint32_t b = e0; b < e1; b += 32u) {
+            const uint32_t e = b + lane;
+            const bool valid = e < e1;
+            uint32_t d = kRadixDigits;  // lanes past the segment: a digit of their own
+            if (valid) d = (((__float_as_uint(s_w[src[e]]) & kStageOrigMask) - omin) >> shift) & (kRadixDigits - 1u);
+            const uint32_t peers = __match_any_sync(0xffffffffu, d);
+            if (valid && lane == (uint32_t)(__ffs(peers) - 1)) s_cnt[d * kWarps + warp] += (uint16_t)__popc(peers);
+            __syncwarp();
         }
         __syncthreads();
         {
@@ -373,10 +386,24 @@ __device__ __forceinline__ void radix_sort_by_orig(const float* s_w, uint16_t* s
             cw[1] = make_uint4(out[4], out[5], out[6], out[7]);
         }
         __syncthreads();
-        for (uint32_t e = e0; e < e1; ++e) {
-            const uint16_t pu = src[e];
-            const uint32_t o = __float_as_uint(s_w[pu]) & kStageOrigMask;
-            dst[s_cnt[(((o - omin) >> shift) & 15u) * kNlThreads + tid]++] = pu;
+        for (uint32_t b = e0; b < e1; b += 32u) {
+            const uint32_t e = b + lane;
+            const bool valid = e < e1;
+            uint32_t d = kRadixDigits;
+            uint16_t pu = 0;
+            if (valid) {
+                pu = src[e];
+                d = (((__float_as_uint(s_w[pu]) & kStageOrigMask) - omin) >> shift) & (kRadixDigits - 1u);
+            }
+            const uint32_t peers = __match_any_sync(0xffffffffu, d);
+            uint32_t base = 0;
+            if (valid) {
+                base = s_cnt[d * kWarps + warp];
+                dst[base + __popc(peers & ((1u << lane) - 1u))] = pu;
+            }
+            __syncwarp();
+            if (valid && lane == (uint32_t)(__ffs(peers) - 1)) s_cnt[d * kWarps + warp] = (uint16_t)(base + __popc(peers));
+            __syncwarp();
         }
         __syncthreads();
         uint16_t* t = src;
