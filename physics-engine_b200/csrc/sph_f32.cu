@@ -11,6 +11,7 @@
 // re-expressed against the new cell after each sort). This form does not
 // reproduce the reference's bits; `bench.py --form f32` reports its error
 // against the f64 path.
+#include "list_iter.cuh"
 #include "pe_math.cuh"
 #include "wcsph_device.cuh"
 
@@ -70,11 +71,12 @@ __device__ __forceinline__ bool sees_fluid_f32(const F32Const& k, const double4&
     return -(d.x * nx + d.y * ny + d.z * nz) > -eps;
 }
 
-template <class F>
-__device__ __forceinline__ void for_each_visit(const ListBufs& l, uint32_t s, F&& f) {
-    const ListRef r = list_ref(l, s, kListVisit);
-    for (uint32_t t = 0; t < r.n; ++t) f(__ldg(r.p + (size_t)(t >> 2) * r.step + (t & 3u)));
-}
+// A neighbour's loop state, gathered one entry ahead of its use.
+struct Nb32 {
+    float4 p;
+    int4 key;
+    float4 v;
+};
 
 __global__ void __launch_bounds__(kMaxPassThreads) k_density_f32(uint32_t n, F32Const k, StateBufs s,
                                                           F32Bufs f, ListBufs l) {
@@ -88,15 +90,22 @@ __global__ void __launch_bounds__(kMaxPassThreads) k_density_f32(uint32_t n, F32
     const int4 ki = s.key[i];
     Kahan rho;
     rho.add(k.rho_self);
-    for_each_visit(l, i, [&](uint32_t e) {
-        const uint32_t j = e & kEntrySlotMask;
-        const float4 pj = f.pos[j];
-        const float3 d = rel(ki, pi, s.key[j], pj, k.cell);
-        if ((e & kEntryOriented) && !sees_fluid_f32(k, s.nout[j], d)) return;
-        const float r = sqrtf(d.x * d.x + d.y * d.y + d.z * d.z);
-        const float w = w_f32(r, k);
-        rho.add(((e & kEntryBoundary) ? k.rho0 * pj.w : k.mass) * w);
-    });
+    for_each_loaded(
+        list_ref(l, i, kListVisit),
+        [&](uint32_t e) {
+            Nb32 b;
+            b.p = f.pos[e & kEntrySlotMask];
+            b.key = s.key[e & kEntrySlotMask];
+            return b;
+        },
+        [&](uint32_t e, const Nb32& b) {
+            const float4 pj = b.p;
+            const float3 d = rel(ki, pi, b.key, pj, k.cell);
+            if ((e & kEntryOriented) && !sees_fluid_f32(k, s.nout[e & kEntrySlotMask], d)) return;
+            const float r = sqrtf(d.x * d.x + d.y * d.y + d.z * d.z);
+            const float w = w_f32(r, k);
+            rho.add(((e & kEntryBoundary) ? k.rho0 * pj.w : k.mass) * w);
+        });
     const float r = fmaxf(rho.s, 1e-12f);
     f.vel[i].w = r;
     s.vel[i].w = (double)r;
@@ -174,10 +183,17 @@ __global__ void __launch_bounds__(kMaxPassThreads) k_forces_f32(uint32_t n, F32C
     const float4 vi = f.vel[i];
     const int4 ki = s.key[i];
     Kahan ax, ay, az;
-    for_each_visit(l, i, [&](uint32_t e) {
+    auto load = [&](uint32_t e) {
+        Nb32 b;
+        b.p = f.pos[e & kEntrySlotMask];
+        b.key = s.key[e & kEntrySlotMask];
+        b.v = f.vel[e & kEntrySlotMask];
+        return b;
+    };
+    for_each_loaded(list_ref(l, i, kListVisit), load, [&](uint32_t e, const Nb32& b) {
         const uint32_t j = e & kEntrySlotMask;
-        const float4 pj = f.pos[j];
-        const float3 d = rel(ki, pi, s.key[j], pj, k.cell);  // x_j - x_i
+        const float4 pj = b.p;
+        const float3 d = rel(ki, pi, b.key, pj, k.cell);  // x_j - x_i
         const float r2 = d.x * d.x + d.y * d.y + d.z * d.z;
         if (r2 < 1e-30f) return;
         const float inv_r = rsqrtf(r2);
@@ -197,7 +213,7 @@ __global__ void __launch_bounds__(kMaxPassThreads) k_forces_f32(uint32_t n, F32C
             }
             return;
         }
-        const float4 vj = f.vel[j];
+        const float4 vj = b.v;
         const float press = pi.w + pj.w;
         const float vr = (vi.x - vj.x) * -d.x + (vi.y - vj.y) * -d.y + (vi.z - vj.z) * -d.z;
         float pic = 0.f;
@@ -237,14 +253,22 @@ __global__ void __launch_bounds__(kMaxPassThreads) k_xsph_f32(uint32_t n, F32Con
     const float4 pi = f.pos[i];
     const int4 ki = s.key[i];
     Kahan dx, dy, dz;
-    for_each_visit(l, i, [&](uint32_t e) {
+    auto load = [&](uint32_t e) {
+        Nb32 b{};
+        if (!(e & kEntryBoundary)) {
+            b.p = f.pos[e & kEntrySlotMask];
+            b.key = s.key[e & kEntrySlotMask];
+            b.v = f.vel[e & kEntrySlotMask];
+        }
+        return b;
+    };
+    for_each_loaded(list_ref(l, i, kListVisit), load, [&](uint32_t e, const Nb32& b) {
         if (e & kEntryBoundary) return;
-        const uint32_t j = e & kEntrySlotMask;
-        const float4 pj = f.pos[j];
-        const float3 d = rel(ki, pi, s.key[j], pj, k.cell);
+        const float4 pj = b.p;
+        const float3 d = rel(ki, pi, b.key, pj, k.cell);
         const float r = sqrtf(d.x * d.x + d.y * d.y + d.z * d.z);
         const float w = w_f32(r, k);
-        const float4 vj = f.vel[j];
+        const float4 vj = b.v;
         const float g = k.mass * 2.f / (vi.w + vj.w) * w;
         dx.add((vj.x - vi.x) * g);
         dy.add((vj.y - vi.y) * g);
