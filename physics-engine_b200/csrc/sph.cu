@@ -50,7 +50,7 @@ __global__ void __launch_bounds__(kMaxPassThreads) k_density(uint32_t n, StepCon
     }
     const double4 xi = s.pos[i];
     double rho = k.rho_self;  // 0.0 + mass * W(0)
-    for_each_loaded(
+    for_each_loaded2(
         list_ref(l, i, kListVisit), [&](uint32_t e) { return s.pos[e & kEntrySlotMask]; },
         [&](uint32_t e, const double4& xj) {
         const uint32_t j = e & kEntrySlotMask;
@@ -308,7 +308,7 @@ __global__ void __launch_bounds__(kMaxPassThreads) k_xsph(uint32_t n, StepConst 
     }
     const double4 xi = s.pos[i];
     double dvx = 0.0, dvy = 0.0, dvz = 0.0;
-    for_each_loaded(
+    for_each_loaded2(
         list_ref(l, i, kListVisit),
         [&](uint32_t e) {
             PosVel d{};
