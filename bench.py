@@ -56,7 +56,7 @@ FORCE_TRAFFIC_PER_FLUID = (427.213568e6 + 20.616448e6) / 262144
 # sm__pipe_fp64_cycles_active of the force pass in the same capture
 FORCE_FP64_PIPE_ACTIVE = 0.550
 # smsp__issue_active of the list build (k_nlist_both) in the same capture
-LISTS_ISSUE_ACTIVE = 0.472
+LISTS_ISSUE_ACTIVE = 0.435
 # Whole step, per fluid / per boundary particle (cell key 28 + sort 8 +
 # density 32 + XSPH 80 + forces 104; boundary 28 + 8 + 3 x 24).
 STEP_BYTES_FLUID, STEP_BYTES_BOUNDARY = 252.0, 108.0
