@@ -220,3 +220,35 @@ def test_dfsph_slow_path_bit_exact():
     assert w.last_iterations() == o.iterations()
     assert w.status() & pe.STATUS_SLOW_UNION
     w.close()
+
+
+def test_widely_spread_indices_sort_in_three_passes_bit_exact():
+    """A fluid block whose original indices are spread over 400,000 (one
+    particle in 200 is fluid; the rest are boundary samples of a plane far
+    below), so the widest cell union's fluid indices span 314,000 > 2^18
+    (19 bits) and the list build's radix sort takes three 9-bit passes. The lower lists (ascending original index) order the force sums,
+    so the step is bit-exact only if the sort is right."""
+    n_total, every = 400_000, 200
+    side = int(np.ceil(np.sqrt(n_total)))
+    fl = [(0.1 + DX * (k % 12), 0.1 + DX * ((k // 12) % 12), 0.1 + DX * (k // 144)) for k in range(n_total // every)]
+
+    def build(sc):
+        f = b = 0
+        for k in range(n_total):
+            if k % every == 0:
+                sc.push_fluid(fl[f])
+                f += 1
+            else:
+                sc.push_boundary((DX * (b % side), DX * (b // side), -3.0), DX ** 3)
+                b += 1
+
+    ps, os_ = _scenes(2 * DX, build)
+    prm, op = _params()
+    w = pe.WcsphWorld(ps, prm)
+    o = O.World(os_, op)
+    for _ in range(2):
+        w.step(1e-4)
+        o.step(1e-4)
+    _compare(w, o, "spread indices")
+    assert w.status() == 0
+    w.close()
