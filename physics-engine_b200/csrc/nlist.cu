@@ -6,12 +6,13 @@
 // CTA's cell are visited in the reference's (dz, dy, dx) order; their
 // particles (each cell's run already in ascending original index) are staged
 // in shared memory as single-precision coordinates relative to the cell
-// corner, and every particle of the centre cell filters the staged union with
-// a conservative squared-distance bound (`r2_filter` exceeds (2h)^2 by a
-// relative 1e-4, far above the single-precision error of the staged
-// coordinates), so every pair with q = r/h < 2 is kept. Extra borderline
-// candidates are harmless: the f64 passes evaluate q exactly and such pairs
-// contribute an exact +-0.
+// corner, one array per coordinate, and every particle of the centre cell
+// filters the staged union with a conservative squared-distance bound
+// (`r2_filter` exceeds (2h)^2 by a relative 1e-4, far above the
+// single-precision error of the staged coordinates), four candidates per
+// 16-byte read on paired f32x2 arithmetic, so every pair with q = r/h < 2 is
+// kept. Extra borderline candidates are harmless: the f64 passes evaluate q
+// exactly and such pairs contribute an exact +-0.
 //
 // k_nlist_both writes, for fluid particles, the "visit" list (in-support
 // candidates, self excluded, in visiting order, each flagged boundary /
@@ -19,8 +20,8 @@
 // reference's j > i and boundary pairs) and the "lower" list: for fluid
 // particles the fluid neighbours with a smaller original index, for boundary
 // particles all fluid neighbours, both in ascending original index; the order
-// comes from a shared-memory radix sort of the union's fluid entries per
-// cell. k_nlist_visit writes the visit list alone (the passes that need no
+// comes from a shared-memory radix sort (9-bit digits) of the union's fluid
+// entries per cell. k_nlist_visit writes the visit list alone (the passes that need no
 // ascending-index order).
 //
 // The kernels work on chunks of up to 64 centre particles with four threads
