@@ -111,7 +111,8 @@ typedef struct PeWcsphConfig {
 /* Single-precision form: cell-local float positions and float velocities,
  * single-precision pair arithmetic with Kahan-compensated density, force and
  * XSPH sums; the grid, its sort and the sound-speed control stay f64. Not the
- * reference's bits; see bench_precision.py for its error. */
+ * reference's bits: its error against the f64 step is measured by bench.py
+ * (the f32 leg: density error, centre-of-mass and energy drift). */
 #define PE_PRECISION_F32 1
 
 /* Conservation / error reductions (crates/pe-fluid/src/diagnostics.rs:35-102,
@@ -429,25 +430,29 @@ double pe_fluid_suggested_dt(double h, double sound_speed, double v_max, double 
  * library a fixed device budget or route every device allocation through
  * their own allocator, and real-time loops that must not pay for cudaMalloc's
  * device-wide synchronisation. It computes what `rebuild_grid` followed by
- * `compute_density` gives (wcsph.rs:102-154, the same bits as the world API):
- * rho[i] for every particle, rest_density for boundary samples.
+ * `compute_density` give (wcsph.rs:102-154) for a world whose density kernel
+ * is the cubic spline (PE_KERNEL_CUBIC, the WcsphParams default; no other
+ * kernel is offered here), with the same bits as the world API: rho[i] for
+ * every particle, rest_density for boundary samples.
  *
- * x [n*3], kind [n], psi [n] (may be NULL), n_out [n*3] (may be NULL) and the
- * output rho [n] are DEVICE pointers; `stream` is a cudaStream_t (NULL = the
- * legacy default stream). Nothing is allocated: the working memory is one
- * fixed array in the library's device image (about 18 MB per device that
- * loads the library, held until the process exits). Limits: n <=
+ * x [n*3], kind [n], psi [n] (may be NULL: every boundary sample then has
+ * psi 0), n_out [n*3] (may be NULL: no sample is oriented) and the output
+ * rho [n] are DEVICE pointers; `stream` is a cudaStream_t (NULL = the legacy
+ * default stream). Nothing is allocated: the working memory is one fixed
+ * array in the library's device image (about 18 MB per device that loads the
+ * library, held until the process exits). Limits: n <=
  * PE_FLUID_NOALLOC_MAX_PARTICLES and a cell-key bounding box of at most
  * PE_FLUID_NOALLOC_MAX_CELLS cells (2h-sized cells); beyond either the call
- * returns PE_ERR_BOUNDS without launching anything else.
+ * returns PE_ERR_BOUNDS and leaves rho untouched. A non-finite value in x,
+ * psi or n_out returns PE_ERR_ARG, rho untouched.
  *
- * The first call on each device, with that device current, looks up the
- * array's device address (cudaGetSymbolAddress); make that first call before
- * any stream capture on the device. The call waits for its stream once (to
- * read the key bounding box). All calls share the one array, which keeps the
- * previous call's contents; every call clears what must start at zero. Calls
- * that overlap on the GPU race on the array: issue them in order on one
- * stream or otherwise serialise them. */
+ * Every call, with the caller's device current, looks up the array's device
+ * address (cudaGetSymbolAddress, which allocates nothing). The call waits for
+ * its stream once, midway (to read the key bounding box that sizes the grid).
+ * All calls share the one array, which keeps the previous call's contents;
+ * every call clears what must start at zero. Calls that overlap on the GPU
+ * race on the array: issue them in order on one stream or otherwise
+ * serialise them. */
 #define PE_FLUID_NOALLOC_MAX_PARTICLES 131072u
 #define PE_FLUID_NOALLOC_MAX_CELLS 262144u
 int pe_fluid_density_noalloc(int32_t dim, double rest_density, double mass, double h, uint64_t n,

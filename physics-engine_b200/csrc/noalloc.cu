@@ -1,24 +1,25 @@
 // pe_fluid_density_noalloc: the density pass (grid rebuild followed by the
-// density summation of wcsph.rs:102-154) for callers that cannot allocate
-// device memory — applications that hand the library a fixed device budget
-// or manage every device allocation through their own allocator, and
-// real-time loops that must not pay cudaMalloc's device-wide synchronisation.
+// density summation of wcsph.rs:102-154, cubic-spline kernel) for callers that
+// cannot allocate device memory — applications that hand the library a fixed
+// device budget or manage every device allocation through their own
+// allocator, and real-time loops that must not pay cudaMalloc's device-wide
+// synchronisation.
 //
 // All working memory is one file-scope __device__ array of kScratchBytes. The
 // caller passes inputs and the output in its own device memory; this path
 // calls no cudaMalloc, cudaFree or allocating library routine.
 //
-// Host code must not take the array's name as a device address: on the first
-// call on each device (with that device current) the address is fetched with
-// cudaGetSymbolAddress, checked, cached, and passed to every kernel. That
-// first call should therefore come before any stream capture on the device.
+// Host code must not take the array's name as a device address: every call
+// looks the address up with cudaGetSymbolAddress (with the caller's device
+// current), checks it, and passes it to every kernel. The lookup allocates
+// nothing, and it is not cached, so a context that was torn down and created
+// again (cudaDeviceReset) never sees the previous context's address.
 // Every call on a device shares the one array and leaves its contents
 // behind: the counters that must start at zero are cleared on each call, and
 // calls that overlap on the GPU (different streams, or threads without
 // ordering) race on it — serialise them.
 #include <cmath>
 #include <cstdint>
-#include <mutex>
 
 #include "../../include/pe_fluid_wcsph.h"
 #include "pe_math.cuh"
@@ -63,9 +64,6 @@ static_assert(kScratchBytes <= (size_t)20 << 20, "the scratch array should stay 
 
 static __device__ __align__(256) unsigned char g_density_scratch[kScratchBytes];
 
-std::mutex g_setup_mutex;
-void* g_scratch_ptr[64] = {};
-
 // Original-order packing of the caller's arrays, and the key bounding box.
 __global__ void k_na_pack(uint32_t n, const double* __restrict__ x, const uint8_t* __restrict__ kind,
                           const double* __restrict__ psi, const double* __restrict__ n_out,
@@ -80,8 +78,14 @@ __global__ void k_na_pack(uint32_t n, const double* __restrict__ x, const uint8_
     const bool b = kind[i] != 0;
     const double nx = n_out ? n_out[3 * (size_t)i] : 0.0, ny = n_out ? n_out[3 * (size_t)i + 1] : 0.0,
                  nz = n_out ? n_out[3 * (size_t)i + 2] : 0.0;
+    const double ps = psi ? psi[i] : 0.0;
+    // pe-ffi rejects non-finite input (docs/FFI.md:29-35); the host reads the
+    // flag with the key box and returns PE_ERR_ARG before the grid is sized.
+    if (!(isfinite(px) && isfinite(py) && isfinite(pz) && isfinite(nx) && isfinite(ny) && isfinite(nz) &&
+          isfinite(ps)))
+        atomicOr(&hd->nonfinite, 1u);
     const bool oriented = b && (nx * nx + ny * ny + nz * nz) > 0.0;
-    pos[i] = make_double4(px, py, pz, b ? (psi ? psi[i] : 0.0) : 0.0);
+    pos[i] = make_double4(px, py, pz, b ? ps : 0.0);
     flags[i] = (b ? kFlagBoundary : 0) | (oriented ? kFlagOriented : 0);
     orig[i] = i;
     const int32_t k[3] = {floor_i32(px * inv_cell), floor_i32(py * inv_cell),
@@ -168,23 +172,15 @@ __global__ void k_na_density(uint32_t n, GridDesc g, StepConst k, const unsigned
 
 inline uint32_t blocks_for(uint64_t n, uint32_t t) { return (uint32_t)((n + t - 1) / t); }
 
-// Device address of the scratch array for the current device (fetched once).
+// Device address of the scratch array in the current device's context,
+// looked up on every call (no cache that could outlive the context).
 unsigned char* scratch_for_current_device(int* err) {
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_density_scratch) != cudaSuccess || !p) {
         *err = PE_ERR_DEVICE;
         return nullptr;
     }
-    std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch_ptr[dev]) {
-        void* p = nullptr;
-        if (cudaGetSymbolAddress(&p, g_density_scratch) != cudaSuccess || !p) {
-            *err = PE_ERR_DEVICE;
-            return nullptr;
-        }
-        g_scratch_ptr[dev] = p;
-    }
-    return static_cast<unsigned char*>(g_scratch_ptr[dev]);
+    return static_cast<unsigned char*>(p);
 }
 
 }  // namespace
@@ -217,6 +213,7 @@ extern "C" int pe_fluid_density_noalloc(int32_t dim, double rest_density, double
     if (cudaMemcpyAsync(&hd, scratch + kOffHeader, sizeof(hd), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
         cudaStreamSynchronize(st) != cudaSuccess)
         return PE_ERR_DEVICE;
+    if (hd.nonfinite) return PE_ERR_ARG;
     GridDesc g{};
     g.kx0 = hd.kmin[0];
     g.ky0 = hd.kmin[1];

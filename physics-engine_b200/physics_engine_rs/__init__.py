@@ -1229,10 +1229,11 @@ def suggested_dt(h, sound_speed, v_max, a_max, lambda_v=0.25, lambda_f=0.25):
 # --------------------------------------------------------------------------
 # Functions kept from the reference module (python/src/fluid.rs:288-305).
 # The analytic ones restate crates/pe-fluid/src/oracles.rs and coupling.rs;
-# the PBF / DFSPH / coupling solvers are not part of this WCSPH build and
-# raise NotImplementedError with that reason.
+# the canonical PBF and DFSPH tanks step on the GPU solvers of this package.
+# The coupled-tank hash needs the rigid-body world (pe-rigid), which this
+# package does not contain, so it raises NotImplementedError with that reason.
 # --------------------------------------------------------------------------
-_NOT_ON_PATH = ("this build provides the WCSPH solver path only; the {} solver is not included")
+_NOT_ON_PATH = ("this package provides the fluid side only; the {} is not included")
 
 
 FLUID_HASH_STEPS, FLUID_HASH_DT = 40, 1.0 / 120.0
@@ -1291,7 +1292,7 @@ def canonical_dfsph_hash() -> int:
 
 
 def canonical_coupling_hash() -> int:
-    raise NotImplementedError(_NOT_ON_PATH.format("fluid-rigid coupling (DFSPH)"))
+    raise NotImplementedError(_NOT_ON_PATH.format("rigid-body world of the coupled tank"))
 
 
 def fluid_ritter_front(g: float, h0: float, t: float) -> float:
@@ -1421,5 +1422,21 @@ def fluid_canonical_mass() -> float:
     return mass_from_spacing(1000.0, 0.05, 3) * 64.0
 
 
+def _kinetic_energy_diag(v, kind, mass) -> float:
+    """diagnostics.rs:52-60: sum of 0.5 m |v|^2 over fluid particles in index
+    order (|v|^2 = x*x + y*y + z*z, pe-math vec3.rs)."""
+    ke = 0.0
+    for (vx, vy, vz), k in zip(np.asarray(v).tolist(), np.asarray(kind).tolist()):
+        if k == FLUID:
+            ke += 0.5 * mass * (vx * vx + vy * vy + vz * vz)
+    return ke
+
+
 def fluid_canonical_ke_after_hash_steps() -> float:
-    raise NotImplementedError(_NOT_ON_PATH.format("PBF"))
+    """python/src/fluid.rs:277-285: kinetic energy of the canonical PBF tank
+    after FLUID_HASH_STEPS steps of FLUID_HASH_DT, stepped on the GPU."""
+    w = fluid_hash_world()
+    w.run(FLUID_HASH_DT, FLUID_HASH_STEPS)
+    ke = _kinetic_energy_diag(w.velocities(), w.kinds(), w.mass)
+    w.close()
+    return ke

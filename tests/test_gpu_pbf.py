@@ -23,6 +23,22 @@ def test_canonical_fluid_hash_matches_reference():
     assert pe.canonical_fluid_hash() == PBF_TANK_HASH
 
 
+def test_canonical_ke_after_hash_steps_matches_oracle():
+    """python/src/fluid.rs:277-285: KE of the canonical tank after 40 steps;
+    the oracle's run of the same tank, summed in index order
+    (diagnostics.rs:52-60), gives the same bits."""
+    o = O.pbf_hash_world()
+    o.run(pe.FLUID_HASH_DT, pe.FLUID_HASH_STEPS)
+    assert o.hash64() == PBF_TANK_HASH
+    v = o.v()
+    m = pe.mass_from_spacing(1000.0, 0.05, 3)
+    want = 0.0
+    for i in range(64):  # the 64 fluid particles come first (scenarios.rs:36-46)
+        want += 0.5 * m * (v[i, 0] * v[i, 0] + v[i, 1] * v[i, 1] + v[i, 2] * v[i, 2])
+    got = pe.fluid_canonical_ke_after_hash_steps()
+    assert got == want and got > 0.0
+
+
 def _scenes(dim, nx, ny, nz, dx, h, box, jitter_seed=None):
     rho0 = 1000.0
     mass = pe.mass_from_spacing(rho0, dx, dim)

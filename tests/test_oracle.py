@@ -1,7 +1,7 @@
 """CPU tests that pin the oracle (the C++ restatement of the reference WCSPH
 path) to the reference's own known answers and analytic tests.
 
-The reference ships no WCSPH golden vector, so each test
+The reference ships no WCSPH golden vector or hash, so each test
 below restates a reference test or a property fixed by the reference's code:
 crates/pe-fluid/tests/fluid_analytic.rs, crates/pe-fluid/src/grid.rs:159-181,
 crates/pe-math/src/rng.rs, and the exact rounding of the Tait power.
