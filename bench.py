@@ -88,6 +88,15 @@ def _args():
     ap.add_argument("--loop-sample", type=int, default=32,
                     help="tanks of the batch timed one by one for the per-tank loop")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-forms", action="store_true",
+                    help="plain form: skip the FP32 and learned legs of the default line")
+    ap.add_argument("--f32-steps", type=int, default=200,
+                    help="plain form's FP32 leg: steps both forms advance before the error comparison")
+    ap.add_argument("--f32-timed-steps", type=int, default=20)
+    ap.add_argument("--leg-train-tanks", type=int, default=4,
+                    help="plain form's learned leg: seeded 64k-particle training tanks")
+    ap.add_argument("--leg-train-steps", type=int, default=100)
+    ap.add_argument("--leg-rollout-steps", type=int, default=50)
     return ap.parse_args()
 
 
@@ -98,6 +107,18 @@ def fp64_rate(pe, device):
     g = C.c_double(0.0)
     rc = pe.load_library().pe_fluid_probe_fp64_rate(int(device), C.byref(g))
     return g.value if rc == 0 else None
+
+
+def phase_overhead(pe, device, phases=64):
+    """Measured cost of one phase boundary: a kernel node of a replayed CUDA
+    graph against a grid-wide barrier inside one cooperative kernel (us)."""
+    import ctypes as C
+
+    a, b = C.c_double(0.0), C.c_double(0.0)
+    f = pe.load_library().pe_fluid_probe_phase_overhead
+    f.argtypes = [C.c_int32, C.c_uint32, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    rc = f(int(device), int(phases), C.byref(a), C.byref(b))
+    return {"graph_node_us": a.value, "grid_barrier_us": b.value, "phases": phases} if rc == 0 else None
 
 
 def _peaks():
@@ -197,86 +218,135 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def cpu_baseline(steps=5):
-    """The oracle (CPU port of the reference step), single-threaded, on a bounded
-    sample: the 32^3 dam break (same dx, h, physics) for `steps` steps."""
+def _cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except Exception:
+        pass
+    return None
+
+
+def _oracle_world_1m(O, workload, threads):
+    """The bench workload built by the oracle's builders (the reference's
+    fill_box / fill_box_boundary / jitter), stepped by the oracle with
+    `threads` host threads (the parallel oracle gives the sequential one's
+    bits). Neighbour lists are materialised as the reference does
+    (wcsph.rs:102-114) when the host has the memory for them (~1,700 entries
+    of 8 bytes per fluid particle)."""
+    import psutil
+
+    (nx, ny, nz), box = WORKLOADS[workload]
+    s = O.dam_break_scene(None, dx=DX, box=box, jitter=JITTER, seed=SEED, nxyz=(nx, ny, nz))
+    need = nx * ny * nz * 1800 * 8 * 1.5
+    materialize = psutil.virtual_memory().available > need
+    w = O.World(s, O.dam_break_params(materialize=materialize))
+    w.set_threads(threads)
+    return w, nx * ny * nz, materialize
+
+
+def cpu_baseline(workload, steps=2, single_steps=5):
+    """The oracle (CPU port of the reference step) on the bench workload with
+    all host threads for `steps` steps, and the single-threaded sequential
+    oracle on the 32^3 dam break for `single_steps` steps (the reference path
+    is single-threaded, docs/FLUID.md:104)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
 
-    s = O.dam_break_scene(32)
-    w = O.World(s, O.dam_break_params(materialize=True))
-    w.step(DT)  # first step outside the timing (allocation of neighbour lists)
+    threads = os.cpu_count() or 1
+    w, nf, mat = _oracle_world_1m(O, workload, threads)
+    w.step(DT)  # first step outside the timing (neighbour-list allocation)
     t0 = time.perf_counter()
     w.run(DT, steps)
     sec = time.perf_counter() - t0
-    nf = 32 ** 3
-    return {"value": nf * steps / sec, "unit": UNIT, "cores": 1, "kind": "port",
-            "sample": f"32^3 dam break (32,768 fluid + 24,802 boundary, dx 0.01, h 2dx), {steps} "
-                      f"steps of the single-threaded C++ restatement of WcsphWorld::step, "
-                      f"-O2 -ffp-contract=off, neighbour lists materialised as the reference; "
+    del w
+    s1 = O.dam_break_scene(32)
+    w1 = O.World(s1, O.dam_break_params(materialize=True))
+    w1.step(DT)
+    t1 = time.perf_counter()
+    w1.run(DT, single_steps)
+    sec1 = time.perf_counter() - t1
+    return {"value": nf * steps / sec, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{workload}: {steps} steps of the oracle's restatement of WcsphWorld::step "
+                      f"(-O2 -ffp-contract=off) on {threads} host threads, the parallel form whose "
+                      f"results are the sequential oracle's bits; neighbour lists "
+                      f"{'materialised as the reference' if mat else 'not materialised (host memory)'}; "
                       f"{sec:.1f} s",
-            "host_cpus": os.cpu_count()}
+            "cpu_model": _cpu_model(), "host_cpus": os.cpu_count(),
+            "single_thread": {"value": 32 ** 3 * single_steps / sec1, "unit": UNIT, "cores": 1,
+                              "sample": f"32^3 dam break (32,768 fluid + 24,802 boundary), {single_steps} "
+                                        f"steps of the sequential oracle, 1 thread used, neighbour lists "
+                                        f"materialised; {sec1:.1f} s"}}
 
 
 def run_reference(args, ws, rank):
+    """The reference arm: the oracle's restatement of WcsphWorld::step on the
+    same workload, one whole step of the tank per bench step, with every host
+    thread (the parallel oracle; same bits as the sequential one). Rank 0 only."""
     if rank != 0:
         return
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
 
-    s = O.dam_break_scene(32)
-    w = O.World(s, O.dam_break_params(materialize=True))
+    threads = os.cpu_count() or 1
+    w, nf, mat = _oracle_world_1m(O, args.workload, threads)
     for _ in range(args.warmup):
         w.step(DT)
     t0 = time.perf_counter()
     for _ in range(args.steps):
         w.step(DT)
     sec = time.perf_counter() - t0
-    nf = 32 ** 3
     value = nf * args.steps / sec
-    sample = ("one step of the 32^3 dam break per bench step (32,768 fluid + 24,802 boundary, "
-              "same dx, h and physics as the 1M tank); oracle port of WcsphWorld::step, single "
-              "thread (the reference path is single-threaded by design, docs/FLUID.md:104)")
+    sample = (f"one whole step of the {args.workload} tank per bench step; oracle port of "
+              f"WcsphWorld::step on {threads} host threads (the parallel form reproduces the "
+              f"sequential restatement bit for bit; the reference itself is single-threaded, "
+              f"docs/FLUID.md:104); neighbour lists "
+              f"{'materialised as the reference' if mat else 'not materialised (host memory)'}")
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * sec / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "impl": "reference",
-            "config": {"workload": args.workload, "sample": "dam_break_32k"},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port",
-                             "sample": sample},
+            "config": _config(args.workload, nf, w.n - nf, ws),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": sample, "cpu_model": _cpu_model()},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
-def _state_summary(world, nf_mask, mass, g):
-    """f64 reductions of the fluid state (diagnostics.rs:35-71 quantities)."""
+def _config(workload, nf, nb, ws):
+    return {"workload": workload, "fluid_particles": nf, "boundary_particles": nb,
+            "dx": DX, "dt": DT, "h_over_dx": 2.0, "sound_speed": 20.0,
+            "adapt_sound_speed": False, "xsph": 0.25, "visc_alpha": 0.01,
+            "parallelism": f"{ws} independent tank(s), one per GPU",
+            "l2": "state + neighbour lists (> 2 GB) exceed the 126 MB L2; no flush needed"}
+
+
+def _device_summary(world):
+    """Fluid centre of mass and total energy (kinetic + m g z) from the device
+    FP64 reductions in original index order (diagnostics.rs:52-71)."""
+    d = world.diagnostics()
+    return world.fluid_center_of_mass(), d["kinetic_energy"] + d["gravitational_potential"], d
+
+
+def f32_leg(workload, local, torch, pe, timed_steps, warm, total_steps):
+    """The single-precision form next to the f64 step on the same tank, both
+    from the same start: `warm` untimed steps, `timed_steps` steps timed with
+    CUDA events on each world's stream, then steps up to `total_steps`; then
+    densities (per particle, host), the centre of mass and the total energy
+    (FP64 device reductions) of the f32 world against the f64 world's."""
     import numpy as np
 
-    x, v, rho = world.positions(), world.velocities(), world.densities()
-    x, v, rho = x[nf_mask], v[nf_mask], rho[nf_mask]
-    com = x.mean(axis=0)
-    ke = float((0.5 * mass * (v * v).sum(axis=1)).sum())
-    pe = float((mass * g * x[:, 2]).sum())
-    return rho, com, ke + pe
-
-
-def run_f32(args, ws, rank, local, torch, pe):
-    """Single-precision form next to the f64 step on the same tank: both advance
-    warmup + steps steps; the f32 world is timed, then densities, centre of mass
-    and total energy are compared with the f64 world's."""
-    import numpy as np
-
-    ps, prm, nf = build_scene(pe, args.workload)
+    ps, prm, nf = build_scene(pe, workload)
     nb = len(ps) - nf
-    kind = ps.arrays()["kind"]
-    fluid = kind == 0
+    fluid = ps.arrays()["kind"] == 0
     w64 = pe.WcsphWorld(ps, prm, pe.WcsphConfig(device=local))
     w32 = pe.WcsphWorld(ps, prm, pe.WcsphConfig(device=local, precision=pe.PRECISION_F32))
     del ps
     timings = {}
     for name, w in (("f32", w32), ("f64", w64)):
         stream = torch.cuda.ExternalStream(w.stream_handle(), device=local)
-        w.run(DT, max(args.warmup, 3))
+        w.run(DT, warm)
         torch.cuda.synchronize()
         sampler = ClockSampler(local) if name == "f32" else None
         if sampler:
@@ -287,38 +357,36 @@ def run_f32(args, ws, rank, local, torch, pe):
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
         a.record(stream)
-        w.run(DT, args.steps)
+        w.run(DT, timed_steps)
         b.record(stream)
         b.synchronize()
         timings[name] = (a.elapsed_time(b), w.profile(reset=True), w.kernel_launches(),
                          sampler.stop() if sampler else None, w.status())
         w.set_profiling(False)
-    g = -prm.gravity[2]
-    rho32, com32, e32 = _state_summary(w32, fluid, w32.mass, g)
-    rho64, com64, e64 = _state_summary(w64, fluid, w64.mass, g)
+        rest = total_steps - warm - timed_steps
+        if rest > 0:
+            w.run(DT, rest)
+    com32, e32, _ = _device_summary(w32)
+    com64, e64, _ = _device_summary(w64)
+    rho32, rho64 = w32.densities()[fluid], w64.densities()[fluid]
     rel = np.abs(rho32 - rho64) / rho64
     ms32, prof32, launches, clocks, status = timings["f32"]
     ms64 = timings["f64"][0]
-    value = nf * args.steps / (ms32 / 1e3)
     hbm_peak, peak_kind = _peaks()
     f_ms, f_n = prof32["forces"]
     achieved = FORCE_BYTES_F32 * nf * f_n / (f_ms / 1e3) / 1e9 if f_ms > 0 else 0.0
-    line = {
-        "metric": "SPH fluid particle-steps/s @1M (FP32 form)", "value": value, "unit": UNIT,
-        "n_gpus": 1, "steps": args.steps, "warmup": max(args.warmup, 3),
-        "ms_per_step": ms32 / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic", "form": "f32",
-        "config": {"workload": args.workload, "fluid_particles": nf, "boundary_particles": nb,
-                   "dx": DX, "dt": DT, "sound_speed": 20.0, "adapt_sound_speed": False},
+    leg = {
+        "value": nf * timed_steps / (ms32 / 1e3), "unit": UNIT, "ms_per_step": ms32 / timed_steps,
+        "timed_steps": timed_steps, "warmup": warm, "dtype": "f32 pair arithmetic (Kahan sums), f64 grid/CFL/reductions",
+        "f64_ms_per_step": ms64 / timed_steps, "speedup_vs_f64_step": ms64 / ms32,
         "gpu_launches": int(launches), "status": int(status),
-        "phases_ms_per_step": {k: v[0] / max(1, args.steps) for k, v in prof32.items()},
-        "f64_ms_per_step": ms64 / args.steps,
-        "speedup_vs_f64_step": ms64 / ms32,
+        "phases_ms_per_step": {k: v[0] / max(1, timed_steps) for k, v in prof32.items()},
         "error_vs_f64": {
-            "after_steps": max(args.warmup, 3) + args.steps,
+            "after_steps": max(total_steps, warm + timed_steps),
             "density_rel_max": float(rel.max()), "density_rel_mean": float(rel.mean()),
             "com_drift_m": float(np.linalg.norm(com32 - com64)),
             "energy_rel_drift": float((e32 - e64) / abs(e64)),
+            "reductions": "centre of mass and energy: FP64 device sums in original index order",
         },
         "roofline": {"bound": "hbm", "kernel": "k_forces_f32 (force + kick + drift)",
                      "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
@@ -329,6 +397,22 @@ def run_f32(args, ws, rank, local, torch, pe):
     }
     w32.close()
     w64.close()
+    return leg, nf, nb
+
+
+def run_f32(args, ws, rank, local, torch, pe):
+    """Single-precision form next to the f64 step on the same tank."""
+    warm = max(args.warmup, 3)
+    leg, nf, nb = f32_leg(args.workload, local, torch, pe, args.steps, warm, warm + args.steps)
+    line = {
+        "metric": "SPH fluid particle-steps/s @1M (FP32 form)", "value": leg["value"], "unit": UNIT,
+        "n_gpus": 1, "steps": args.steps, "warmup": warm, "ms_per_step": leg["ms_per_step"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic", "form": "f32",
+        "config": {"workload": args.workload, "fluid_particles": nf, "boundary_particles": nb,
+                   "dx": DX, "dt": DT, "sound_speed": 20.0, "adapt_sound_speed": False},
+    }
+    line.update({k: v for k, v in leg.items() if k not in ("value", "unit", "ms_per_step")})
     if rank == 0:
         print(json.dumps(line), flush=True)
 
@@ -409,7 +493,9 @@ def run_batched(args, ws, rank, local, torch, pe):
                    "seed": seed, "dx": DX, "dt": DT, "sound_speed": 20.0, "adapt_sound_speed": False,
                    "parallelism": f"{ws} rank(s), each its own batch of tanks",
                    "l2": "state + lists of the batch exceed the 126 MB L2; no flush needed"},
-        "execution": {"graph_steps": 6, "autotuned_shapes": shapes, "scene_build_s": build_s},
+        "execution": {"graph_steps": 6, "autotuned_shapes": shapes, "scene_build_s": build_s,
+                      "launches_per_step": launches / max(1, args.steps),
+                      "phase_boundary_cost": phase_overhead(pe, local)},
         "gpu_launches": int(launches), "status": int(status),
         "neighbour_lists": {"used_gb": cap["list_groups_used"] * 16 / 1e9,
                             "pool_gb": cap["list_groups_capacity"] * 16 / 1e9},
@@ -427,10 +513,10 @@ def run_batched(args, ws, rank, local, torch, pe):
         print(json.dumps(line), flush=True)
 
 
-def run_learned_form(args, ws, rank, local, torch, pe):
+def learned_leg(workload, local, torch, pe, train_tanks, train_steps, rollout_steps):
     """The learned surrogate: trained online on plain rollouts of seeded
-    64k-particle tanks (tank extents 0.45..1.0 m), then the 1M dam break run
-    with learned steps judged every 10 steps by the plain SPH density (a window
+    64k-particle tanks (tank extents 0.45..1.0 m), then the bench tank run with
+    learned steps judged every 10 steps by the plain SPH density (a window
     whose relative density error exceeds 1% is rerun with the plain step),
     next to the plain f64 run of the same steps."""
     import numpy as np
@@ -440,22 +526,29 @@ def run_learned_form(args, ws, rank, local, torch, pe):
     prm = pe.WcsphParams.water(1000.0, 20.0, (0.0, 0.0, -9.81))
     prm.adapt_sound_speed = False
     # ---- training ----
-    tanks, _ = scenes.batch_dam_break(args.train_tanks, SEED + 7, 64000, 64000, 0.45, 1.0)
+    tanks, _ = scenes.batch_dam_break(train_tanks, SEED + 7, 64000, 64000, 0.45, 1.0)
     train = pe.WcsphWorld.from_tanks(prm, tanks, pe.WcsphConfig(device=local))
     del tanks
     sur = S.Surrogate(seed=SEED)
     t0 = time.perf_counter()
-    losses = S.train_on_rollouts(sur, train, DT, args.train_steps, iters_per_step=2, lr=5e-4, stat_steps=20)
+    losses = S.train_on_rollouts(sur, train, DT, train_steps, iters_per_step=2, lr=5e-4, stat_steps=20)
     torch.cuda.synchronize()
     train_s = time.perf_counter() - t0
     train.close()
-    # ---- rollouts at 1M ----
-    ps, _, nf = build_scene(pe, args.workload)
+    # one-step loss on a 64k tank never trained on: the network against the
+    # mean prediction and against persistence (reusing the last plain step's
+    # dv/dt, drho/dt)
+    held_tanks, _ = scenes.batch_dam_break(1, SEED + 99, 64000, 64000, 0.45, 1.0)
+    held = pe.WcsphWorld.from_tanks(prm, held_tanks, pe.WcsphConfig(device=local))
+    heldout = S.heldout_comparison(sur, held, DT, steps_before=min(150, train_steps))
+    held.close()
+    # ---- rollouts on the bench tank ----
+    ps, _, nf = build_scene(pe, workload)
     fluid = ps.arrays()["kind"] == 0
     plain = pe.WcsphWorld(ps, prm, pe.WcsphConfig(device=local))
     learned = pe.WcsphWorld(ps, prm, pe.WcsphConfig(device=local))
     del ps
-    steps = args.rollout_steps
+    steps = rollout_steps
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     plain.run(DT, steps)
@@ -471,40 +564,46 @@ def run_learned_form(args, ws, rank, local, torch, pe):
     # ---- error against the plain f64 run ----
     r64, r_l = plain.densities()[fluid], learned.densities()[fluid]
     x64, x_l = plain.positions()[fluid], learned.positions()[fluid]
-    v64, v_l = plain.velocities()[fluid], learned.velocities()[fluid]
     rel = np.abs(r_l - r64) / r64
-    mass = plain.mass
-
-    def energy(x, v):
-        return float((0.5 * mass * (v * v).sum(1)).sum() + (mass * 9.81 * x[:, 2]).sum())
-
-    e64, e_l = energy(x64, v64), energy(x_l, v_l)
-    value = nf * steps / learned_s
-    line = {
-        "metric": "SPH fluid particle-steps/s @1M (learned surrogate, judged every 10 steps)",
-        "value": value, "unit": UNIT, "n_gpus": 1, "steps": steps, "warmup": 0,
-        "ms_per_step": learned_s / steps * 1e3, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "bf16 network, f64 state", "data": "synthetic", "form": "learned",
-        "config": {"workload": args.workload, "fluid_particles": nf, "dx": DX, "dt": DT,
-                   "network": "2-hop message passing, MLP width 128 x 2 hidden layers, r_msg = h",
-                   "judge_every": 10, "fallback_bound": 0.01,
-                   "training": {"tanks": args.train_tanks, "particles_per_tank": 64000,
-                                "plain_steps": args.train_steps, "normalisation_steps": 20,
-                                "adam_steps": len(losses), "lr": 5e-4, "seconds": train_s,
-                                "final_loss": float(np.mean(losses[-20:])) if losses else None}},
+    com64, e64, _ = _device_summary(plain)
+    com_l, e_l, _ = _device_summary(learned)
+    leg = {
+        "value": nf * steps / learned_s, "unit": UNIT, "ms_per_step": learned_s / steps * 1e3,
+        "rollout_steps": steps, "dtype": "bf16 network (fp32 accumulation), f64 state",
+        "network": "2-hop message passing, MLP width 128 x 2 hidden layers, r_msg = h",
+        "judge_every": 10, "fallback_bound": 0.01,
+        "training": {"tanks": train_tanks, "particles_per_tank": 64000,
+                     "plain_steps": train_steps, "normalisation_steps": 20,
+                     "adam_steps": len(losses), "lr": 5e-4, "seconds": train_s,
+                     "final_loss": float(np.mean(losses[-20:])) if losses else None},
         "plain_f64": {"ms_per_step": plain_s / steps * 1e3, "value": nf * steps / plain_s},
         "speedup_vs_plain_step": plain_s / learned_s,
+        "heldout_one_step_loss": heldout,
         "judge": st, "fallback_rate": st["fallbacks"] / max(1, st["windows"]),
         "error_vs_f64": {"after_steps": steps, "density_rel_max": float(rel.max()),
                          "density_rel_mean": float(rel.mean()),
                          "position_rms_m": float(np.sqrt(((x_l - x64) ** 2).sum(1).mean())),
-                         "com_drift_m": float(np.linalg.norm(x_l.mean(0) - x64.mean(0))),
+                         "com_drift_m": float(np.linalg.norm(com_l - com64)),
                          "energy_rel_drift": float((e_l - e64) / abs(e64))},
         "timing": "wall clock around synchronous runs (the learned run synchronises at every judge)",
         "clocks": clocks,
     }
     plain.close()
     learned.close()
+    return leg, nf
+
+
+def run_learned_form(args, ws, rank, local, torch, pe):
+    leg, nf = learned_leg(args.workload, local, torch, pe, args.train_tanks, args.train_steps,
+                          args.rollout_steps)
+    line = {
+        "metric": "SPH fluid particle-steps/s @1M (learned surrogate, judged every 10 steps)",
+        "value": leg["value"], "unit": UNIT, "n_gpus": 1, "steps": leg["rollout_steps"], "warmup": 0,
+        "ms_per_step": leg["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": leg["dtype"], "data": "synthetic", "form": "learned",
+        "config": {"workload": args.workload, "fluid_particles": nf, "dx": DX, "dt": DT},
+    }
+    line.update({k: v for k, v in leg.items() if k not in ("value", "unit", "ms_per_step", "dtype")})
     if rank == 0:
         print(json.dumps(line), flush=True)
 
@@ -766,11 +865,7 @@ def main():
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
         "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": args.workload, "fluid_particles": nf, "boundary_particles": nb,
-                   "dx": DX, "dt": DT, "h_over_dx": 2.0, "sound_speed": 20.0,
-                   "adapt_sound_speed": False, "xsph": 0.25, "visc_alpha": 0.01,
-                   "parallelism": f"{ws} independent tank(s), one per GPU",
-                   "l2": "state + neighbour lists (> 2 GB) exceed the 126 MB L2; no flush needed"},
+        "config": _config(args.workload, nf, nb, ws),
         "gpu_launches": int(launches),
         "status": int(status),
         "phases_ms_per_step": {k: v[0] / max(1, args.steps) for k, v in prof.items()},
@@ -815,9 +910,19 @@ def main():
                            "get_positions + get_velocities (state round-trips through the host)"},
         "clocks": clocks,
     }
-    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline()
     world.close()
+    # ---- the other forms of the metric, on the same tank (1 GPU) ----
+    if ws == 1 and not args.no_forms:
+        forms = {}
+        leg, _, _ = f32_leg(args.workload, local, torch, pe, args.f32_timed_steps, max(args.warmup, 3),
+                            args.f32_steps)
+        forms["f32"] = leg
+        leg, _ = learned_leg(args.workload, local, torch, pe, args.leg_train_tanks, args.leg_train_steps,
+                             args.leg_rollout_steps)
+        forms["learned"] = leg
+        line["forms"] = forms
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(args.workload)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if ws > 1:

@@ -115,8 +115,8 @@ typedef struct PeWcsphConfig {
  * (the f32 leg: density error, centre-of-mass and energy drift). */
 #define PE_PRECISION_F32 1
 
-/* Conservation / error reductions (crates/pe-fluid/src/diagnostics.rs:35-102,
- * wcsph.rs:350-369), computed in f64. */
+/* Conservation / error reductions (crates/pe-fluid/src/diagnostics.rs:19-102,
+ * wcsph.rs:350-369), computed in f64 on the device. */
 typedef struct PeFluidDiagnostics {
     double total_mass;
     double linear_momentum[3];
@@ -338,11 +338,15 @@ int pe_fluid_wcsph_tanks(PeWcsph* w, uint32_t* n_tanks);
 /* The persisted sound speed of every tank (n_tanks must equal the world's). */
 int pe_fluid_wcsph_get_sound_speeds(PeWcsph* w, double* out, uint32_t n_tanks);
 /* Launch-shape autotuner (no reference counterpart): times the candidate block
- * sizes of the density, force and XSPH passes (64, 128, 256) and list-build CTAs
- * per SM on the current state without advancing it, and keeps the fastest.
+ * sizes of the density, force and XSPH passes (64, 128, 256), and the list
+ * build's tile (32 or 64 centre particles per chunk) with its CTAs per SM, on
+ * the current state without advancing it, and keeps the fastest. No shape
+ * changes a result bit.
  * out (may be NULL) = {density, forces, xsph block sizes, list CTAs per SM}. */
 int pe_fluid_wcsph_autotune(PeWcsph* w, uint32_t out[4]);
 int pe_fluid_wcsph_shapes(PeWcsph* w, uint32_t out[4]);
+/* The list build's tile in use: centre particles per chunk (32 or 64). */
+int pe_fluid_wcsph_list_chunk(PeWcsph* w, uint32_t* out);
 
 /* WcsphWorld::step (wcsph.rs:326). Synchronous; returns PE_ERR_BOUNDS if the
  * step raised PE_STATUS_DOMAIN or PE_STATUS_NEIGHBOUR_OVERFLOW. */
@@ -396,7 +400,13 @@ int pe_fluid_wcsph_clear_status(PeWcsph* w);
  * asked for, union stage capacity, list pool capacity in 16-byte groups,
  * occupied cells, dense cells, list-build CTAs}. */
 int pe_fluid_wcsph_capacity_info(PeWcsph* w, uint64_t out[8]);
+/* diagnostics.rs:19-102 and wcsph.rs:350-369, reduced on the device with the
+ * reference's bits: sums in original index order, the FNV-1a hash of the
+ * fluid (x, v); no copy of the state to the host. */
 int pe_fluid_wcsph_diagnostics(PeWcsph* w, PeFluidDiagnostics* out);
+/* Fluid centre of mass (no reference counterpart): the fluid positions summed
+ * in original index order on the device, divided by the fluid count. */
+int pe_fluid_wcsph_fluid_center_of_mass(PeWcsph* w, double out[3]);
 /* Per-phase device time, measured with CUDA events on the world's stream:
  * 0 grid build, 1 neighbour lists, 2 density, 3 pressure, 4 forces + kick/drift,
  * 5 boundary reaction forces, 6 XSPH (no reference counterpart). */
@@ -464,6 +474,14 @@ int pe_fluid_density_noalloc(int32_t dim, double rest_density, double mass, doub
  * compile to, in 1e9 operations per second. The denominator of the step's FP64
  * roofline. */
 int pe_fluid_probe_fp64_rate(int32_t device, double* gops);
+
+/* Measured cost of one phase boundary (no reference counterpart), in
+ * microseconds: a kernel node of a replayed CUDA graph of `phases` nodes
+ * (node_us), against a grid-wide barrier inside one cooperative persistent
+ * kernel of `phases` phases (barrier_us; the barrier's wait is bounded and a
+ * timeout returns PE_ERR_DEVICE). Both over the same co-resident grid with
+ * token work per phase. 2 <= phases <= 4096. */
+int pe_fluid_probe_phase_overhead(int32_t device, uint32_t phases, double* node_us, double* barrier_us);
 
 /* Library version string. */
 const char* pe_fluid_version(void);

@@ -171,6 +171,8 @@ def lib():
             "ow_a_max": (d, [vp]),
             "ow_v_max": (d, [vp]),
             "ow_hash": (u64, [vp]),
+            "ow_set_threads": (None, [vp, C.c_int]),
+            "ow_set_pow_perturbation": (None, [vp, d, u64]),
             "ow_get_x": (None, [vp, vp]),
             "ow_get_v": (None, [vp, vp]),
             "ow_get_a": (None, [vp, vp]),
@@ -377,6 +379,16 @@ class World:
 
     def hash64(self):
         return lib().ow_hash(self._w)
+
+    def set_threads(self, threads: int):
+        """Parallel oracle: OpenMP over particles, forces as the bit-identical
+        gather (same results as one thread)."""
+        lib().ow_set_threads(self._w, int(threads))
+
+    def set_pow_perturbation(self, rate: float, seed: int):
+        """Sensitivity hook: each fluid particle's Tait power moves one ulp
+        with probability `rate` per pressure pass (seeded)."""
+        lib().ow_set_pow_perturbation(self._w, float(rate), int(seed))
 
     def v_max(self):
         return lib().ow_v_max(self._w)

@@ -24,7 +24,9 @@
 // pins the pow normalisations of the poly6 and spiky kernels.
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
+#include <thread>
 #include <cstdint>
 #include <cstring>
 #include <limits>
@@ -32,6 +34,63 @@
 #include <vector>
 
 namespace oracle {
+
+// ---------------------------------------------------------------------------
+// Parallel oracle helpers (threads > 1 only; one thread runs inline).
+// ---------------------------------------------------------------------------
+// fn(i, worker) for i in [0, n), handed out in chunks from a shared counter.
+template <typename F>
+static void parallel_for(size_t n, int threads, F fn, size_t chunk = 256) {
+    if (threads <= 1 || n <= chunk) {
+        for (size_t i = 0; i < n; ++i) fn(i, 0);
+        return;
+    }
+    std::atomic<size_t> next{0};
+    auto work = [&](int w) {
+        for (;;) {
+            size_t a = next.fetch_add(chunk);
+            if (a >= n) return;
+            size_t b = std::min(n, a + chunk);
+            for (size_t i = a; i < b; ++i) fn(i, w);
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int w = 1; w < threads; ++w) pool.emplace_back(work, w);
+    work(0);
+    for (auto& t : pool) t.join();
+}
+
+// Sort by a strict total order: sorted chunks merged pairwise. A total order
+// has one sorted result, so this equals the sequential stable sort.
+template <typename T, typename Lt>
+static void parallel_sort_total(std::vector<T>& v, Lt lt, int threads) {
+    const size_t n = v.size();
+    if (threads <= 1 || n < 65536) {
+        std::stable_sort(v.begin(), v.end(), lt);
+        return;
+    }
+    size_t parts = 1;
+    while (parts < (size_t)threads) parts *= 2;
+    std::vector<size_t> cut(parts + 1);
+    for (size_t k = 0; k <= parts; ++k) cut[k] = n * k / parts;
+    {
+        std::vector<std::thread> pool;
+        for (size_t k = 0; k < parts; ++k)
+            pool.emplace_back([&, k] { std::sort(v.begin() + cut[k], v.begin() + cut[k + 1], lt); });
+        for (auto& t : pool) t.join();
+    }
+    std::vector<T> tmp(n);
+    for (size_t width = 1; width < parts; width *= 2) {
+        std::vector<std::thread> pool;
+        for (size_t k = 0; k < parts; k += 2 * width)
+            pool.emplace_back([&, k] {
+                std::merge(v.begin() + cut[k], v.begin() + cut[k + width], v.begin() + cut[k + width],
+                           v.begin() + cut[k + 2 * width], tmp.begin() + cut[k], lt);
+            });
+        for (auto& t : pool) t.join();
+        v.swap(tmp);
+    }
+}
 
 // ---------------------------------------------------------------------------
 // pe-math Vec3 (crates/pe-math/src/vec3.rs:9-183): component-wise ops.
@@ -419,21 +478,23 @@ struct UniformGrid {
         return CellKey{ix, iy, iz};
     }
     // grid.rs:76 rebuild: sort by (key, index), run-length occupied cells
-    void rebuild(const std::vector<V3>& pos) {
+    // threads > 1 (parallel oracle): the same keys and the same order, since
+    // (key, index) is a total order and the sort's result is unique.
+    void rebuild(const std::vector<V3>& pos, int threads = 1) {
         size_t n = pos.size();
         keys.resize(n);
-        order.clear();
-        order.reserve(n);
-        for (size_t i = 0; i < n; ++i) {
+        order.resize(n);
+        parallel_for(n, threads, [&](size_t i, int) {
             keys[i] = key_of(pos[i]);
-            order.push_back(i);
-        }
+            order[i] = i;
+        }, 4096);
         const std::vector<CellKey>& k = keys;
-        std::stable_sort(order.begin(), order.end(), [&k](size_t a, size_t b) {
+        auto lt = [&k](size_t a, size_t b) {
             if (key_lt(k[a], k[b])) return true;
             if (key_lt(k[b], k[a])) return false;
             return a < b;
-        });
+        };
+        parallel_sort_total(order, lt, threads);
         occupied.clear();
         ranges.clear();
         if (n == 0) return;
@@ -508,6 +569,17 @@ struct World {
     UniformGrid grid;
     WParams prm;
     double t = 0.0;
+    // Parallel oracle (threads > 1): every per-particle loop runs on
+    // std::threads and compute_forces runs as the gather of forces_gather_*; the
+    // results are the sequential oracle's bits (tests check both on the same
+    // scenes). Used to time the CPU baseline on large tanks.
+    int threads = 1;
+    // Sensitivity test hook: with rate > 0, each fluid particle's Tait power
+    // moves one ulp (up or down) with probability `rate`, drawn from a seeded
+    // counter per pressure pass; models a last-ulp difference of the pow.
+    double pow_perturb_rate = 0.0;
+    uint64_t pow_perturb_seed = 0;
+    uint64_t pressure_calls = 0;
     std::vector<size_t> neigh;
     std::vector<std::vector<size_t>> neigh_lists;
     std::vector<V3> xsph_dv;
@@ -518,42 +590,44 @@ struct World {
 
     // wcsph.rs:102 rebuild_grid
     void rebuild_grid() {
-        grid.rebuild(parts.x);
+        grid.rebuild(parts.x, threads);
         size_t n = parts.len();
         if (neigh_lists.size() != n) neigh_lists.resize(n);
-        for (size_t i = 0; i < n; ++i) {
+        parallel_for(n, threads, [&](size_t i, int) {
             neigh_lists[i].clear();
-            if (prm.materialize_neigh_lists && parts.kind[i] == FLUID)
-                grid.neighbours(i, neigh_lists[i]);
-        }
+            if (prm.materialize_neigh_lists && parts.kind[i] == FLUID) grid.neighbours(i, neigh_lists[i]);
+        });
     }
     // wcsph.rs:117 compute_density
     void compute_density() {
         size_t n = parts.len();
+        if (threads > 1) {
+            std::vector<std::vector<size_t>> nb(threads);
+            parallel_for(n, threads, [&](size_t i, int w) { parts.rho[i] = density_of(i, nb[w]); });
+            return;
+        }
+        for (size_t i = 0; i < n; ++i) parts.rho[i] = density_of(i, neigh);
+    }
+    double density_of(size_t i, std::vector<size_t>& nb) const {
         double h = parts.h, mass = parts.mass, rho0 = parts.rest_density;
         Dim dim = parts.dim;
-        for (size_t i = 0; i < n; ++i) {
-            if (parts.kind[i] != FLUID) {
-                parts.rho[i] = rho0;
-                continue;
+        if (parts.kind[i] != FLUID) return rho0;
+        nb.clear();
+        grid.neighbours(i, nb);
+        V3 xi = parts.x[i];
+        double rho = 0.0;
+        rho += mass * kern_w(kk(), 0.0, h, dim);
+        for (size_t j : nb) {
+            if (j == i) continue;
+            double r = norm(parts.x[j] - xi);
+            double wij = kern_w(kk(), r, h, dim);
+            if (parts.kind[j] == FLUID) {
+                rho += mass * wij;
+            } else if (parts.boundary_sees_fluid(j, xi)) {
+                rho += rho0 * parts.psi[j] * wij;
             }
-            neigh.clear();
-            grid.neighbours(i, neigh);
-            V3 xi = parts.x[i];
-            double rho = 0.0;
-            rho += mass * kern_w(kk(), 0.0, h, dim);
-            for (size_t j : neigh) {
-                if (j == i) continue;
-                double r = norm(parts.x[j] - xi);
-                double wij = kern_w(kk(), r, h, dim);
-                if (parts.kind[j] == FLUID) {
-                    rho += mass * wij;
-                } else if (parts.boundary_sees_fluid(j, xi)) {
-                    rho += rho0 * parts.psi[j] * wij;
-                }
-            }
-            parts.rho[i] = std::fmax(rho, 1e-12);  // f64::max (NaN -> other)
         }
+        return std::fmax(rho, 1e-12);  // f64::max (NaN -> other)
     }
     // viscosity.rs:89 max_speed over fluid
     double max_speed() const {
@@ -580,8 +654,27 @@ struct World {
             c = c < min_c ? min_c : c;
             prm.eos_sound_speed = c;
         }
-        for (size_t i = 0; i < parts.len(); ++i)
-            parts.p[i] = parts.kind[i] == FLUID ? eos_pressure(parts.rho[i]) : 0.0;
+        const uint64_t call = pressure_calls++;
+        parallel_for(parts.len(), threads, [&](size_t i, int) {
+            parts.p[i] = parts.kind[i] == FLUID ? eos_pressure_at(parts.rho[i], i, call) : 0.0;
+        }, 4096);
+    }
+    static uint64_t splitmix64(uint64_t z) {
+        z += 0x9E3779B97F4A7C15ULL;
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+        return z ^ (z >> 31);
+    }
+    // eos_pressure, with the sensitivity hook's one-ulp move of the power
+    double eos_pressure_at(double density, size_t i, uint64_t call) const {
+        if (pow_perturb_rate <= 0.0) return eos_pressure(density);
+        double ratio = density / prm.eos_rest_density;
+        double b = prm.eos_rest_density * prm.eos_sound_speed * prm.eos_sound_speed / prm.eos_gamma;
+        double pw = oracle_pow(ratio, prm.eos_gamma);
+        const uint64_t r = splitmix64(pow_perturb_seed ^ splitmix64(call * 0x100000001ULL + i));
+        if ((double)(r >> 11) * 0x1.0p-53 < pow_perturb_rate)
+            pw = std::nextafter(pw, (r & 1) ? INFINITY : -INFINITY);
+        return b * (pw - 1.0);
     }
     // viscosity.rs:51 pi_ij
     double pi_ij(double h, double c, V3 xi, V3 xj, V3 vi, V3 vj, double rhoi, double rhoj) const {
@@ -602,8 +695,12 @@ struct World {
         double c0 = prm.eos_sound_speed;
         Dim dim = parts.dim;
         V3 g = v3(prm.gravity[0], prm.gravity[1], prm.gravity[2]);
-        for (auto& a : parts.a) a = zero3();
         if (boundary_force.size() != n) boundary_force.resize(n);
+        if (threads > 1 && prm.st_sigma == 0.0) {
+            forces_gather();
+            return;
+        }
+        for (auto& a : parts.a) a = zero3();
         for (auto& f : boundary_force) f = zero3();
         for (size_t i = 0; i < n; ++i) {
             if (parts.kind[i] != FLUID) continue;
@@ -645,6 +742,91 @@ struct World {
             for (size_t i = 0; i < n; ++i)
                 if (parts.kind[i] == FLUID) parts.a[i] += st_a[i];
         }
+    }
+    // Parallel form of compute_forces. The scatter above gives a[k] the
+    // sequence 0 - f(i1,k) - f(i2,k) - ... (fluid i < k, ascending i), then
+    // + f(k,j) (fluid j > k and boundary j, visiting order), then + g; and
+    // f(i,k) = -f(k,i) bit for bit (the pressure sum and pi_ij are symmetric,
+    // grad W flips sign exactly), so x - f(i,k) = x + f(k,i). A boundary
+    // sample's reaction is the sum over fluid i in ascending i. The cell
+    // neighbour relation is symmetric, so each particle finds those partners
+    // among its own candidates.
+    V3 fluid_pair_force(size_t i, size_t j, V3 gw) const {
+        double rho_i = parts.rho[i], p_i = parts.p[i], rho_j = parts.rho[j], p_j = parts.p[j];
+        double press = p_i / (rho_i * rho_i) + p_j / (rho_j * rho_j);
+        V3 f_press = gw * (-parts.mass * press);
+        double pi = pi_ij(parts.h, prm.eos_sound_speed, parts.x[i], parts.x[j], parts.v[i], parts.v[j], rho_i,
+                          rho_j);
+        V3 f_visc = gw * (-parts.mass * pi);
+        return f_press + f_visc;
+    }
+    V3 gather_fluid_accel(size_t k, std::vector<size_t>& nb, std::vector<size_t>& low) const {
+        const double h = parts.h, rho0 = parts.rest_density;
+        const Dim dim = parts.dim;
+        nb.clear();
+        grid.neighbours(k, nb);
+        low.clear();
+        for (size_t j : nb)
+            if (j < k && parts.kind[j] == FLUID) low.push_back(j);
+        std::sort(low.begin(), low.end());
+        const V3 xk = parts.x[k];
+        V3 a = zero3();
+        for (size_t i : low) {
+            V3 rij = parts.x[i] - xk;
+            if (norm(rij) < 1e-30) continue;
+            a += fluid_pair_force(k, i, grad_w(kk(), rij, h, dim));
+        }
+        const double rho_k = parts.rho[k], p_k = parts.p[k];
+        for (size_t j : nb) {
+            if (j == k) continue;
+            V3 rij = parts.x[j] - xk;
+            if (norm(rij) < 1e-30) continue;
+            V3 gw = grad_w(kk(), rij, h, dim);
+            if (parts.kind[j] == FLUID) {
+                if (j < k) continue;
+                a += fluid_pair_force(k, j, gw);
+            } else {
+                if (!parts.boundary_sees_fluid(j, xk)) continue;
+                double press = p_k / (rho_k * rho_k);
+                a += gw * (-(rho0 * parts.psi[j]) * press);
+            }
+        }
+        a += v3(prm.gravity[0], prm.gravity[1], prm.gravity[2]);
+        return a;
+    }
+    V3 gather_boundary_force(size_t b, std::vector<size_t>& nb, std::vector<size_t>& low) const {
+        const double h = parts.h, mass = parts.mass, rho0 = parts.rest_density;
+        const Dim dim = parts.dim;
+        nb.clear();
+        grid.neighbours(b, nb);
+        low.clear();
+        for (size_t j : nb)
+            if (parts.kind[j] == FLUID) low.push_back(j);
+        std::sort(low.begin(), low.end());
+        V3 f = zero3();
+        for (size_t i : low) {
+            V3 rij = parts.x[b] - parts.x[i];
+            if (norm(rij) < 1e-30) continue;
+            if (!parts.boundary_sees_fluid(b, parts.x[i])) continue;
+            V3 gw = grad_w(kk(), rij, h, dim);
+            double press = parts.p[i] / (parts.rho[i] * parts.rho[i]);
+            V3 fi = gw * (-(rho0 * parts.psi[b]) * press);
+            f += fi * (-mass);
+        }
+        return f;
+    }
+    void forces_gather() {
+        const size_t n = parts.len();
+        std::vector<std::vector<size_t>> nb(threads), low(threads);
+        parallel_for(n, threads, [&](size_t i, int w) {
+            if (parts.kind[i] == FLUID) {
+                parts.a[i] = gather_fluid_accel(i, nb[w], low[w]);
+                boundary_force[i] = zero3();
+            } else {
+                parts.a[i] = zero3();
+                boundary_force[i] = gather_boundary_force(i, nb[w], low[w]);
+            }
+        });
     }
     // surface_tension.rs:112-220 surface_tension_accel over the grid's lists
     void surface_tension_accel(std::vector<V3>& normals, std::vector<V3>& out) {
@@ -721,14 +903,14 @@ struct World {
         double h = parts.h, mass = parts.mass;
         Dim dim = parts.dim;
         xsph_dv.assign(n, zero3());
-        for (size_t i = 0; i < n; ++i) {
-            if (parts.kind[i] != FLUID) continue;
-            neigh.clear();
-            grid.neighbours(i, neigh);
+        auto one = [&](size_t i, std::vector<size_t>& nb) {
+            if (parts.kind[i] != FLUID) return;
+            nb.clear();
+            grid.neighbours(i, nb);
             V3 xi = parts.x[i], vi = parts.v[i];
             double rho_i = parts.rho[i];
             V3 dv = zero3();
-            for (size_t j : neigh) {
+            for (size_t j : nb) {
                 if (j == i || parts.kind[j] != FLUID) continue;
                 double r = norm(parts.x[j] - xi);
                 double wij = kern_w(kk(), r, h, dim);
@@ -736,6 +918,12 @@ struct World {
                 dv += (parts.v[j] - vi) * (mass / rho_bar * wij);
             }
             xsph_dv[i] = dv * eps;
+        };
+        if (threads > 1) {
+            std::vector<std::vector<size_t>> nb(threads);
+            parallel_for(n, threads, [&](size_t i, int w) { one(i, nb[w]); });
+        } else {
+            for (size_t i = 0; i < n; ++i) one(i, neigh);
         }
         for (size_t i = 0; i < n; ++i)
             if (parts.kind[i] == FLUID) parts.v[i] += xsph_dv[i];
@@ -1554,6 +1742,11 @@ double ow_sound_speed(OWorld* w) { return W(w).prm.eos_sound_speed; }
 double ow_a_max(OWorld* w) { return W(w).a_max(); }
 double ow_v_max(OWorld* w) { return W(w).max_speed(); }
 uint64_t ow_hash(OWorld* w) { return particles_hash64(W(w).parts); }
+void ow_set_threads(OWorld* w, int threads) { W(w).threads = threads < 1 ? 1 : threads; }
+void ow_set_pow_perturbation(OWorld* w, double rate, uint64_t seed) {
+    W(w).pow_perturb_rate = rate;
+    W(w).pow_perturb_seed = seed;
+}
 
 static void put3(const std::vector<V3>& src, double* out) {
     for (size_t i = 0; i < src.size(); ++i) {

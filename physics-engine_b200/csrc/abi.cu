@@ -115,15 +115,6 @@ int check_params(const PeWcsphParams* p) {
 }
 
 
-uint64_t fnv1a(uint64_t h, double x) {
-    uint64_t bits;
-    std::memcpy(&bits, &x, 8);
-    for (int k = 0; k < 8; ++k) {
-        h ^= (bits >> (8 * k)) & 0xffULL;
-        h *= 0x100000001b3ULL;
-    }
-    return h;
-}
 
 }  // namespace
 
@@ -578,6 +569,12 @@ int pe_fluid_wcsph_shapes(PeWcsph* w, uint32_t out[4]) {
     return PE_OK;
 }
 
+int pe_fluid_wcsph_list_chunk(PeWcsph* w, uint32_t* out) {
+    if (!w || !out) return PE_ERR_NULL;
+    *out = w->world->shapes().list_chunk;
+    return PE_OK;
+}
+
 int pe_fluid_wcsph_get_params(PeWcsph* w, PeWcsphParams* out) {
     if (!w || !out) return PE_ERR_NULL;
     return guard([&] {
@@ -727,49 +724,29 @@ int pe_fluid_wcsph_clear_status(PeWcsph* w) {
 int pe_fluid_wcsph_diagnostics(PeWcsph* w, PeFluidDiagnostics* out) {
     if (!w || !out) return PE_ERR_NULL;
     return guard([&] {
-        pe::World& W = *w->world;
-        const uint64_t n = W.len();
-        std::vector<double> x(3 * n), v(3 * n), a(3 * n), rho(n);
-        std::vector<uint8_t> kind(n);
-        if (n) {
-            W.get_vec(0, x.data());
-            W.get_vec(1, v.data());
-            W.get_vec(2, a.data());
-            W.get_scalar(0, rho.data());
-            W.get_kind(kind.data());
-        }
-        const double m = W.mass(), rho0 = W.rest_density();
-        const double g = -W.params().gravity[2];
-        PeFluidDiagnostics d{};
-        uint64_t nf = 0;
-        double s_err = 0.0, vmax2 = 0.0, amax2 = 0.0;
-        uint64_t h = 0xcbf29ce484222325ULL;
-        for (uint64_t i = 0; i < n; ++i) {
-            if (kind[i] != PE_PARTICLE_FLUID) continue;
-            ++nf;
-            const double* xi = &x[3 * i];
-            const double* vi = &v[3 * i];
-            const double* ai = &a[3 * i];
-            d.linear_momentum[0] += vi[0] * m;  // diagnostics.rs:45 (v * mass)
-            d.linear_momentum[1] += vi[1] * m;
-            d.linear_momentum[2] += vi[2] * m;
-            const double v2 = vi[0] * vi[0] + vi[1] * vi[1] + vi[2] * vi[2];
-            d.kinetic_energy += 0.5 * m * v2;                    // diagnostics.rs:56
-            d.gravitational_potential += m * g * xi[2];          // diagnostics.rs:67
-            const double e = std::fabs(rho[i] - rho0) / rho0;    // diagnostics.rs:79
-            s_err += e;
-            if (e > d.max_density_error) d.max_density_error = e;
-            if (v2 > vmax2) vmax2 = v2;
-            amax2 = std::fmax(amax2, ai[0] * ai[0] + ai[1] * ai[1] + ai[2] * ai[2]);
-            for (int c = 0; c < 3; ++c) h = fnv1a(h, xi[c]);
-            for (int c = 0; c < 3; ++c) h = fnv1a(h, vi[c]);
-        }
-        d.total_mass = m * (double)nf;
-        d.mean_density_error = nf ? s_err / (double)nf : 0.0;
-        d.v_max = std::sqrt(vmax2);
-        d.a_max = std::sqrt(amax2);
-        d.hash64 = h;
-        *out = d;
+        pe::World::Diagnostics d{};
+        w->world->diagnostics(&d);
+        PeFluidDiagnostics r{};
+        r.total_mass = d.total_mass;
+        for (int c = 0; c < 3; ++c) r.linear_momentum[c] = d.linear_momentum[c];
+        r.kinetic_energy = d.kinetic_energy;
+        r.gravitational_potential = d.gravitational_potential;
+        r.mean_density_error = d.mean_density_error;
+        r.max_density_error = d.max_density_error;
+        r.v_max = d.v_max;
+        r.a_max = d.a_max;
+        r.hash64 = d.hash64;
+        *out = r;
+        return PE_OK;
+    });
+}
+
+int pe_fluid_wcsph_fluid_center_of_mass(PeWcsph* w, double out[3]) {
+    if (!w || !out) return PE_ERR_NULL;
+    return guard([&] {
+        pe::World::Diagnostics d{};
+        w->world->diagnostics(&d);
+        for (int c = 0; c < 3; ++c) out[c] = d.fluid_com[c];
         return PE_OK;
     });
 }

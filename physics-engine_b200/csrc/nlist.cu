@@ -24,8 +24,8 @@
 // entries per cell. k_nlist_visit writes the visit list alone (the passes that need no
 // ascending-index order).
 //
-// The kernels work on chunks of up to 64 centre particles with four threads
-// per particle. A first pass, each thread taking a quarter of the candidates
+// The kernels work on chunks of up to 64 (or 32) centre particles with four
+// (or eight) threads per particle. A first pass, each thread taking a quarter of the candidates
 // (union words, or sorted positions), keeps the in-support bit masks in shared
 // memory and counts; the chunk's longest lists size one block of the list
 // pool, reserved with one atomic add; a second pass writes the entries, each
@@ -41,8 +41,9 @@ namespace pe {
 namespace {
 
 constexpr int kNlThreads = 256;
-constexpr uint32_t kChunk = 64;                    // centre particles per chunk
-constexpr uint32_t kWays = kNlThreads / kChunk;    // threads per centre particle
+// Centre particles per chunk (a launch shape the world's autotuner picks:
+// 32 or 64); kNlThreads / chunk threads work on each centre particle.
+constexpr uint32_t kDefaultChunk = 64;
 constexpr uint32_t kWarps = kNlThreads / 32;
 // Largest stage: the fused kernel's 38 dynamic bytes per staged entry (f32
 // position 16, slot 4, sort index 2, visit masks 8, lower masks or sort
@@ -270,7 +271,9 @@ struct ChunkBlock {
 
 // Cursor over the set bits of one centre's masks (word w at m[w * kChunk]),
 // in ascending bit order: entry t of the list is the t-th set bit.
+template <uint32_t kChunk>
 struct MaskCursor {
+    static constexpr uint32_t kWays = kNlThreads / kChunk;
     const uint32_t* m;
     uint32_t w, bits;
     // Positioned on entry t0, given this centre's per-way counts cnt[r] of the
@@ -563,13 +566,14 @@ __device__ __forceinline__ void lower_slow(const StepConst& k, float r2f, const 
 // Dynamic shared memory (ucap a multiple of kStageStep): float x, y, z, w[ucap] (Stage);
 // uint32 s_ent[ucap]; uint32 s_mask[(ucap / 32) * kChunk] (word w of chunk
 // lane c at s_mask[w * kChunk + c]).
-template <int DIM, bool LOWER_FLAGS>
+template <int DIM, bool LOWER_FLAGS, uint32_t kChunk>
 __global__ void __launch_bounds__(kNlThreads) k_nlist_visit(GridDesc g, Tanks tk, StepConst k, uint32_t ucap,
                                                             const uint32_t* __restrict__ occ,
                                                             const uint32_t* __restrict__ cell_start,
                                                             StateBufs s, ListBufs l,
                                                             DeviceScalars* sc) {
     constexpr int NC = DIM == 3 ? 27 : 9;
+    constexpr uint32_t kWays = kNlThreads / kChunk;
     extern __shared__ __align__(16) unsigned char smem[];
     Stage st(reinterpret_cast<float*>(smem), ucap);
     uint32_t* s_ent = reinterpret_cast<uint32_t*>(smem) + 4 * (size_t)ucap;
@@ -650,7 +654,7 @@ __global__ void __launch_bounds__(kNlThreads) k_nlist_visit(GridDesc g, Tanks tk
                     if (blk.ok && fluidc && v0 < v1) {
                         const size_t step = 4u * nc;
                         uint32_t* pv = l.pool + 4 * (size_t)gv;
-                        MaskCursor cur(s_mask, s_cv, lane, W, v0);
+                        MaskCursor<kChunk> cur(s_mask, s_cv, lane, W, v0);
                         for (uint32_t t = v0; t < v1; ++t) {
                             const uint32_t u = cur.next();
                             uint32_t e = s_ent[u];
@@ -683,12 +687,13 @@ __global__ void __launch_bounds__(kNlThreads) k_nlist_visit(GridDesc g, Tanks tk
 // s_ent[ucap] (slot | flags); uint32 s_vmask[(ucap / 32) * kChunk]; uint16
 // s_sorted[ucap]; then a region used first by the radix sort and then by the
 // lower masks over sorted positions.
-template <int DIM>
+template <int DIM, uint32_t kChunk>
 __global__ void __launch_bounds__(kNlThreads, 2) k_nlist_both(GridDesc g, Tanks tk, StepConst k, uint32_t ucap,
                                                            const uint32_t* __restrict__ occ,
                                                            const uint32_t* __restrict__ cell_start,
                                                            StateBufs s, ListBufs l, DeviceScalars* sc) {
     constexpr int NC = DIM == 3 ? 27 : 9;
+    constexpr uint32_t kWays = kNlThreads / kChunk;
     extern __shared__ __align__(16) unsigned char smem[];
     Stage st(reinterpret_cast<float*>(smem), ucap);
     uint32_t* s_ent = reinterpret_cast<uint32_t*>(smem) + 4 * (size_t)ucap;
@@ -866,7 +871,7 @@ __global__ void __launch_bounds__(kNlThreads, 2) k_nlist_both(GridDesc g, Tanks 
                         const uint32_t v0 = nv * q / kWays, v1 = nv * (q + 1u) / kWays;
                         if (fluidc && v0 < v1) {
                             uint32_t* pv = l.pool + 4 * (size_t)gv;
-                            MaskCursor cur(s_vmask, s_cv, lane, W, v0);
+                            MaskCursor<kChunk> cur(s_vmask, s_cv, lane, W, v0);
                             for (uint32_t t = v0; t < v1; ++t) {
                                 const uint32_t u = cur.next();
                                 uint32_t e = s_ent[u];
@@ -878,7 +883,7 @@ __global__ void __launch_bounds__(kNlThreads, 2) k_nlist_both(GridDesc g, Tanks 
                         const uint32_t l0 = nl * q / kWays, l1 = nl * (q + 1u) / kWays;
                         if (l0 < l1) {
                             uint32_t* pl = l.pool + 4 * (size_t)gl;
-                            MaskCursor cur(s_lmask, s_cl, lane, WR, l0);
+                            MaskCursor<kChunk> cur(s_lmask, s_cl, lane, WR, l0);
                             for (uint32_t t = l0; t < l1; ++t)
                                 pl[(t >> 2) * step + (t & 3u)] = s_ent[s_sorted[cur.next()]] & kEntrySlotMask;
                         }
@@ -896,15 +901,17 @@ __global__ void __launch_bounds__(kNlThreads, 2) k_nlist_both(GridDesc g, Tanks 
     if (tid == 0 && max_union) atomicMax(&sc->max_union, max_union);
 }
 
-size_t both_smem_bytes(uint32_t ucap) {
+size_t both_smem_bytes(uint32_t ucap, uint32_t chunk) {
     const size_t sort = (size_t)ucap * sizeof(uint16_t) + 16 * kNlThreads * sizeof(uint16_t);
-    const size_t mask = (size_t)(ucap / 32) * kChunk * sizeof(uint32_t);
+    const size_t mask = (size_t)(ucap / 32) * chunk * sizeof(uint32_t);
     return (size_t)ucap * (sizeof(float4) + sizeof(uint32_t) + sizeof(uint16_t)) + mask + (sort > mask ? sort : mask);
 }
 
-size_t visit_smem_bytes(uint32_t ucap) {
-    return (size_t)ucap * (sizeof(float4) + sizeof(uint32_t)) + (size_t)(ucap / 32) * kChunk * sizeof(uint32_t);
+size_t visit_smem_bytes(uint32_t ucap, uint32_t chunk) {
+    return (size_t)ucap * (sizeof(float4) + sizeof(uint32_t)) + (size_t)(ucap / 32) * chunk * sizeof(uint32_t);
 }
+
+uint32_t valid_chunk(uint32_t chunk) { return chunk == 32u ? 32u : kDefaultChunk; }
 
 }  // namespace
 
@@ -918,44 +925,55 @@ uint32_t nlist_union_capacity(uint32_t max_union) {
     return (uint32_t)want;
 }
 
-size_t nlist_smem_bytes(uint32_t ucap) {
-    const size_t a = visit_smem_bytes(ucap), b = both_smem_bytes(ucap);
+size_t nlist_smem_bytes(uint32_t ucap, uint32_t chunk) {
+    chunk = valid_chunk(chunk);
+    const size_t a = visit_smem_bytes(ucap, chunk), b = both_smem_bytes(ucap, chunk);
     return a > b ? a : b;
 }
 
-uint32_t nlist_prepare(int dim, uint32_t ucap) {
-    const int sv = (int)visit_smem_bytes(ucap), sb = (int)both_smem_bytes(ucap);
+namespace {
+template <int DIM, uint32_t C>
+uint32_t prepare_for(uint32_t ucap) {
+    const int sv = (int)visit_smem_bytes(ucap, C), sb = (int)both_smem_bytes(ucap, C);
     int bv = 0, bb = 0;
-    if (dim == 3) {
-        cudaFuncSetAttribute(k_nlist_visit<3, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sv);
-        cudaFuncSetAttribute(k_nlist_both<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bv, k_nlist_visit<3, false>, kNlThreads, sv);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bb, k_nlist_both<3>, kNlThreads, sb);
-    } else {
-        cudaFuncSetAttribute(k_nlist_visit<2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sv);
-        cudaFuncSetAttribute(k_nlist_both<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bv, k_nlist_visit<2, false>, kNlThreads, sv);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bb, k_nlist_both<2>, kNlThreads, sb);
-    }
+    cudaFuncSetAttribute(k_nlist_visit<DIM, false, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, sv);
+    cudaFuncSetAttribute(k_nlist_both<DIM, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, sb);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bv, k_nlist_visit<DIM, false, C>, kNlThreads, sv);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bb, k_nlist_both<DIM, C>, kNlThreads, sb);
     const int b = bv > bb ? bv : bb;
     return b > 0 ? (uint32_t)b : 1u;
+}
+
+template <int DIM, uint32_t C>
+void launch_for(const GridDesc& g, const Tanks& tk, const StepConst& k, uint32_t ucap, uint32_t nblocks,
+                const uint32_t* occ, const uint32_t* cell_start, const StateBufs& s, const ListBufs& l,
+                DeviceScalars* sc, cudaStream_t st, bool visit_only) {
+    if (visit_only)
+        k_nlist_visit<DIM, false, C><<<nblocks, kNlThreads, visit_smem_bytes(ucap, C), st>>>(
+            g, tk, k, ucap, occ, cell_start, s, l, sc);
+    else
+        k_nlist_both<DIM, C><<<nblocks, kNlThreads, both_smem_bytes(ucap, C), st>>>(g, tk, k, ucap, occ,
+                                                                                  cell_start, s, l, sc);
+}
+}  // namespace
+
+uint32_t nlist_prepare(int dim, uint32_t ucap, uint32_t chunk) {
+    chunk = valid_chunk(chunk);
+    if (dim == 3) return chunk == 32u ? prepare_for<3, 32>(ucap) : prepare_for<3, 64>(ucap);
+    return chunk == 32u ? prepare_for<2, 32>(ucap) : prepare_for<2, 64>(ucap);
 }
 
 void launch_nlist(const GridDesc& g, const Tanks& tk, const StepConst& k, uint32_t ucap,
                   uint32_t nblocks, const uint32_t* occ, const uint32_t* cell_start,
                   const StateBufs& s, const ListBufs& l, DeviceScalars* sc, cudaStream_t st,
-                  bool visit_only) {
-    const size_t sv = visit_smem_bytes(ucap), sb = both_smem_bytes(ucap);
+                  bool visit_only, uint32_t chunk) {
+    chunk = valid_chunk(chunk);
     if (g.dim == 3) {
-        if (visit_only)
-            k_nlist_visit<3, false><<<nblocks, kNlThreads, sv, st>>>(g, tk, k, ucap, occ, cell_start, s, l, sc);
-        else
-            k_nlist_both<3><<<nblocks, kNlThreads, sb, st>>>(g, tk, k, ucap, occ, cell_start, s, l, sc);
+        if (chunk == 32u) launch_for<3, 32>(g, tk, k, ucap, nblocks, occ, cell_start, s, l, sc, st, visit_only);
+        else launch_for<3, 64>(g, tk, k, ucap, nblocks, occ, cell_start, s, l, sc, st, visit_only);
     } else {
-        if (visit_only)
-            k_nlist_visit<2, false><<<nblocks, kNlThreads, sv, st>>>(g, tk, k, ucap, occ, cell_start, s, l, sc);
-        else
-            k_nlist_both<2><<<nblocks, kNlThreads, sb, st>>>(g, tk, k, ucap, occ, cell_start, s, l, sc);
+        if (chunk == 32u) launch_for<2, 32>(g, tk, k, ucap, nblocks, occ, cell_start, s, l, sc, st, visit_only);
+        else launch_for<2, 64>(g, tk, k, ucap, nblocks, occ, cell_start, s, l, sc, st, visit_only);
     }
 }
 

@@ -130,7 +130,7 @@ __global__ void k_pressure(uint32_t n, StepConst k, Tanks tk, StateBufs s) {
 
 // Pressure + Monaghan viscosity force of fluid pair (k, j), seen from k:
 // rx = x_j - x_k (wcsph.rs:219), pi_ij(x_k, x_j, v_k, v_j, rho_k, rho_j).
-template <bool CUBIC>
+template <bool CUBIC, bool BETA0>
 __device__ __forceinline__ void fluid_pair(const StepConst& kc, double nac, double4 xk, double4 vk,
                                            double4 xj, double4 vj, double& ax, double& ay,
                                            double& az) {
@@ -146,13 +146,17 @@ __device__ __forceinline__ void fluid_pair(const StepConst& kc, double nac, doub
     // viscosity.rs:51-73 with r_ij = x_k - x_j, v_ij = v_k - v_j. Evaluated for
     // every pair and selected, so that approaching and receding pairs do not
     // split the warp; a receding pair's value is discarded (pi = 0 exactly).
-    const double qx = xk.x - xj.x, qy = xk.y - xj.y, qz = xk.z - xj.z;
+    // x_k - x_j is exactly -(x_j - x_k) (round to nearest is symmetric), so
+    // |x_k - x_j|^2 is r2 bit for bit and v_ij . (x_k - x_j) is -(v_ij . r)
+    // up to the sign of a zero, which only ever selects pi = 0.
     const double wx = vk.x - vj.x, wy = vk.y - vj.y, wz = vk.z - vj.z;
-    const double vr = wx * qx + wy * qy + wz * qz;
-    const double q2 = qx * qx + qy * qy + qz * qz;
-    const double mu = kc.h * vr / (q2 + kc.eps_h2);
+    const double vr = -(wx * rx + wy * ry + wz * rz);
+    const double mu = kc.h * vr / (r2 + kc.eps_h2);
     const double rho_bar = 0.5 * (vk.w + vj.w);
-    const double pic = (nac * mu + kc.visc_beta * mu * mu) / rho_bar;
+    // With beta = 0 the beta mu^2 term is a signed zero, which leaves the
+    // nonzero nac * mu of an approaching pair (mu < 0) unchanged.
+    const double num = BETA0 ? nac * mu : nac * mu + kc.visc_beta * mu * mu;
+    const double pic = num / rho_bar;
     const double pi = vr >= 0.0 ? 0.0 : pic;
     const double mv = -kc.mass * pi;
     ax += gx * mp + gx * mv;
@@ -179,7 +183,7 @@ __device__ __forceinline__ void boundary_pair(const StepConst& kc, double4 xk, d
     az += gz * m;
 }
 
-template <bool INTEGRATE, int DIM, bool CUBIC>
+template <bool INTEGRATE, int DIM, bool CUBIC, bool BETA0>
 __global__ void __launch_bounds__(kMaxPassThreads) k_forces(uint32_t n, StepConst kc, Tanks tk,
                                                             StateBufs s, ListBufs l, double dt,
                                                             double4* __restrict__ pos_next,
@@ -193,7 +197,6 @@ __global__ void __launch_bounds__(kMaxPassThreads) k_forces(uint32_t n, StepCons
     const double4 xk = s.pos[k];
     const double4 vk = s.vel[k];
     double ax = 0.0, ay = 0.0, az = 0.0;
-    // fluid i < k, ascending original index
     // neighbour state gathered one entry ahead (boundary samples need no velocity)
     auto load = [&](uint32_t e) {
         PosVel d;
@@ -202,43 +205,63 @@ __global__ void __launch_bounds__(kMaxPassThreads) k_forces(uint32_t n, StepCons
         d.v = (e & kEntryBoundary) ? make_double4(0.0, 0.0, 0.0, 0.0) : s.vel[j];
         return d;
     };
-    for_each_loaded(list_ref(l, k, kListLower), load, [&](uint32_t, const PosVel& d) {
-        fluid_pair<CUBIC>(kc, nac, xk, vk, d.x, d.v, ax, ay, az);
-    });
-    // fluid j > k and boundary j, visiting order: the visit list without the
-    // entries flagged lower (those came from the lower list, in index order).
-    // The list is taken in chunks of kCompact entries whose kept entries are
-    // first compacted into this thread's column of shared memory, so the pair
-    // loop of a warp runs over kept entries only (the flagged ones are about
-    // half and fall at different positions in each thread's list).
+    // One stream of pairs per thread: the lower list (fluid i < k, ascending
+    // original index), then the visit list without the entries flagged lower
+    // (fluid j > k and boundary j, visiting order; the flagged ones came from
+    // the lower list). Each thread refills its own column of shared memory,
+    // kCompact entries of a list at a time, when it runs empty, so the warp's
+    // pair code runs with every lane that still has pairs; lanes do not wait
+    // for the fullest lane of each chunk, only for the longest stream.
     extern __shared__ uint32_t s_keep[];  // kCompact x blockDim.x, column per thread
     const uint32_t tid = threadIdx.x, bd = blockDim.x;
-    const ListRef vr = list_ref(l, k, kListVisit);
-    for (uint32_t t0 = 0; t0 < vr.n; t0 += kCompact) {
-        const uint32_t t1 = min(vr.n, t0 + kCompact);
-        uint32_t c = 0;
-        for (uint32_t t = t0; t < t1; t += 4) {
-            const uint4 g4 = __ldg(reinterpret_cast<const uint4*>(vr.p + (size_t)(t >> 2) * vr.step));
-            const uint32_t ge[4] = {g4.x, g4.y, g4.z, g4.w};
+    const ListRef lo = list_ref(l, k, kListLower);
+    const ListRef vi = list_ref(l, k, kListVisit);
+    uint32_t lt = 0, vt = 0;  // next unread entry of each list
+    uint32_t c = 0, u = 0;    // buffered entries, next buffered entry
+    uint32_t e = 0;
+    PosVel d{};
+    for (;;) {
+        if (u == c) {
+            c = 0;
+            u = 0;
+            if (lt < lo.n) {
+                const uint32_t t1 = min(lo.n, lt + kCompact);
+                for (uint32_t t = lt; t < t1; t += 4) {
+                    const uint4 g4 = __ldg(reinterpret_cast<const uint4*>(lo.p + (size_t)(t >> 2) * lo.step));
+                    const uint32_t ge[4] = {g4.x, g4.y, g4.z, g4.w};
 #pragma unroll
-            for (uint32_t q = 0; q < 4; ++q)
-                if (t + q < t1 && !(ge[q] & kEntryLower)) s_keep[(c++) * bd + tid] = ge[q];
-        }
-        if (c == 0) continue;
-        uint32_t e = s_keep[tid];
-        PosVel d = load(e);
-        for (uint32_t u = 0; u < c; ++u) {
-            const uint32_t ec = e;
-            const PosVel dc = d;
-            if (u + 1 < c) {
-                e = s_keep[(u + 1) * bd + tid];
-                d = load(e);
-            }
-            if (ec & kEntryBoundary) {
-                boundary_pair<CUBIC>(kc, xk, dc.x, (ec & kEntryOriented) != 0u, s.nout, ec & kEntrySlotMask, ax, ay, az);
+                    for (uint32_t q = 0; q < 4; ++q)
+                        if (t + q < t1) s_keep[(c++) * bd + tid] = ge[q];
+                }
+                lt = t1;
             } else {
-                fluid_pair<CUBIC>(kc, nac, xk, vk, dc.x, dc.v, ax, ay, az);
+                while (c == 0 && vt < vi.n) {
+                    const uint32_t t1 = min(vi.n, vt + kCompact);
+                    for (uint32_t t = vt; t < t1; t += 4) {
+                        const uint4 g4 = __ldg(reinterpret_cast<const uint4*>(vi.p + (size_t)(t >> 2) * vi.step));
+                        const uint32_t ge[4] = {g4.x, g4.y, g4.z, g4.w};
+#pragma unroll
+                        for (uint32_t q = 0; q < 4; ++q)
+                            if (t + q < t1 && !(ge[q] & kEntryLower)) s_keep[(c++) * bd + tid] = ge[q];
+                    }
+                    vt = t1;
+                }
             }
+            if (c == 0) break;  // both lists done
+            e = s_keep[tid];
+            d = load(e);
+        }
+        // the current pair, with the next buffered neighbour's state in flight
+        const uint32_t ec = e;
+        const PosVel dc = d;
+        if (++u < c) {
+            e = s_keep[u * bd + tid];
+            d = load(e);
+        }
+        if (ec & kEntryBoundary) {
+            boundary_pair<CUBIC>(kc, xk, dc.x, (ec & kEntryOriented) != 0u, s.nout, ec & kEntrySlotMask, ax, ay, az);
+        } else {
+            fluid_pair<CUBIC, BETA0>(kc, nac, xk, vk, dc.x, dc.v, ax, ay, az);
         }
     }
     ax += kc.gx;
@@ -378,24 +401,32 @@ void launch_forces(uint32_t n, uint32_t threads, const StepConst& k, const Tanks
     const uint32_t b = blocks_for(n, threads);
     const size_t sm = (size_t)kCompact * threads * sizeof(uint32_t);
     const bool cubic = k.kernel == 0;
-#define PE_FORCES(I, D, C) k_forces<I, D, C><<<b, threads, sm, st>>>(n, k, tk, s, l, dt, pos_next, vel_next, st_a)
+#define PE_FORCES(I, D, C, B) \
+    k_forces<I, D, C, B><<<b, threads, sm, st>>>(n, k, tk, s, l, dt, pos_next, vel_next, st_a)
+#define PE_FORCES_B(I, D, C)              \
+    do {                                  \
+        if (beta0) PE_FORCES(I, D, C, true); \
+        else PE_FORCES(I, D, C, false);   \
+    } while (0)
+    const bool beta0 = k.visc_beta == 0.0;
     if (k.dim == 3) {
         if (cubic) {
-            if (integrate) PE_FORCES(true, 3, true);
-            else PE_FORCES(false, 3, true);
+            if (integrate) PE_FORCES_B(true, 3, true);
+            else PE_FORCES_B(false, 3, true);
         } else {
-            if (integrate) PE_FORCES(true, 3, false);
-            else PE_FORCES(false, 3, false);
+            if (integrate) PE_FORCES_B(true, 3, false);
+            else PE_FORCES_B(false, 3, false);
         }
     } else {
         if (cubic) {
-            if (integrate) PE_FORCES(true, 2, true);
-            else PE_FORCES(false, 2, true);
+            if (integrate) PE_FORCES_B(true, 2, true);
+            else PE_FORCES_B(false, 2, true);
         } else {
-            if (integrate) PE_FORCES(true, 2, false);
-            else PE_FORCES(false, 2, false);
+            if (integrate) PE_FORCES_B(true, 2, false);
+            else PE_FORCES_B(false, 2, false);
         }
     }
+#undef PE_FORCES_B
 #undef PE_FORCES
 }
 

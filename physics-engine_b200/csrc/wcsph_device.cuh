@@ -225,16 +225,17 @@ void launch_gather(uint32_t n, const uint32_t* perm, const StateBufs& src, const
 
 // ----- neighbour lists -----
 uint32_t nlist_union_capacity(uint32_t max_union);
-size_t nlist_smem_bytes(uint32_t ucap);
+size_t nlist_smem_bytes(uint32_t ucap, uint32_t chunk = 64);
 void launch_surface_tension(uint32_t n, const StepConst& k, const SurfConst& c, const StateBufs& s,
                             const ListBufs& l, double4* normals, double4* out, cudaStream_t st);
 // Sets the dynamic shared-memory limit of the list kernel for this stage size
 // and returns how many of its CTAs fit on one SM.
-uint32_t nlist_prepare(int dim, uint32_t ucap);
+// chunk = centre particles per chunk of the list build (32 or 64).
+uint32_t nlist_prepare(int dim, uint32_t ucap, uint32_t chunk = 64);
 void launch_nlist(const GridDesc& g, const Tanks& tk, const StepConst& k, uint32_t ucap,
                   uint32_t nblocks, const uint32_t* occ, const uint32_t* cell_start,
                   const StateBufs& s, const ListBufs& l, DeviceScalars* sc, cudaStream_t st,
-                  bool visit_only = false);
+                  bool visit_only = false, uint32_t chunk = 64);
 
 // ----- SPH passes -----
 void launch_density(uint32_t n, uint32_t threads, const StepConst& k, const StateBufs& s,

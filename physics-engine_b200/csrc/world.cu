@@ -581,7 +581,7 @@ void World::ensure_lists(bool visit_only) {
             check(cudaMemsetAsync(&sc_->list_used, 0, sizeof(unsigned long long), st_), "memset");
             prof_begin(kLists);
             launch_nlist(g_, tanks_, kc_, ucap_, nl_blocks_, occ_, cell_start_, cur_, lists_, sc_, st_,
-                         build_visit_only);
+                         build_visit_only, list_chunk_);
             prof_end();
             launches_ += 1;
             check(cudaGetLastError(), "neighbour lists");
@@ -869,7 +869,7 @@ bool World::capture_graph(double dt) {
 }
 
 void World::configure_lists() {
-    uint32_t per_sm = nlist_prepare(dim_, ucap_);
+    uint32_t per_sm = nlist_prepare(dim_, ucap_, list_chunk_);
     check(cudaGetLastError(), "nlist prepare");
     const uint32_t mult = list_ctas_per_sm_ ? list_ctas_per_sm_ : std::max<uint32_t>(per_sm, 1u) * 4u;
     nl_blocks_ = sms_ * mult;
@@ -882,6 +882,7 @@ World::Shapes World::shapes() const {
     r.forces = shape_.forces;
     r.xsph = shape_.xsph;
     r.list_ctas_per_sm = nl_blocks_ / std::max<uint32_t>(sms_, 1u);
+    r.list_chunk = list_chunk_;
     return r;
 }
 
@@ -939,25 +940,38 @@ World::Shapes World::autotune() {
     });
     if (!f32_ && prm_.xsph_epsilon != 0.0)
         pick(shape_.xsph, [&] { launch_xsph(n, shape_.xsph, kc_, cur_, lists_, vel_nx_, st_); });
-    // list-build CTAs per SM: multiples of the resident count
+    // list build: tile (centre particles per chunk) x CTAs per SM (multiples
+    // of the resident count). The lists' entries and order do not depend on
+    // either; a smaller chunk never asks for more of the pool (each chunk
+    // reserves its longest list's rows), so the pool sized at creation fits.
     {
-        const uint32_t per_sm = std::max<uint32_t>(nlist_prepare(dim_, ucap_), 1u);
         float best = 0.f;
-        uint32_t best_m = 0;
-        for (uint32_t m : {1u, 2u, 4u, 8u}) {
-            nl_blocks_ = sms_ * per_sm * m;
-            const float ms = time_it([&] {
-                check(cudaMemsetAsync(&sc_->list_used, 0, sizeof(unsigned long long), st_), "memset");
-                launch_nlist(g_, tanks_, kc_, ucap_, nl_blocks_, occ_, cell_start_, cur_, lists_, sc_, st_,
-                             !lists_full_);
-            });
-            if (best_m == 0 || ms < best) {
-                best = ms;
-                best_m = per_sm * m;
+        uint32_t best_m = 0, best_c = list_chunk_;
+        for (uint32_t chunk : {64u, 32u}) {
+            const uint32_t per_sm = std::max<uint32_t>(nlist_prepare(dim_, ucap_, chunk), 1u);
+            for (uint32_t m : {1u, 2u, 4u, 8u}) {
+                nl_blocks_ = sms_ * per_sm * m;
+                const float ms = time_it([&] {
+                    check(cudaMemsetAsync(&sc_->list_used, 0, sizeof(unsigned long long), st_), "memset");
+                    launch_nlist(g_, tanks_, kc_, ucap_, nl_blocks_, occ_, cell_start_, cur_, lists_, sc_, st_,
+                                 !lists_full_, chunk);
+                });
+                if (best_m == 0 || ms < best) {
+                    best = ms;
+                    best_m = per_sm * m;
+                    best_c = chunk;
+                }
             }
         }
+        list_chunk_ = best_c;
         list_ctas_per_sm_ = best_m;
+        nlist_prepare(dim_, ucap_, list_chunk_);
         nl_blocks_ = sms_ * best_m;
+        // the lists in the pool now come from the last timed build; rebuild
+        // them with the chosen shape so their layout is the one used from now
+        check(cudaMemsetAsync(&sc_->list_used, 0, sizeof(unsigned long long), st_), "memset");
+        launch_nlist(g_, tanks_, kc_, ucap_, nl_blocks_, occ_, cell_start_, cur_, lists_, sc_, st_, !lists_full_,
+                     list_chunk_);
     }
     check(cudaGetLastError(), "autotune");
     event_pool_.push_back(a);

@@ -96,6 +96,15 @@ class World {
     void get_neighbour_counts(uint32_t* candidates, uint32_t* in_support);
     uint32_t status();
     void clear_status();
+    // diagnostics.rs:19-102 and wcsph.rs:350-369, reduced on the device with
+    // the reference's bits (sums in original index order); no state copy.
+    struct Diagnostics {
+        double total_mass, linear_momentum[3], kinetic_energy, gravitational_potential;
+        double mean_density_error, max_density_error, v_max, a_max;
+        uint64_t hash64, fluid;
+        double fluid_com[3];  // sum of fluid positions in index order / fluid count
+    };
+    void diagnostics(Diagnostics* out);
     // status, largest union, list groups the last build asked for, union stage
     // capacity, list pool groups, occupied cells, dense cells, list-build CTAs
     void capacity_info(uint64_t* out);
@@ -115,10 +124,12 @@ class World {
     void profile_read(double* ms, uint64_t* count, bool reset);
 
     // Launch shapes picked by autotune(): block sizes of the density, force and
-    // XSPH passes and the list-build CTAs per SM. Timing repeats idempotent
+    // XSPH passes, and the list build's CTAs per SM and tile (centre particles
+    // per chunk, 32 or 64). Timing repeats idempotent
     // passes on the current state, so the simulation does not advance.
     struct Shapes {
         uint32_t density, forces, xsph, list_ctas_per_sm;
+        uint32_t list_chunk;  // centre particles per chunk of the list build (32 or 64)
     };
     Shapes shapes() const;
     Shapes autotune();
@@ -204,6 +215,7 @@ class World {
     std::vector<TankDesc> tank_host_;
     PassShape shape_{};
     uint32_t list_ctas_per_sm_ = 0;  // 0: four times the resident count
+    uint32_t list_chunk_ = 64;       // centre particles per list-build chunk
     StepConst kc_{};
     uint32_t ucap_ = 0, nl_blocks_ = 0, sms_ = 148;
 
@@ -219,6 +231,7 @@ class World {
     uint32_t* insup_ = nullptr;
     DeviceScalars* sc_ = nullptr;
     double* xfer_ = nullptr;  // n * 4 doubles of export/import staging
+    unsigned char* diag_buf_ = nullptr;  // diagnostics: results, hash tables and maps
     std::vector<void*> allocs_;
     std::vector<void*> list_allocs_;
 

@@ -222,6 +222,8 @@ def load_library():
         "pe_fluid_wcsph_clear_status": (C.c_int, [vp]),
         "pe_fluid_wcsph_capacity_info": (C.c_int, [vp, vp]),
         "pe_fluid_wcsph_diagnostics": (C.c_int, [vp, C.POINTER(_Diag)]),
+        "pe_fluid_wcsph_fluid_center_of_mass": (C.c_int, [vp, C.POINTER(C.c_double)]),
+        "pe_fluid_wcsph_list_chunk": (C.c_int, [vp, C.POINTER(C.c_uint32)]),
         "pe_fluid_wcsph_kernel_launches": (C.c_int, [vp, C.POINTER(u64), i32]),
         "pe_fluid_wcsph_profile": (C.c_int, [vp, i32]),
         "pe_fluid_wcsph_profile_read": (C.c_int, [vp, C.POINTER(_Profile), i32]),
@@ -570,16 +572,21 @@ class WcsphWorld:
         return out
 
     def autotune(self) -> dict:
-        """Pick the passes' block sizes and the list-build CTAs per SM by timing
-        them on the current state (the simulation does not advance)."""
+        """Pick the passes' block sizes and the list build's tile and CTAs per
+        SM by timing them on the current state (the simulation does not
+        advance)."""
         out = np.zeros(4, np.uint32)
         _ok(_lib.pe_fluid_wcsph_autotune(self._w, _ptr(out)), "autotune")
-        return dict(zip(("density", "forces", "xsph", "list_ctas_per_sm"), (int(v) for v in out)))
+        return self.shapes()
 
     def shapes(self) -> dict:
         out = np.zeros(4, np.uint32)
         _ok(_lib.pe_fluid_wcsph_shapes(self._w, _ptr(out)), "shapes")
-        return dict(zip(("density", "forces", "xsph", "list_ctas_per_sm"), (int(v) for v in out)))
+        r = dict(zip(("density", "forces", "xsph", "list_ctas_per_sm"), (int(v) for v in out)))
+        c = C.c_uint32(0)
+        _ok(_lib.pe_fluid_wcsph_list_chunk(self._w, C.byref(c)), "list_chunk")
+        r["list_chunk"] = int(c.value)
+        return r
 
     def close(self):
         if getattr(self, "_w", None) and _lib is not None:
@@ -739,6 +746,12 @@ class WcsphWorld:
                     kinetic_energy=d.kinetic_energy, gravitational_potential=d.gravitational_potential,
                     mean_density_error=d.mean_density_error, max_density_error=d.max_density_error,
                     v_max=d.v_max, a_max=d.a_max, hash64=d.hash64)
+
+    def fluid_center_of_mass(self) -> np.ndarray:
+        """Fluid positions summed in index order on the device / fluid count."""
+        out = (C.c_double * 3)()
+        _ok(_lib.pe_fluid_wcsph_fluid_center_of_mass(self._w, out), "fluid_center_of_mass")
+        return np.array(out[:])
 
     def v_max(self):
         return self.diagnostics()["v_max"]

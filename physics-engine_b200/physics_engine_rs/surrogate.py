@@ -178,6 +178,34 @@ def run_learned(world, surrogate: Surrogate, dt: float, steps: int, judge_every:
                 plain_steps=int(out[3]), max_error=float(out[4]), last_error=float(out[5]))
 
 
+def heldout_comparison(surrogate: Surrogate, world, dt: float, steps_before: int = 150, tank: int = 0) -> dict:
+    """One-step prediction loss on a world never trained on (the mean of the
+    normalised squared error over tank `tank`'s fluid particles, the training
+    loss), after `steps_before` plain steps, for three predictors of the next
+    plain step's (a, drho/dt): the trained network; the mean prediction (the
+    network's output zeroed); and persistence (the previous plain step's
+    (dv/dt, drho/dt) reused, which needs no network)."""
+    a, b = tank_range(world, tank)
+    world.run(dt, max(steps_before - 1, 0))
+    # tanks are stored tank-major: original indices [a, b) are the tank's
+    v0, r0 = world.velocities()[a:b], world.densities()[a:b]
+    world.step(dt)
+    v1, r1 = world.velocities()[a:b], world.densities()[a:b]
+    surrogate.graph_from_world(world, a, b)
+    world.step(dt)
+    v2, r2 = world.velocities()[a:b], world.densities()[a:b]
+    surrogate.targets_from_world(world, dt, update_stats=False)
+    trained = surrogate.train_step(0.0)
+    fluid = world.kinds()[a:b] == 0
+    mean, std = (np.asarray(t, np.float64) for t in surrogate.stats())
+    t_prev = np.concatenate([(v1 - v0) / dt, ((r1 - r0) / dt)[:, None]], axis=1)[fluid]
+    t_now = np.concatenate([(v2 - v1) / dt, ((r2 - r1) / dt)[:, None]], axis=1)[fluid]
+    persist = float((((t_prev - t_now) / std) ** 2).sum(axis=1).mean())
+    mean_pred = float((((t_now - mean) / std) ** 2).sum(axis=1).mean())
+    return {"trained": float(trained), "mean_prediction": mean_pred, "persistence": persist,
+            "after_steps": steps_before, "fluid_particles": int(fluid.sum())}
+
+
 def train_on_rollouts(surrogate: Surrogate, world, dt: float, steps: int, iters_per_step: int = 2,
                       lr: float = 1e-3, stat_steps: int = 20, log=None):
     """Online training on a (batched) world's plain rollout. The first

@@ -91,3 +91,16 @@ def test_batch_f32_runs_close_to_f64():
     assert np.max(np.abs(r32 - r64) / r64) < 2e-4
     w64.close()
     w32.close()
+
+
+def test_phase_boundary_probe():
+    """The probe behind the batched form's design choice: a graph kernel node
+    and a bounded grid barrier both cost microseconds per phase boundary."""
+    import ctypes as C
+
+    f = pe.load_library().pe_fluid_probe_phase_overhead
+    f.argtypes = [C.c_int32, C.c_uint32, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    a, b = C.c_double(0.0), C.c_double(0.0)
+    assert f(0, 32, C.byref(a), C.byref(b)) == pe.PE_OK
+    assert 0.0 < a.value < 1000.0 and 0.0 < b.value < 1000.0, (a.value, b.value)
+    assert f(0, 1, C.byref(a), C.byref(b)) == pe.PE_ERR_ARG
