@@ -150,6 +150,13 @@ def max_over_ranks(x: float, torch) -> float:
     return float(t.item())
 
 
+def job_throughput(units_per_rank, steps, slowest_ms, ranks):
+    """Whole-job particle-steps/s: every rank advances its own tank(s) of
+    `units_per_rank` fluid particles for `steps` steps; the job's time is the
+    slowest rank's (max over ranks)."""
+    return ranks * units_per_rank * steps / (slowest_ms / 1e3)
+
+
 def build_scene(pe, workload):
     (nx, ny, nz), box = WORKLOADS[workload]
     mass = pe.mass_from_spacing(1000.0, DX, 3)
@@ -460,7 +467,7 @@ def run_batched(args, ws, rank, local, torch, pe):
     status = w.status()
     cap = w.capacity_info()
     ms = max_over_ranks(ms, torch)
-    value = ws * nf * args.steps / (ms / 1e3)
+    value = job_throughput(nf, args.steps, ms, ws)
     w.close()
     del w
 
@@ -716,7 +723,7 @@ def run_solver_form(args, ws, rank, local, torch, pe):
     clocks = sampler.stop()
     status = w.status()
     ms = max_over_ranks(ms, torch)
-    value = ws * nf * args.steps / (ms / 1e3)
+    value = job_throughput(nf, args.steps, ms, ws)
     fluid = w.kinds() == 0
     rho = w.densities()[fluid]
     v = w.velocities()[fluid]
@@ -816,7 +823,7 @@ def main():
     status = world.status()
     cap = world.capacity_info()
     ms = max_over_ranks(ms, torch)
-    value = ws * nf * args.steps / (ms / 1e3)
+    value = job_throughput(nf, args.steps, ms, ws)
 
     # ---- end-to-end through the public API with host buffers ----
     if args.e2e_steps <= 0:
