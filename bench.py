@@ -95,7 +95,9 @@ def _args():
     ap.add_argument("--f32-timed-steps", type=int, default=20)
     ap.add_argument("--leg-train-tanks", type=int, default=4,
                     help="plain form's learned leg: seeded 64k-particle training tanks")
-    ap.add_argument("--leg-train-steps", type=int, default=100)
+    ap.add_argument("--leg-train-steps", type=int, default=150)
+    ap.add_argument("--leg-warm-steps", type=int, default=100,
+                    help="learned form: untimed plain steps of the bench tank before the rollout")
     ap.add_argument("--leg-rollout-steps", type=int, default=50)
     return ap.parse_args()
 
@@ -520,7 +522,7 @@ def run_batched(args, ws, rank, local, torch, pe):
         print(json.dumps(line), flush=True)
 
 
-def learned_leg(workload, local, torch, pe, train_tanks, train_steps, rollout_steps):
+def learned_leg(workload, local, torch, pe, train_tanks, train_steps, rollout_steps, warm_steps=100):
     """The learned surrogate: trained online on plain rollouts of seeded
     64k-particle tanks (tank extents 0.45..1.0 m), then the bench tank run with
     learned steps judged every 10 steps by the plain SPH density (a window
@@ -556,6 +558,11 @@ def learned_leg(workload, local, torch, pe, train_tanks, train_steps, rollout_st
     learned = pe.WcsphWorld(ps, prm, pe.WcsphConfig(device=local))
     del ps
     steps = rollout_steps
+    # both worlds leave the lattice start's first steps (never trained on)
+    # with untimed plain steps
+    if warm_steps:
+        plain.run(DT, warm_steps)
+        learned.run(DT, warm_steps)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     plain.run(DT, steps)
@@ -576,7 +583,8 @@ def learned_leg(workload, local, torch, pe, train_tanks, train_steps, rollout_st
     com_l, e_l, _ = _device_summary(learned)
     leg = {
         "value": nf * steps / learned_s, "unit": UNIT, "ms_per_step": learned_s / steps * 1e3,
-        "rollout_steps": steps, "dtype": "bf16 network (fp32 accumulation), f64 state",
+        "rollout_steps": steps, "plain_steps_before_rollout": warm_steps,
+        "dtype": "bf16 network (fp32 accumulation), f64 state",
         "network": "2-hop message passing, MLP width 128 x 2 hidden layers, r_msg = h",
         "judge_every": 10, "fallback_bound": 0.01,
         "training": {"tanks": train_tanks, "particles_per_tank": 64000,
@@ -587,7 +595,7 @@ def learned_leg(workload, local, torch, pe, train_tanks, train_steps, rollout_st
         "speedup_vs_plain_step": plain_s / learned_s,
         "heldout_one_step_loss": heldout,
         "judge": st, "fallback_rate": st["fallbacks"] / max(1, st["windows"]),
-        "error_vs_f64": {"after_steps": steps, "density_rel_max": float(rel.max()),
+        "error_vs_f64": {"after_steps": warm_steps + steps, "density_rel_max": float(rel.max()),
                          "density_rel_mean": float(rel.mean()),
                          "position_rms_m": float(np.sqrt(((x_l - x64) ** 2).sum(1).mean())),
                          "com_drift_m": float(np.linalg.norm(com_l - com64)),
@@ -602,7 +610,7 @@ def learned_leg(workload, local, torch, pe, train_tanks, train_steps, rollout_st
 
 def run_learned_form(args, ws, rank, local, torch, pe):
     leg, nf = learned_leg(args.workload, local, torch, pe, args.train_tanks, args.train_steps,
-                          args.rollout_steps)
+                          args.rollout_steps, args.leg_warm_steps)
     line = {
         "metric": "SPH fluid particle-steps/s @1M (learned surrogate, judged every 10 steps)",
         "value": leg["value"], "unit": UNIT, "n_gpus": 1, "steps": leg["rollout_steps"], "warmup": 0,
@@ -925,7 +933,7 @@ def main():
                             args.f32_steps)
         forms["f32"] = leg
         leg, _ = learned_leg(args.workload, local, torch, pe, args.leg_train_tanks, args.leg_train_steps,
-                             args.leg_rollout_steps)
+                             args.leg_rollout_steps, args.leg_warm_steps)
         forms["learned"] = leg
         line["forms"] = forms
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
