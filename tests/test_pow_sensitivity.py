@@ -43,3 +43,17 @@ def test_last_ulp_pow_moves_a_small_tank_less_than_1e10_after_100_steps(rate):
     assert 0.0 < dv, "the perturbation must reach the state"
     assert dx < 1e-10 and dv < 1e-10, (rate, dx, dv)
 
+
+
+def test_recorded_c1_sensitivity_within_1e10_after_100_steps():
+    """pow_sensitivity_c1.json (made by golden/make_pow_sensitivity.py on the
+    32^3 dam break): every rate stays below 1e-10 at 100 steps; the 1000-step
+    figures are recorded for the report. The record's unperturbed run is the
+    golden C1 run (same hashes)."""
+    rec = json.load(open(os.path.join(HERE, "golden", "pow_sensitivity_c1.json")))
+    gold = json.load(open(os.path.join(HERE, "golden", "c1_dam_break_32k.json")))
+    for steps in ("1", "10", "100", "1000"):
+        assert rec["records"][steps]["base_hash"] == gold["records"][steps]["hash64"], steps
+    for r in rec["rates"]:
+        at100 = rec["records"]["100"][str(r)]
+        assert 0.0 < at100["v_rel"] < 1e-10 and at100["x_rel"] < 1e-10, (r, at100)
