@@ -24,8 +24,10 @@
 // entries per cell. k_nlist_visit writes the visit list alone (the passes that need no
 // ascending-index order).
 //
-// The kernels work on chunks of up to 64 (or 32) centre particles with four
-// (or eight) threads per particle. A first pass, each thread taking a quarter of the candidates
+// The kernels work on chunks of up to 32 (or 64) centre particles with eight
+// (or four) threads per particle; the fused kernel is compiled for three
+// resident CTAs per SM (80 registers), which the 32-centre tile's shared
+// memory allows. A first pass, each thread taking a quarter of the candidates
 // (union words, or sorted positions), keeps the in-support bit masks in shared
 // memory and counts; the chunk's longest lists size one block of the list
 // pool, reserved with one atomic add; a second pass writes the entries, each
@@ -42,7 +44,8 @@ namespace {
 
 constexpr int kNlThreads = 256;
 // Centre particles per chunk (a launch shape the world's autotuner picks:
-// 32 or 64); kNlThreads / chunk threads work on each centre particle.
+// 32, the world's default, or 64); kNlThreads / chunk threads work on each
+// centre particle. kDefaultChunk is what an unknown value falls back to.
 constexpr uint32_t kDefaultChunk = 64;
 constexpr uint32_t kWarps = kNlThreads / 32;
 // Largest stage: the fused kernel's 38 dynamic bytes per staged entry (f32
@@ -688,7 +691,7 @@ __global__ void __launch_bounds__(kNlThreads) k_nlist_visit(GridDesc g, Tanks tk
 // s_sorted[ucap]; then a region used first by the radix sort and then by the
 // lower masks over sorted positions.
 template <int DIM, uint32_t kChunk>
-__global__ void __launch_bounds__(kNlThreads, 2) k_nlist_both(GridDesc g, Tanks tk, StepConst k, uint32_t ucap,
+__global__ void __launch_bounds__(kNlThreads, 3) k_nlist_both(GridDesc g, Tanks tk, StepConst k, uint32_t ucap,
                                                            const uint32_t* __restrict__ occ,
                                                            const uint32_t* __restrict__ cell_start,
                                                            StateBufs s, ListBufs l, DeviceScalars* sc) {
@@ -916,9 +919,12 @@ uint32_t valid_chunk(uint32_t chunk) { return chunk == 32u ? 32u : kDefaultChunk
 }  // namespace
 
 uint32_t nlist_union_capacity(uint32_t max_union) {
-    // The largest union seen plus a quarter, in steps of kStageStep, within
-    // the shared-memory limit; larger unions take the slow path.
-    uint64_t want = (uint64_t)max_union + max_union / 4u;
+    // The largest union seen plus an eighth, in steps of kStageStep, within
+    // the shared-memory limit; larger unions take the slow path. The margin
+    // is kept small so that three CTAs of the fused kernel fit an SM at the
+    // 32-centre tile (at 1M: a 2,304-entry stage, 75 KB per CTA; with a
+    // quarter's margin the stage was 2,560 entries and two CTAs fit).
+    uint64_t want = (uint64_t)max_union + max_union / 8u;
     want = (want + kStageStep - 1) / kStageStep * kStageStep;
     if (want < kStageStep) want = kStageStep;
     if (want > kMaxUnionStage) want = kMaxUnionStage;

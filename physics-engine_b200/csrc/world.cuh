@@ -215,7 +215,7 @@ class World {
     std::vector<TankDesc> tank_host_;
     PassShape shape_{};
     uint32_t list_ctas_per_sm_ = 0;  // 0: four times the resident count
-    uint32_t list_chunk_ = 64;       // centre particles per list-build chunk
+    uint32_t list_chunk_ = 32;       // centre particles per list-build chunk
     StepConst kc_{};
     uint32_t ucap_ = 0, nl_blocks_ = 0, sms_ = 148;
 
