@@ -52,11 +52,11 @@ FORCE_OPS_PER_PAIR = 65.0
 # DRAM bytes (read + write) of one force-pass launch per fluid particle, from
 # the ncu capture of the 262,144-particle dam break (the neighbour lists
 # dominate; traffic grows with the particle count).
-FORCE_TRAFFIC_PER_FLUID = (427.213568e6 + 20.616448e6) / 262144
+FORCE_TRAFFIC_PER_FLUID = (428.454400e6 + 20.749056e6) / 262144
 # sm__pipe_fp64_cycles_active of the force pass in the same capture
-FORCE_FP64_PIPE_ACTIVE = 0.550
+FORCE_FP64_PIPE_ACTIVE = 0.512
 # smsp__issue_active of the list build (k_nlist_both) in the same capture
-LISTS_ISSUE_ACTIVE = 0.435
+LISTS_ISSUE_ACTIVE = 0.592
 # Whole step, per fluid / per boundary particle (cell key 28 + sort 8 +
 # density 32 + XSPH 80 + forces 104; boundary 28 + 8 + 3 x 24).
 STEP_BYTES_FLUID, STEP_BYTES_BOUNDARY = 252.0, 108.0
