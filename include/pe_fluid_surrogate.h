@@ -40,7 +40,12 @@ int pe_surrogate_get_grad(PeSurrogate* s, int32_t i, float* W, float* b);
 int pe_surrogate_set_graph(PeSurrogate* s, int32_t n, int32_t E, const int32_t* row, const int32_t* src,
                            const float* f, const float* xe, const uint8_t* fluid);
 int pe_surrogate_set_targets(PeSurrogate* s, const float* t); /* n x 4, normalised */
-int pe_surrogate_forward(PeSurrogate* s, float* y);           /* n x 4, normalised */
+int pe_surrogate_forward(PeSurrogate* s, float* y);
+/* Inference runs each hop's edge MLP and its sum per destination as one fused
+ * tensor-core kernel (on = 1, the default) or as the three GEMMs and the
+ * segment sum that training uses (on = 0); the two differ only in the order
+ * of the fp32 message sums. */
+int pe_surrogate_set_fused_edges(PeSurrogate* s, int32_t on);           /* n x 4, normalised */
 /* Forward, loss (mean over fluid nodes of the squared error), backward; one
  * Adam step when lr > 0. */
 int pe_surrogate_train_step(PeSurrogate* s, float lr, float* loss);

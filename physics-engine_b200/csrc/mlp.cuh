@@ -1,5 +1,5 @@
-// Learned surrogate: tensor-core GEMM building block and the message-passing
-// network kernels (mlp_gemm.cu, surrogate.cu).
+// Learned surrogate: tensor-core GEMM building block, the fused edge MLP and
+// the message-passing network kernels (mlp_gemm.cu, edge_fused.cu, surrogate.cu).
 #pragma once
 
 #include <cstddef>
@@ -31,6 +31,30 @@ struct GemmArgs {
     const int* idx1 = nullptr;
     int ld_add = 0;
 };
+
+// One hop's edge MLP fused into one persistent kernel (edge_fused.cu), for
+// inference: out[dst[e]] += relu(relu(x_e Wc + b1 + P[dst[e]] + Q[src[e]]) W2
+// + b2) W3 + b3 over the E edges (sorted by destination); out [n x 128] must
+// be zero. P, Q fp32 [n x 128]; x_e bf16 [E x 16]; Wc, W2, W3 bf16 K-major
+// ([128 x 16], [128 x 128], [128 x 128]).
+struct EdgeHopArgs {
+    int E;
+    const int* src;
+    const int* dst;
+    const __nv_bfloat16* xe;
+    const float* P;
+    const float* Q;
+    const __nv_bfloat16* Wc;
+    const float* b1;
+    const __nv_bfloat16* W2;
+    const float* b2;
+    const __nv_bfloat16* W3;
+    const float* b3;
+    float* out;
+    uint32_t* err;  // bit 0: a bounded wait ran out
+};
+bool edge_hop_prepare();
+void launch_edge_hop(const EdgeHopArgs& a, int sms, cudaStream_t st);
 
 size_t gemm_smem_bytes();
 bool gemm_prepare();

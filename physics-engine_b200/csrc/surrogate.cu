@@ -236,6 +236,12 @@ Surrogate::Surrogate(uint64_t seed, double r_msg_over_h) : r_msg_over_h_(r_msg_o
     cu(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking), "stream");
     own_stream_ = true;
     if (!gemm_prepare()) throw std::runtime_error("surrogate: GEMM shared-memory limit");
+    if (!edge_hop_prepare()) throw std::runtime_error("surrogate: fused edge kernel shared-memory limit");
+    {
+        int dev = 0;
+        if (cudaGetDevice(&dev) == cudaSuccess)
+            cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, dev);
+    }
     err_ = dalloc<uint32_t>(1);
     allocs_.push_back(err_);
     loss_ = dalloc<float>(1);
@@ -489,7 +495,13 @@ void Surrogate::forward(bool keep_for_backward) {
         const int base = 3 + 8 * l;
         linear_fwd(layers_[base + 0], hb_[l], n, P_, nullptr, false);
         linear_fwd(layers_[base + 1], hb_[l], n, Q_, nullptr, false);
-        if (E > 0) {
+        if (E > 0 && fused_edges_ && !keep_for_backward) {
+            // the whole edge MLP and the sum per destination in one kernel
+            const Linear &L0 = layers_[base + 2], &L1 = layers_[base + 3], &L2 = layers_[base + 4];
+            cu(cudaMemsetAsync(A_, 0, sizeof(float) * nW, st_), "memset");
+            EdgeHopArgs ea{E, g_.src, g_.dst, g_.xe, P_, Q_, L0.Wt16, L0.b, L1.Wt16, L1.b, L2.Wt16, L2.b, A_, err_};
+            launch_edge_hop(ea, sms_, st_);
+        } else if (E > 0) {
             // layer 1: relu(x_e Wc + b1 + P[dst] + Q[src]), the gathers fused into the GEMM's epilogue
             const Linear& L0 = layers_[base + 2];
             GemmArgs ga{g_.xe, L0.Wt16, nullptr, eh1_[l], L0.b, E, L0.Np, L0.K, L0.K, L0.K, L0.Np, 1, err_};
@@ -502,7 +514,8 @@ void Surrogate::forward(bool keep_for_backward) {
             linear_fwd(layers_[base + 3], eh1_[l], E, nullptr, eh2_[l], true);
             linear_fwd(layers_[base + 4], eh2_[l], E, M_, nullptr, false);
         }
-        k_segsum<<<blocks((size_t)n * 32, 256), 256, 0, st_>>>(n, g_.row, M_, 1.f, A_);
+        if (!(E > 0 && fused_edges_ && !keep_for_backward))
+            k_segsum<<<blocks((size_t)n * 32, 256), 256, 0, st_>>>(n, g_.row, M_, 1.f, A_);
         k_concat<<<blocks(2 * nW, 256), 256, 0, st_>>>(n, hb_[l], A_, kAggScale, xn_[l]);
         mlp_fwd(base + 5, xn_[l], n, na1_[l], na2_[l], U_);
         k_residual<<<blocks(nW, 256), 256, 0, st_>>>(n, U_, g_.fluid, h_, hb_[l + 1]);

@@ -100,6 +100,11 @@ class Surrogate {
     cudaStream_t stream() const { return st_; }
     void set_stream(cudaStream_t s) { st_ = s; }
     uint32_t device_error();
+    // inference (forward without backward) runs each hop's edge MLP as one
+    // fused kernel (edge_fused.cu) when on; off: the three GEMMs and the
+    // segment sum that training uses
+    void set_fused_edges(bool on) { fused_edges_ = on; }
+    bool fused_edges() const { return fused_edges_; }
 
    private:
     void alloc_params(uint64_t seed);
@@ -130,6 +135,8 @@ class Surrogate {
     double st_count_ = 0.0;
     int adam_t_ = 0;
     uint32_t* err_ = nullptr;
+    bool fused_edges_ = false;
+    int sms_ = 148;
     float* loss_ = nullptr;
     float* part_ = nullptr;
     size_t part_floats_ = 0;

@@ -131,6 +131,12 @@ int pe_surrogate_forward(PeSurrogate* s, float* y) {
     });
 }
 
+int pe_surrogate_set_fused_edges(PeSurrogate* s, int32_t on) {
+    if (!s) return PE_ERR_NULL;
+    s->s->set_fused_edges(on != 0);
+    return PE_OK;
+}
+
 int pe_surrogate_train_step(PeSurrogate* s, float lr, float* loss) {
     if (!s) return PE_ERR_NULL;
     return guard_s([&] {

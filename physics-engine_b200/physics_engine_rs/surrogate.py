@@ -20,6 +20,7 @@ _SIGS = {
                                          C.c_void_p, C.c_void_p]),
     "pe_surrogate_set_targets": (C.c_int, [C.c_void_p, C.c_void_p]),
     "pe_surrogate_forward": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "pe_surrogate_set_fused_edges": (C.c_int, [C.c_void_p, C.c_int32]),
     "pe_surrogate_train_step": (C.c_int, [C.c_void_p, C.c_float, C.POINTER(C.c_float)]),
     "pe_surrogate_get_stats": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "pe_surrogate_set_stats": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
@@ -113,6 +114,11 @@ class Surrogate:
         y = np.zeros((self.n, 4), np.float32)
         _ok(self._L.pe_surrogate_forward(self._s, _ptr(y)), "forward")
         return y
+
+    def set_fused_edges(self, on: bool):
+        """Inference's edge MLP as one fused kernel (True, the default) or as
+        the GEMMs and segment sum that training uses (False)."""
+        _ok(self._L.pe_surrogate_set_fused_edges(self._s, 1 if on else 0), "set_fused_edges")
 
     def train_step(self, lr: float = 0.0) -> float:
         loss = C.c_float()
