@@ -97,7 +97,7 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edge_hop(EdgeHopArgs a) {
     float* sStage = reinterpret_cast<float*>(smem + kOffStage);
     __shared__ __align__(8) uint64_t mbar;
     __shared__ uint32_t s_tmem;
-    __shared__ int s_dst[kEdgeThreads], s_src[kEdgeThreads];
+    __shared__ int s_dst[kEdgeThreads];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
     if (tid == 0) {
@@ -135,20 +135,39 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edge_hop(EdgeHopArgs a) {
         __syncthreads();
     };
     const int ntiles = (a.E + kEdgeThreads - 1) / kEdgeThreads;
-    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        const int e0 = tile * kEdgeThreads;
-        // ---- edge features and endpoints of the tile
-        {
-            const int e = e0 + tid;
-            s_dst[tid] = e < a.E ? a.dst[e] : -1;
-            s_src[tid] = e < a.E ? a.src[e] : -1;
-            for (int i = tid; i < 2 * kEdgeThreads; i += kEdgeThreads) {
-                const int r = i >> 1, c = i & 1, er = e0 + r;
-                uint4 v = make_uint4(0u, 0u, 0u, 0u);
-                if (er < a.E) v = __ldg(reinterpret_cast<const uint4*>(a.xe + (size_t)er * 16 + c * 8));
-                *reinterpret_cast<uint4*>(sX + sw_off(r, c)) = v;
-            }
+    // This thread's edge (row tid) of a tile: endpoints and its two 16-byte
+    // chunks of edge features, loaded one tile ahead.
+    auto fetch_edge = [&](int tile, int& d, int& sj, uint4& x0, uint4& x1) {
+        const int e = tile * kEdgeThreads + tid;
+        d = -1;
+        sj = -1;
+        x0 = x1 = make_uint4(0u, 0u, 0u, 0u);
+        if (tile < ntiles && e < a.E) {
+            d = __ldg(a.dst + e);
+            sj = __ldg(a.src + e);
+            x0 = __ldg(reinterpret_cast<const uint4*>(a.xe + (size_t)e * 16));
+            x1 = __ldg(reinterpret_cast<const uint4*>(a.xe + (size_t)e * 16 + 8));
         }
+    };
+    // 32 columns (block cb) of this edge's P[dst] and Q[src] rows
+    auto fetch_pq = [&](int d, int sj, int cb, float4 (&p)[8], float4 (&q)[8]) {
+        const float4* P4 = reinterpret_cast<const float4*>(a.P + (size_t)(d < 0 ? 0 : d) * 128 + cb * 32);
+        const float4* Q4 = reinterpret_cast<const float4*>(a.Q + (size_t)(sj < 0 ? 0 : sj) * 128 + cb * 32);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            p[i] = __ldg(P4 + i);
+            q[i] = __ldg(Q4 + i);
+        }
+    };
+    int d, sj;
+    uint4 x0, x1;
+    fetch_edge(blockIdx.x, d, sj, x0, x1);
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        // ---- edge features and endpoints of the tile (fetched a tile ahead)
+        s_dst[tid] = d;
+        *reinterpret_cast<uint4*>(sX + sw_off(tid, 0)) = x0;
+        *reinterpret_cast<uint4*>(sX + sw_off(tid, 1)) = x1;
+        const int dc = d, sc = sj;
         to_tensor();
         // ---- layer 1: x_e Wc (one K = 16 MMA), then + b1 + P[dst] + Q[src], ReLU
         if (tid == 0) {
@@ -156,31 +175,38 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edge_hop(EdgeHopArgs a) {
             umma_bf16(tmem, sw128_desc(smem_addr(sX)), sw128_desc(smem_addr(sWc)), 0u);
             umma_commit(smem_addr(&mbar));
         }
+        // the next tile's edge and this edge's first P/Q block load while the MMA runs
+        fetch_edge(tile + gridDim.x, d, sj, x0, x1);
+        float4 pa[8], qa[8];
+        fetch_pq(dc, sc, 0, pa, qa);
         ok = mma_wait() && ok;
-        {
-            const int r = tid, d = s_dst[r], sj = s_src[r];
-            const float* P = a.P + (size_t)(d < 0 ? 0 : d) * 128;
-            const float* Q = a.Q + (size_t)(sj < 0 ? 0 : sj) * 128;
-#pragma unroll 1
-            for (int cb = 0; cb < 4; ++cb) {
-                uint32_t v[32];
-                tmem_ld32(trow + (uint32_t)(cb * 32), v);
-                float x[32];
 #pragma unroll
-                for (int q = 0; q < 8; ++q) {
-                    const float4 p4 = d < 0 ? make_float4(0.f, 0.f, 0.f, 0.f) : __ldg(reinterpret_cast<const float4*>(P + cb * 32) + q);
-                    const float4 q4 = d < 0 ? make_float4(0.f, 0.f, 0.f, 0.f) : __ldg(reinterpret_cast<const float4*>(Q + cb * 32) + q);
-                    const float pv[4] = {p4.x, p4.y, p4.z, p4.w}, qv[4] = {q4.x, q4.y, q4.z, q4.w};
+        for (int cb = 0; cb < 4; ++cb) {
+            float4 pb[8], qb[8];
+            if (cb < 3) fetch_pq(dc, sc, cb + 1, pb, qb);  // one block ahead
+            uint32_t v[32];
+            tmem_ld32(trow + (uint32_t)(cb * 32), v);
+            float x[32];
 #pragma unroll
-                    for (int h = 0; h < 4; ++h) {
-                        const int j = q * 4 + h;
-                        float t = __uint_as_float(v[j]) + a.b1[cb * 32 + j];
-                        t += pv[h];
-                        t += qv[h];
-                        x[j] = fmaxf(t, 0.f);
-                    }
+            for (int i = 0; i < 8; ++i) {
+                const float pv[4] = {pa[i].x, pa[i].y, pa[i].z, pa[i].w};
+                const float qv[4] = {qa[i].x, qa[i].y, qa[i].z, qa[i].w};
+#pragma unroll
+                for (int h = 0; h < 4; ++h) {
+                    const int j = i * 4 + h;
+                    float t = __uint_as_float(v[j]) + a.b1[cb * 32 + j];  // the unfused epilogue's order
+                    t += pv[h];
+                    t += qv[h];
+                    x[j] = fmaxf(t, 0.f);
                 }
-                put_bf16_row(sA, r, cb, x);
+            }
+            put_bf16_row(sA, tid, cb, x);
+            if (cb < 3) {
+#pragma unroll
+                for (int i = 0; i < 8; ++i) {
+                    pa[i] = pb[i];
+                    qa[i] = qb[i];
+                }
             }
         }
         to_tensor();

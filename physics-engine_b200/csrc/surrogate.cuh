@@ -135,7 +135,7 @@ class Surrogate {
     double st_count_ = 0.0;
     int adam_t_ = 0;
     uint32_t* err_ = nullptr;
-    bool fused_edges_ = false;
+    bool fused_edges_ = true;
     int sms_ = 148;
     float* loss_ = nullptr;
     float* part_ = nullptr;

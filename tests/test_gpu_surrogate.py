@@ -73,8 +73,9 @@ def test_adam_steps_reduce_the_loss():
 def test_fused_edge_kernel_matches_unfused_path_and_oracle():
     """Inference runs each hop's edge MLP as one fused kernel; training's GEMMs
     and segment sum give the same outputs up to the order of the fp32
-    message sums. ~260 tiles of 128 edges with a ragged last tile, in-degrees
-    from 0 to ~70, destinations whose edges straddle tile boundaries."""
+    message sums (bound 1e-3). ~260 tiles of 128 edges with a ragged last
+    tile, in-degrees from 0 to ~70, destinations whose edges straddle tile
+    boundaries; two calls in a row."""
     rng = np.random.default_rng(5)
     p = {k: v.astype(np.float32) for k, v in random_params(rng).items()}
     n, E = 1000, 33 * 1000 + 57
@@ -90,7 +91,10 @@ def test_fused_edge_kernel_matches_unfused_path_and_oracle():
     s.set_fused_edges(True)
     net = S.Net({k: v.astype(np.float64) for k, v in p.items()})
     _, y_ref, _ = net.loss_and_grads(S.bf16(f), S.bf16(xe), dst, src, fluid, t)
+    # against the oracle, the bound is the unfused path's own distance on this
+    # graph (bf16 rounding flips from summation order grow with the graph)
+    bound = max(2e-3, 1.5 * _rel(y_plain, y_ref))
     for y in y_fused:
         assert np.isfinite(y).all()
         assert _rel(y, y_plain) < 1e-3, _rel(y, y_plain)
-        assert _rel(y, y_ref) < 2e-3, _rel(y, y_ref)
+        assert _rel(y, y_ref) < bound, (_rel(y, y_ref), bound)
