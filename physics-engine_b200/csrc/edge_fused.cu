@@ -10,9 +10,13 @@
 // which the unfused path computes as three GEMM launches writing E x 128
 // activations to memory (~60 GB of traffic per hop at 3.3e7 edges) and a
 // segment sum. Here one persistent CTA per SM keeps Wc, W2 and W3 in shared
-// memory and walks tiles of 128 edges: x_e W c is one K=16 tcgen05 MMA into
-// the tensor-memory accumulator; the epilogue (thread r = edge r = TMEM lane
-// r) adds b1, P[i] and Q[j] in the unfused epilogue's order, applies ReLU and
+// memory; its two warpgroups walk their own tiles of 128 edges, each with its
+// own 128 tensor-memory columns, buffers and barriers, so one group's MMA
+// waits and gathers overlap the other's epilogues. Per tile, x_e Wc is one
+// K=16 tcgen05 MMA into the group's accumulator; the epilogue (thread r =
+// edge r = TMEM lane r) adds b1, P[i] and Q[j] in the unfused epilogue's
+// order (the next tile's endpoints and features, and the next 32-column block
+// of P[i] and Q[j], are already loading), applies ReLU and
 // writes bf16 into a swizzled shared-memory tile that is the A operand of
 // the next 8 MMAs (K = 128), and so on; the last epilogue stages the
 // messages in shared memory and sums each run of equal destinations before
@@ -35,19 +39,40 @@ namespace {
 
 using namespace umma;
 
-constexpr int kEdgeThreads = 128;        // one thread per edge of a tile (TMEM lane)
+constexpr int kGroups = 2;             // warpgroups per CTA, each on its own tiles
+constexpr int kGroupThreads = 128;     // one thread per edge of a tile (TMEM lane)
+constexpr int kEdgeThreads = kGroups * kGroupThreads;
 constexpr uint32_t kSlice = 128u * 128u;  // bytes of a 128-row x 64-column bf16 slice
 constexpr uint32_t kOffWc = 0;                    // Wc^T [128 x 16]: chunks 0-1 of one slice
 constexpr uint32_t kOffW2 = kOffWc + kSlice;      // W2^T [128 x 128]: two slices
 constexpr uint32_t kOffW3 = kOffW2 + 2 * kSlice;  // W3^T: two slices
-constexpr uint32_t kOffX = kOffW3 + 2 * kSlice;   // edge features [128 x 16]: chunks 0-1
-constexpr uint32_t kOffA = kOffX + kSlice;        // activations [128 x 128]: two slices
-constexpr uint32_t kOffStage = kOffA + 2 * kSlice;  // fp32 messages, 128 rows x 32 columns
-constexpr uint32_t kStageLd = 33;                   // padded row (conflict-free both ways)
-constexpr uint32_t kSmemBytes = kOffStage + 128u * kStageLd * 4u + 1024u;  // + alignment slack
+constexpr uint32_t kOffGroup = kOffW3 + 2 * kSlice;
+// per warpgroup: the edge-feature slice [128 x 16] (chunks 0-1), which the
+// last epilogue reuses for the fp32 messages (128 rows x 32 columns, column
+// j of row r at j ^ (r & 31)), then the activation tile [128 x 128]
+constexpr uint32_t kGroupBytes = 3 * kSlice;
+constexpr uint32_t kSmemBytes = kOffGroup + kGroups * kGroupBytes + 1024u;  // + alignment slack
 
 __device__ __forceinline__ uint32_t sw_off(int row, int chunk) {
     return (uint32_t)row * 128u + ((uint32_t)(chunk ^ (row & 7)) << 4);
+}
+
+// barrier of warpgroup g alone (ids 1, 2; 0 is __syncthreads')
+__device__ __forceinline__ void group_sync(int g) {
+    asm volatile("bar.sync %0, %1;" ::"r"(g + 1), "r"(kGroupThreads) : "memory");
+}
+// the same barrier, returning whether v holds on every thread of the group
+__device__ __forceinline__ bool group_all(int g, bool v) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 p, %1, 0;\n\t"
+        "bar.red.and.pred q, %2, %3, p;\n\t"
+        "selp.u32 %0, 1, 0, q;\n\t}"
+        : "=r"(r)
+        : "r"((uint32_t)v), "r"(g + 1), "r"(kGroupThreads)
+        : "memory");
+    return r != 0;
 }
 
 // Rows 0..127 of a K-major bf16 matrix (row length ld) into swizzled slices:
@@ -89,24 +114,26 @@ __device__ __forceinline__ void issue_k128(uint32_t tmem, const uint8_t* sA, con
 __global__ void __launch_bounds__(kEdgeThreads) k_edge_hop(EdgeHopArgs a) {
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+    __shared__ __align__(8) uint64_t mbar[kGroups];
+    __shared__ uint32_t s_tmem;
+    __shared__ int s_dst[kGroups][kGroupThreads];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int g = tid / kGroupThreads, gt = tid % kGroupThreads, gw = gt >> 5;
     uint8_t* sWc = smem + kOffWc;
     uint8_t* sW2 = smem + kOffW2;
     uint8_t* sW3 = smem + kOffW3;
-    uint8_t* sX = smem + kOffX;
-    uint8_t* sA = smem + kOffA;
-    float* sStage = reinterpret_cast<float*>(smem + kOffStage);
-    __shared__ __align__(8) uint64_t mbar;
-    __shared__ uint32_t s_tmem;
-    __shared__ int s_dst[kEdgeThreads];
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    uint8_t* sX = smem + kOffGroup + (uint32_t)g * kGroupBytes;
+    float* sStage = reinterpret_cast<float*>(sX);  // free once the tile's first MMA completed
+    uint8_t* sA = sX + kSlice;
+    int* dstv = s_dst[g];
 
     if (tid == 0) {
-        mbar_init(smem_addr(&mbar), 1);
+        for (int i = 0; i < kGroups; ++i) mbar_init(smem_addr(&mbar[i]), 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&s_tmem)),
-                     "r"(128u)
+                     "r"(128u * kGroups)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
@@ -118,13 +145,14 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edge_hop(EdgeHopArgs a) {
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    const uint32_t tmem = s_tmem;
-    const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);  // this warp's lanes
+    const uint32_t tmem = s_tmem + 128u * (uint32_t)g;            // this group's 128 columns
+    const uint32_t trow = tmem + ((uint32_t)(gw * 32) << 16);      // this warp's lanes (warp % 4)
+    const uint32_t bar = smem_addr(&mbar[g]);
 
     bool ok = true;
     uint32_t phase = 0u;
     auto mma_wait = [&]() {
-        const bool done = mbar_wait(smem_addr(&mbar), phase);
+        const bool done = mbar_wait(bar, phase);
         phase ^= 1u;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         return done;
@@ -132,13 +160,14 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edge_hop(EdgeHopArgs a) {
     auto to_tensor = [&]() {  // generic-proxy shared writes visible to the MMAs, TMEM reads done
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-        __syncthreads();
+        group_sync(g);
     };
-    const int ntiles = (a.E + kEdgeThreads - 1) / kEdgeThreads;
-    // This thread's edge (row tid) of a tile: endpoints and its two 16-byte
+    const int ntiles = (a.E + kGroupThreads - 1) / kGroupThreads;
+    const int stride = (int)gridDim.x * kGroups;
+    // This thread's edge (row gt) of a tile: endpoints and its two 16-byte
     // chunks of edge features, loaded one tile ahead.
     auto fetch_edge = [&](int tile, int& d, int& sj, uint4& x0, uint4& x1) {
-        const int e = tile * kEdgeThreads + tid;
+        const int e = tile * kGroupThreads + gt;
         d = -1;
         sj = -1;
         x0 = x1 = make_uint4(0u, 0u, 0u, 0u);
@@ -161,22 +190,23 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edge_hop(EdgeHopArgs a) {
     };
     int d, sj;
     uint4 x0, x1;
-    fetch_edge(blockIdx.x, d, sj, x0, x1);
-    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int first = (int)blockIdx.x * kGroups + g;
+    fetch_edge(first, d, sj, x0, x1);
+    for (int tile = first; tile < ntiles; tile += stride) {
         // ---- edge features and endpoints of the tile (fetched a tile ahead)
-        s_dst[tid] = d;
-        *reinterpret_cast<uint4*>(sX + sw_off(tid, 0)) = x0;
-        *reinterpret_cast<uint4*>(sX + sw_off(tid, 1)) = x1;
+        dstv[gt] = d;
+        *reinterpret_cast<uint4*>(sX + sw_off(gt, 0)) = x0;
+        *reinterpret_cast<uint4*>(sX + sw_off(gt, 1)) = x1;
         const int dc = d, sc = sj;
         to_tensor();
         // ---- layer 1: x_e Wc (one K = 16 MMA), then + b1 + P[dst] + Q[src], ReLU
-        if (tid == 0) {
+        if (gt == 0) {
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             umma_bf16(tmem, sw128_desc(smem_addr(sX)), sw128_desc(smem_addr(sWc)), 0u);
-            umma_commit(smem_addr(&mbar));
+            umma_commit(bar);
         }
         // the next tile's edge and this edge's first P/Q block load while the MMA runs
-        fetch_edge(tile + gridDim.x, d, sj, x0, x1);
+        fetch_edge(tile + stride, d, sj, x0, x1);
         float4 pa[8], qa[8];
         fetch_pq(dc, sc, 0, pa, qa);
         ok = mma_wait() && ok;
@@ -200,7 +230,7 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edge_hop(EdgeHopArgs a) {
                     x[j] = fmaxf(t, 0.f);
                 }
             }
-            put_bf16_row(sA, tid, cb, x);
+            put_bf16_row(sA, gt, cb, x);
             if (cb < 3) {
 #pragma unroll
                 for (int i = 0; i < 8; ++i) {
@@ -211,10 +241,10 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edge_hop(EdgeHopArgs a) {
         }
         to_tensor();
         // ---- layer 2: relu(z1 W2 + b2)
-        if (tid == 0) {
+        if (gt == 0) {
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             issue_k128(tmem, sA, sW2);
-            umma_commit(smem_addr(&mbar));
+            umma_commit(bar);
         }
         ok = mma_wait() && ok;
 #pragma unroll 1
@@ -224,14 +254,14 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edge_hop(EdgeHopArgs a) {
             float x[32];
 #pragma unroll
             for (int j = 0; j < 32; ++j) x[j] = fmaxf(__uint_as_float(v[j]) + a.b2[cb * 32 + j], 0.f);
-            put_bf16_row(sA, tid, cb, x);  // the MMAs that read sA have completed
+            put_bf16_row(sA, gt, cb, x);  // the MMAs that read sA have completed
         }
         to_tensor();
         // ---- layer 3: m_e = z2 W3 + b3, summed per destination
-        if (tid == 0) {
+        if (gt == 0) {
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             issue_k128(tmem, sA, sW3);
-            umma_commit(smem_addr(&mbar));
+            umma_commit(bar);
         }
         ok = mma_wait() && ok;
 #pragma unroll 1
@@ -239,41 +269,42 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edge_hop(EdgeHopArgs a) {
             uint32_t v[32];
             tmem_ld32(trow + (uint32_t)(cb * 32), v);
 #pragma unroll
-            for (int j = 0; j < 32; ++j) sStage[tid * kStageLd + j] = __uint_as_float(v[j]) + a.b3[cb * 32 + j];
-            __syncthreads();
-            // thread (group g, column j): rows 32 g .. 32 g + 31, one atomic per run of a destination
-            const int j = lane, g = warp;
+            for (int j = 0; j < 32; ++j) sStage[gt * 32 + (j ^ (gt & 31))] = __uint_as_float(v[j]) + a.b3[cb * 32 + j];
+            group_sync(g);
+            // thread (warp gw, column j): rows 32 gw .. 32 gw + 31, one atomic per run of a destination
+            const int j = lane;
             int cur = -1;
             float acc = 0.f;
             for (int rr = 0; rr < 32; ++rr) {
-                const int row = g * 32 + rr, d = s_dst[row];
-                if (d < 0) break;  // rows past the last edge close the tile
-                if (d != cur) {
+                const int row = gw * 32 + rr, dd = dstv[row];
+                if (dd < 0) break;  // rows past the last edge close the tile
+                if (dd != cur) {
                     if (cur >= 0) atomicAdd(a.out + (size_t)cur * 128 + cb * 32 + j, acc);
-                    cur = d;
+                    cur = dd;
                     acc = 0.f;
                 }
-                acc += sStage[row * kStageLd + j];
+                acc += sStage[row * 32 + (j ^ (row & 31))];
             }
             if (cur >= 0) atomicAdd(a.out + (size_t)cur * 128 + cb * 32 + j, acc);
-            __syncthreads();  // the staging buffer is reused by the next column block
+            group_sync(g);  // the staging buffer is reused by the next column block
         }
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-        // the tile's TMEM reads and shared-memory use end before the next
-        // tile; a run-out wait on any thread stops every thread (a decision
-        // all threads share, so none is left at a barrier)
-        ok = __syncthreads_and(ok ? 1 : 0) != 0;
+        // the tile's TMEM reads and shared-memory use end before the group's
+        // next tile; a run-out wait on any thread of the group stops the whole
+        // group (a decision its threads share, so none is left at a barrier)
+        ok = group_all(g, ok);
         if (!ok) break;
     }
     // every committed MMA completes before the tensor memory is freed
-    if (tid == 0) umma_commit(smem_addr(&mbar));
+    if (gt == 0) umma_commit(bar);
     ok = mma_wait() && ok;
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     if (warp == 0) {
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(128u) : "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(s_tmem), "r"(128u * kGroups)
+                     : "memory");
     }
-    if (!ok && tid == 0) atomicOr(a.err, 1u);
+    if (!ok && gt == 0) atomicOr(a.err, 1u);
 }
 
 }  // namespace
@@ -285,8 +316,9 @@ bool edge_hop_prepare() {
 
 void launch_edge_hop(const EdgeHopArgs& a, int sms, cudaStream_t st) {
     if (a.E <= 0) return;
-    const int ntiles = (a.E + kEdgeThreads - 1) / kEdgeThreads;
-    const int grid = ntiles < sms ? ntiles : sms;
+    const int ntiles = (a.E + kGroupThreads - 1) / kGroupThreads;
+    const int ctas = (ntiles + kGroups - 1) / kGroups;
+    const int grid = ctas < sms ? ctas : sms;
     k_edge_hop<<<grid, kEdgeThreads, kSmemBytes, st>>>(a);
 }
 
