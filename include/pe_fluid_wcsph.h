@@ -347,6 +347,14 @@ int pe_fluid_wcsph_autotune(PeWcsph* w, uint32_t out[4]);
 int pe_fluid_wcsph_shapes(PeWcsph* w, uint32_t out[4]);
 /* The list build's tile in use: centre particles per chunk (32 or 64). */
 int pe_fluid_wcsph_list_chunk(PeWcsph* w, uint32_t* out);
+/* Pair weights: the density pass keeps each neighbour entry's W(r) for the
+ * XSPH pass of the same lists and positions (on by default for the f64 step;
+ * a device buffer of twice the neighbour-list pool, allocated only while the
+ * device has room for it and 2 GB besides). on = 0 frees it and XSPH
+ * recomputes W. Results are identical either way. pe_fluid_wcsph_pair_weights
+ * reports whether the buffer is in use (1) or not (0). */
+int pe_fluid_wcsph_set_pair_weights(PeWcsph* w, int32_t on);
+int pe_fluid_wcsph_pair_weights(PeWcsph* w, int32_t* out);
 
 /* WcsphWorld::step (wcsph.rs:326). Synchronous; returns PE_ERR_BOUNDS if the
  * step raised PE_STATUS_DOMAIN or PE_STATUS_NEIGHBOUR_OVERFLOW. */

@@ -444,6 +444,7 @@ int pe_fluid_wcsph_create_batch(const PeWcsphParams* params, int32_t dim, double
             ps = zero.data();
         }
         pe::WorldConfig wc = to_config(cfg);
+        wc.pair_weights = 1;
         auto* w = new pe::World(to_world(*params), wc, dim, rest_density, mass, h, n, x, v, kind, ps,
                                 n_out, tank_offsets, n_tanks);
         *out = new PeWcsph{w};
@@ -572,6 +573,20 @@ int pe_fluid_wcsph_shapes(PeWcsph* w, uint32_t out[4]) {
 int pe_fluid_wcsph_list_chunk(PeWcsph* w, uint32_t* out) {
     if (!w || !out) return PE_ERR_NULL;
     *out = w->world->shapes().list_chunk;
+    return PE_OK;
+}
+
+int pe_fluid_wcsph_set_pair_weights(PeWcsph* w, int32_t on) {
+    if (!w) return PE_ERR_NULL;
+    return guard([&] {
+        w->world->set_pair_weights(on != 0);
+        return PE_OK;
+    });
+}
+
+int pe_fluid_wcsph_pair_weights(PeWcsph* w, int32_t* out) {
+    if (!w || !out) return PE_ERR_NULL;
+    *out = w->world->pair_weights() ? 1 : 0;
     return PE_OK;
 }
 

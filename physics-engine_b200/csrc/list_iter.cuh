@@ -44,15 +44,17 @@ __device__ __forceinline__ void for_each_loaded(const ListRef r, Load&& load, F&
     }
 }
 
-// for_each_loaded with the data of the next two entries in flight.
+// Calls f(t, entry, data) over a slot's list in order (t the entry's
+// position), data = load(t, entry), with the data of the next two entries in
+// flight.
 template <class Load, class F>
-__device__ __forceinline__ void for_each_loaded2(const ListRef r, Load&& load, F&& f) {
+__device__ __forceinline__ void for_each_loaded2_t(const ListRef r, Load&& load, F&& f) {
     const uint32_t n = r.n;
     if (n == 0) return;
     auto at = [&](uint32_t t) { return __ldg(r.p + (size_t)(t >> 2) * r.step + (t & 3u)); };
     uint32_t e0 = at(0), e1 = n > 1 ? at(1) : 0u, e2 = n > 2 ? at(2) : 0u;
-    auto d0 = load(e0);
-    auto d1 = n > 1 ? load(e1) : d0;
+    auto d0 = load(0u, e0);
+    auto d1 = n > 1 ? load(1u, e1) : d0;
     for (uint32_t t = 0; t < n; ++t) {
         const uint32_t e = e0;
         const auto d = d0;
@@ -60,11 +62,19 @@ __device__ __forceinline__ void for_each_loaded2(const ListRef r, Load&& load, F
         d0 = d1;
         if (t + 2 < n) {
             e1 = e2;
-            d1 = load(e2);
+            d1 = load(t + 2, e2);
             if (t + 3 < n) e2 = at(t + 3);
         }
-        f(e, d);
+        f(t, e, d);
     }
+}
+
+// for_each_loaded with the data of the next two entries in flight.
+template <class Load, class F>
+__device__ __forceinline__ void for_each_loaded2(const ListRef r, Load&& load, F&& f) {
+    for_each_loaded2_t(
+        r, [&](uint32_t, uint32_t e) { return load(e); },
+        [&](uint32_t, uint32_t e, const auto& d) { f(e, d); });
 }
 
 // Entries a chunk compacts at most (see for_each_kept).

@@ -31,7 +31,12 @@ namespace pe {
 namespace {
 
 constexpr int kThreads = 128;
-constexpr uint32_t kCompact = 32;  // visit entries compacted per chunk in the force pass
+// Visit entries compacted per chunk in the force pass. 64 rather than 32: the
+// warp's pair loop runs to the fullest lane of each chunk, and the spread of
+// the kept counts shrinks relative to their mean as the chunk grows (forces
+// 3.32 -> 3.17 ms at 1M). 64 x 4 bytes per thread is 32 KB per 128-thread
+// CTA, which still leaves the pass register-limited (five CTAs per SM).
+constexpr uint32_t kCompact = 64;
 
 inline uint32_t blocks_for(uint64_t n, uint32_t t) { return (uint32_t)((n + t - 1) / t); }
 
@@ -50,18 +55,34 @@ __global__ void __launch_bounds__(kMaxPassThreads) k_density(uint32_t n, StepCon
     }
     const double4 xi = s.pos[i];
     double rho = k.rho_self;  // 0.0 + mass * W(0)
-    for_each_loaded2(
-        list_ref(l, i, kListVisit), [&](uint32_t e) { return s.pos[e & kEntrySlotMask]; },
-        [&](uint32_t e, const double4& xj) {
+    const ListRef vr = list_ref(l, i, kListVisit);
+    // W of entry t kept at the entry's pool index for the XSPH pass, two
+    // entries per 16-byte store (a whole sector over a group's four entries)
+    double* const wp = l.wpair ? l.wpair + (vr.p - l.pool) : nullptr;
+    double wprev = 0.0;
+    for_each_loaded2_t(
+        vr, [&](uint32_t, uint32_t e) { return s.pos[e & kEntrySlotMask]; },
+        [&](uint32_t t, uint32_t e, const double4& xj) {
         const uint32_t j = e & kEntrySlotMask;
         const double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
         const double r = sqrt(dx * dx + dy * dy + dz * dz);
         const double wij = kw<CUBIC>(r, k);
+        if (wp) {
+            if (t & 1u) {
+                *reinterpret_cast<double2*>(wp + (size_t)(t >> 2) * vr.step + (t & 2u)) = make_double2(wprev, wij);
+            } else {
+                wprev = wij;
+            }
+        }
         if ((e & kEntryOriented) && !sees_fluid(k, xj, s.nout[j], xi.x, xi.y, xi.z)) return;
         // fluid: mass * W; boundary: (rho0 * psi_j) * W (wcsph.rs:143-148)
         const double f = (e & kEntryBoundary) ? k.rho0 * xj.w : k.mass;
         rho += f * wij;
     });
+    if (wp && (vr.n & 1u)) {  // the last entry's W, unpaired
+        const uint32_t t = vr.n - 1u;
+        *reinterpret_cast<double2*>(wp + (size_t)(t >> 2) * vr.step + (t & 2u)) = make_double2(wprev, 0.0);
+    }
     rho = fmax(rho, 1e-12);  // wcsph.rs:152 (f64::max)
     s.vel[i].w = rho;
     // keep the cached p / rho^2 consistent with the new rho (the reference
@@ -218,18 +239,24 @@ __global__ void __launch_bounds__(kMaxPassThreads) k_forces(uint32_t n, StepCons
     // in step across the warp: a per-lane stream that refilled each lane's
     // buffer when it ran empty made the warp wait on every lane's list loads
     // in turn (forces 3.47 -> 4.75 ms at 1M, 19 of 32 lanes active).
+    // The chunks are aligned to the list's end (the first one is the short
+    // one): the kept entries cluster at the end of the visiting order (the
+    // neighbour cells after the particle's own), so there every lane's chunk
+    // is full and none waits on a fuller one.
     extern __shared__ uint32_t s_keep[];  // kCompact x blockDim.x, column per thread
     const uint32_t tid = threadIdx.x, bd = blockDim.x;
     const ListRef vr = list_ref(l, k, kListVisit);
-    for (uint32_t t0 = 0; t0 < vr.n; t0 += kCompact) {
-        const uint32_t t1 = min(vr.n, t0 + kCompact);
+    const uint32_t nv4 = (vr.n + 3u) & ~3u;  // chunk ends stay on 16-byte groups
+    uint32_t t1 = nv4 ? nv4 - (nv4 - 1u) / kCompact * kCompact : 0u;
+    for (uint32_t t0 = 0; t0 < vr.n; t0 = t1, t1 += kCompact) {
+        const uint32_t te = min(vr.n, t1);
         uint32_t c = 0;
-        for (uint32_t t = t0; t < t1; t += 4) {
+        for (uint32_t t = t0; t < te; t += 4) {
             const uint4 g4 = __ldg(reinterpret_cast<const uint4*>(vr.p + (size_t)(t >> 2) * vr.step));
             const uint32_t ge[4] = {g4.x, g4.y, g4.z, g4.w};
 #pragma unroll
             for (uint32_t q = 0; q < 4; ++q)
-                if (t + q < t1 && !(ge[q] & kEntryLower)) s_keep[(c++) * bd + tid] = ge[q];
+                if (t + q < te && !(ge[q] & kEntryLower)) s_keep[(c++) * bd + tid] = ge[q];
         }
         if (c == 0) continue;
         uint32_t e = s_keep[tid];
@@ -342,6 +369,50 @@ __global__ void __launch_bounds__(kMaxPassThreads) k_xsph(uint32_t n, StepConst 
                               vi.z + dvz * kc.xsph_eps, vi.w);
 }
 
+// k_xsph with each pair's W(r) read from the density pass of the same lists
+// and positions (the bits the pair would compute) instead of recomputed from
+// the neighbour's position: per fluid pair one 8-byte read of a stream in
+// place of a 32-byte gather, a square root and the kernel polynomial
+// (XSPH 2.04 -> 1.44 ms at 1M, density 1.16 -> 1.43 ms for the stores).
+__global__ void __launch_bounds__(kMaxPassThreads) k_xsph_w(uint32_t n, StepConst kc, StateBufs s,
+                                                     ListBufs l, double4* __restrict__ vel_out) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double4 vi = s.vel[i];
+    if (s.flags[i] & kFlagBoundary) {
+        vel_out[i] = vi;
+        return;
+    }
+    double dvx = 0.0, dvy = 0.0, dvz = 0.0;
+    const ListRef vr = list_ref(l, i, kListVisit);
+    const double* const wp = l.wpair + (vr.p - l.pool);
+    struct VelW {
+        double4 v;
+        double w;
+    };
+    for_each_loaded2_t(
+        vr,
+        [&](uint32_t t, uint32_t e) {
+            VelW d{};
+            if (!(e & kEntryBoundary)) {
+                d.v = s.vel[e & kEntrySlotMask];
+                d.w = __ldg(wp + (size_t)(t >> 2) * vr.step + (t & 3u));
+            }
+            return d;
+        },
+        [&](uint32_t, uint32_t e, const VelW& d) {
+        if (e & kEntryBoundary) return;
+        const double4 vj = d.v;
+        const double rho_bar = 0.5 * (vi.w + vj.w);
+        const double f = kc.mass / rho_bar * d.w;
+        dvx += (vj.x - vi.x) * f;
+        dvy += (vj.y - vi.y) * f;
+        dvz += (vj.z - vi.z) * f;
+    });
+    vel_out[i] = make_double4(vi.x + dvx * kc.xsph_eps, vi.y + dvy * kc.xsph_eps,
+                              vi.z + dvz * kc.xsph_eps, vi.w);
+}
+
 __global__ void k_in_support(uint32_t n, StepConst kc, StateBufs s, ListBufs l, uint32_t* out) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -360,7 +431,30 @@ __global__ void k_in_support(uint32_t n, StepConst kc, StateBufs s, ListBufs l, 
     out[i] = c;
 }
 
+template <bool I, int D, bool C, bool B>
+void allow_compact_smem() {
+    cudaFuncSetAttribute(k_forces<I, D, C, B>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)(kCompact * kMaxPassThreads * sizeof(uint32_t)));
+}
+
+template <bool I, int D>
+void allow_compact_smem_all() {
+    allow_compact_smem<I, D, true, true>();
+    allow_compact_smem<I, D, true, false>();
+    allow_compact_smem<I, D, false, true>();
+    allow_compact_smem<I, D, false, false>();
+}
+
 }  // namespace
+
+// The force pass's compaction buffer exceeds the 48 KB a launch gets without
+// opting in once a CTA has more than 192 threads.
+void forces_prepare() {
+    allow_compact_smem_all<true, 3>();
+    allow_compact_smem_all<false, 3>();
+    allow_compact_smem_all<true, 2>();
+    allow_compact_smem_all<false, 2>();
+}
 
 void launch_density(uint32_t n, uint32_t threads, const StepConst& k, const StateBufs& s,
                     const ListBufs& l, cudaStream_t st) {
@@ -422,8 +516,12 @@ void launch_boundary_force(uint32_t n, const StepConst& k, const StateBufs& s, c
 }
 
 void launch_xsph(uint32_t n, uint32_t threads, const StepConst& k, const StateBufs& s,
-                 const ListBufs& l, double4* vel_out, cudaStream_t st) {
+                 const ListBufs& l, double4* vel_out, cudaStream_t st, bool use_w) {
     if (!n) return;
+    if (use_w && l.wpair) {
+        k_xsph_w<<<blocks_for(n, threads), threads, 0, st>>>(n, k, s, l, vel_out);
+        return;
+    }
     if (k.kernel == 0) k_xsph<true><<<blocks_for(n, threads), threads, 0, st>>>(n, k, s, l, vel_out);
     else k_xsph<false><<<blocks_for(n, threads), threads, 0, st>>>(n, k, s, l, vel_out);
 }

@@ -124,6 +124,10 @@ struct ListBufs {
     uint32_t* ncand;                  // candidates examined per slot (fluid: union size)
     unsigned long long pool_groups;   // capacity of pool in 16-byte groups (< 2^32)
     uint32_t nslots;
+    // W(r) of each visit entry at the entry's own index into pool (4 *
+    // pool_groups doubles), written by the density pass for the XSPH pass of
+    // the same lists and positions; null when the world keeps none.
+    double* wpair;
 };
 
 // List storage. The list build reserves, for each chunk of consecutive slots
@@ -243,13 +247,16 @@ void launch_density(uint32_t n, uint32_t threads, const StepConst& k, const Stat
 void launch_vmax(uint32_t n, const Tanks& tk, const StateBufs& s, cudaStream_t st);
 void launch_pressure(uint32_t n, const StepConst& k, const Tanks& tk, const StateBufs& s,
                      cudaStream_t st);
+void forces_prepare();  // once per context, before the first launch_forces
 void launch_forces(uint32_t n, uint32_t threads, const StepConst& k, const Tanks& tk,
                    const StateBufs& s, const ListBufs& l, bool integrate, double dt,
                    double4* pos_next, double4* vel_next, const double4* st_a, cudaStream_t st);
 void launch_boundary_force(uint32_t n, const StepConst& k, const StateBufs& s, const ListBufs& l,
                            cudaStream_t st);
+// use_w: l.wpair holds the W of these lists and positions (written by the
+// density pass since the lists were built)
 void launch_xsph(uint32_t n, uint32_t threads, const StepConst& k, const StateBufs& s,
-                 const ListBufs& l, double4* vel_out, cudaStream_t st);
+                 const ListBufs& l, double4* vel_out, cudaStream_t st, bool use_w = false);
 
 // ----- exports / diagnostics -----
 void launch_occupied_export(const GridDesc& g, const uint32_t* occ, const DeviceScalars* sc,

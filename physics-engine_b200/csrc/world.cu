@@ -209,6 +209,7 @@ World::World(const WorldParams& prm, const WorldConfig& cfg, int dim, double res
         g_.dim = dim_;
 
         f32_ = cfg_.precision == 1;
+        pair_w_on_ = cfg_.pair_weights != 0 && !f32_;
         if (f32_ && prm_.surface_tension_sigma != 0.0)
             throw std::invalid_argument("surface tension needs the f64 step");
         if (f32_ && prm_.kernel != 0) throw std::invalid_argument("the single-precision form is cubic-spline only");
@@ -373,8 +374,54 @@ void World::alloc_lists(unsigned long long groups) {
     list_allocs_.push_back(p);
     lists_.pool = static_cast<uint32_t*>(p);
     lists_.pool_groups = groups;
+    lists_.wpair = nullptr;
+    w_valid_ = false;
+    if (pair_w_on_) alloc_pair_weights();
     lists_valid_ = false;
     invalidate_graph();
+}
+
+void World::alloc_pair_weights() {
+    if (lists_.wpair || !lists_.pool_groups) return;
+    // Kept only with room to spare: the buffer is an optimisation, so it
+    // gives way to the list pool (a 512-tank batch's pool alone is ~69 GB).
+    const size_t bytes = (size_t)lists_.pool_groups * 4u * sizeof(double);
+    constexpr size_t kHeadroom = 2ull << 30;
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess || free_b < bytes + kHeadroom) {
+        cudaGetLastError();
+        return;
+    }
+    void* w = nullptr;
+    if (cudaMalloc(&w, bytes) != cudaSuccess) {
+        cudaGetLastError();  // no buffer: XSPH recomputes W
+        return;
+    }
+    list_allocs_.push_back(w);
+    lists_.wpair = static_cast<double*>(w);
+    w_valid_ = false;
+}
+
+void World::free_pair_weights() {
+    if (!lists_.wpair) return;
+    check(cudaStreamSynchronize(st_), "pair weights");
+    for (auto it = list_allocs_.begin(); it != list_allocs_.end(); ++it)
+        if (*it == lists_.wpair) {
+            cudaFree(*it);
+            list_allocs_.erase(it);
+            break;
+        }
+    lists_.wpair = nullptr;
+    w_valid_ = false;
+}
+
+void World::set_pair_weights(bool on) {
+    on = on && !f32_;
+    if (on == pair_w_on_ && (!on || lists_.wpair)) return;
+    pair_w_on_ = on;
+    if (on) alloc_pair_weights();
+    else free_pair_weights();
+    invalidate_graph();  // a captured step bakes in which XSPH kernel runs
 }
 
 World::~World() {
@@ -562,6 +609,7 @@ void World::build_grid(const double4* pos_next, const double4* vel_next) {
     std::swap(cur_, alt_);
     grid_built_ = true;
     lists_valid_ = false;
+    w_valid_ = false;
     check(cudaGetLastError(), "grid build");
 }
 
@@ -569,6 +617,7 @@ void World::ensure_lists(bool visit_only) {
     // the f32 form and the learned step read the visit list only
     const bool build_visit_only = f32_ || visit_only;
     if (lists_valid_ && (lists_full_ || build_visit_only)) return;
+    w_valid_ = false;
     if (!grid_built_) {
         // No grid yet: every neighbour query of the reference returns nothing.
         check(cudaMemsetAsync(lists_.desc, 0, sizeof(uint4) * lists_.nslots, st_), "memset");
@@ -631,6 +680,7 @@ void World::run_density(bool visit_only) {
     prof_end();
     launches_ += 1;
     check(cudaGetLastError(), "density");
+    w_valid_ = !f32_ && lists_.wpair != nullptr;
 }
 
 void World::run_pressure() {
@@ -728,7 +778,7 @@ void World::run_xsph() {
         std::swap(fb_.vel, velf_alt_);
         return;
     }
-    launch_xsph((uint32_t)n_, shape_.xsph, kc_, cur_, lists_, vel_nx_, st_);
+    launch_xsph((uint32_t)n_, shape_.xsph, kc_, cur_, lists_, vel_nx_, st_, w_valid_);
     prof_end();
     launches_ += 1;
     check(cudaGetLastError(), "xsph");
@@ -871,6 +921,8 @@ bool World::capture_graph(double dt) {
 void World::configure_lists() {
     uint32_t per_sm = nlist_prepare(dim_, ucap_, list_chunk_);
     check(cudaGetLastError(), "nlist prepare");
+    forces_prepare();
+    check(cudaGetLastError(), "force pass prepare");
     const uint32_t mult = list_ctas_per_sm_ ? list_ctas_per_sm_ : std::max<uint32_t>(per_sm, 1u) * 4u;
     nl_blocks_ = sms_ * mult;
     invalidate_graph();
@@ -933,13 +985,14 @@ World::Shapes World::autotune() {
         if (f32_) launch_density_f32(n, shape_.density, kf_, cur_, fb_, lists_, st_);
         else launch_density(n, shape_.density, kc_, cur_, lists_, st_);
     });
+    w_valid_ = !f32_ && lists_.wpair != nullptr;  // the density launches wrote W for these lists
     pick(shape_.forces, [&] {
         if (f32_) launch_forces_f32(n, shape_.forces, kf_, tanks_, cur_, fb_, lists_, 0.f, pos_nx_, vel_nx_, nullptr, st_);
         else launch_forces(n, shape_.forces, kc_, tanks_, cur_, lists_, true, 0.0, pos_nx_, vel_nx_,
                            prm_.surface_tension_sigma != 0.0 ? st_a_ : nullptr, st_);
     });
     if (!f32_ && prm_.xsph_epsilon != 0.0)
-        pick(shape_.xsph, [&] { launch_xsph(n, shape_.xsph, kc_, cur_, lists_, vel_nx_, st_); });
+        pick(shape_.xsph, [&] { launch_xsph(n, shape_.xsph, kc_, cur_, lists_, vel_nx_, st_, w_valid_); });
     // list build: tile (centre particles per chunk) x CTAs per SM (multiples
     // of the resident count). The lists' entries and order do not depend on
     // either; a smaller chunk never asks for more of the pool (each chunk

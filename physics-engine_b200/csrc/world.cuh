@@ -35,6 +35,7 @@ struct WorldConfig {
     uint32_t domain_margin_cells;  // minimum extra cells per side (0 = 4)
     int precision;              // 0 = f64 (reference bits), 1 = single-precision form
     int use_graph;              // run() replays captured CUDA graphs of the step
+    int pair_weights;           // keep each visit entry's W for XSPH (World::set_pair_weights)
 };
 
 class CudaError : public std::runtime_error {
@@ -133,6 +134,14 @@ class World {
     };
     Shapes shapes() const;
     Shapes autotune();
+
+    // The density pass keeps each visit entry's W(r) for the XSPH pass of the
+    // same lists and positions, in a buffer of twice the list pool's bytes
+    // that is kept only while the device has room for it (it follows the pool
+    // when that grows). Off, or without the buffer, XSPH recomputes W from the
+    // neighbour's position. The bits are the same either way.
+    void set_pair_weights(bool on);
+    bool pair_weights() const { return lists_.wpair != nullptr; }
 
     // ---- learned surrogate (surrogate.cuh) ----
     // One step with the network's acceleration and density rate in place of
@@ -246,6 +255,10 @@ class World {
     bool grid_current_ = false;  // grid built from the current positions
     bool rho_current_ = false;   // densities computed from the current grid and positions
     bool lists_valid_ = false;   // neighbour lists match the grid and positions
+    bool pair_w_on_ = false;     // keep lists_.wpair (set_pair_weights)
+    bool w_valid_ = false;       // lists_.wpair holds W of the current lists and positions
+    void alloc_pair_weights();
+    void free_pair_weights();
     bool lists_checked_ = false; // list capacity verified for the current positions
     bool lists_sized_ = false;   // the first list sizing has been done
     bool lists_full_ = false;    // the last build wrote upper and lower lists too

@@ -224,6 +224,8 @@ def load_library():
         "pe_fluid_wcsph_diagnostics": (C.c_int, [vp, C.POINTER(_Diag)]),
         "pe_fluid_wcsph_fluid_center_of_mass": (C.c_int, [vp, C.POINTER(C.c_double)]),
         "pe_fluid_wcsph_list_chunk": (C.c_int, [vp, C.POINTER(C.c_uint32)]),
+        "pe_fluid_wcsph_set_pair_weights": (C.c_int, [vp, C.c_int32]),
+        "pe_fluid_wcsph_pair_weights": (C.c_int, [vp, C.POINTER(C.c_int32)]),
         "pe_fluid_wcsph_kernel_launches": (C.c_int, [vp, C.POINTER(u64), i32]),
         "pe_fluid_wcsph_profile": (C.c_int, [vp, i32]),
         "pe_fluid_wcsph_profile_read": (C.c_int, [vp, C.POINTER(_Profile), i32]),
@@ -587,6 +589,18 @@ class WcsphWorld:
         _ok(_lib.pe_fluid_wcsph_list_chunk(self._w, C.byref(c)), "list_chunk")
         r["list_chunk"] = int(c.value)
         return r
+
+    def set_pair_weights(self, on: bool = True):
+        """Let the density pass keep each neighbour entry's W for the XSPH pass
+        (on by default for the f64 step, while the device has room for the
+        buffer); off, XSPH recomputes W. The results are identical."""
+        _ok(_lib.pe_fluid_wcsph_set_pair_weights(self._w, 1 if on else 0), "set_pair_weights")
+
+    def pair_weights(self) -> bool:
+        """Whether the pair-weight buffer is in use."""
+        c = C.c_int32(0)
+        _ok(_lib.pe_fluid_wcsph_pair_weights(self._w, C.byref(c)), "pair_weights")
+        return bool(c.value)
 
     def close(self):
         if getattr(self, "_w", None) and _lib is not None:

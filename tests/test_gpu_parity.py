@@ -88,6 +88,32 @@ def test_steps_bit_exact_small():
     assert w.status() == 0
 
 
+def test_pair_weights_on_and_off_bit_exact():
+    """The density pass keeps each neighbour entry's W for the XSPH pass of
+    the same lists (the default); with the buffer off, XSPH recomputes W from
+    the neighbour's position. Both follow the oracle bit for bit, switched
+    mid-run in both directions (run() replays captured graphs of six steps,
+    which a switch must recapture), and an XSPH pass with no density pass
+    since the grid was rebuilt takes the recomputing kernel."""
+    _, o = _pair(**SMALL)
+    w = pe.WcsphWorld(product_dam_break(SMALL["nx"], SMALL["ny"], SMALL["nz"], box=SMALL["box"], jitter=1e-4),
+                      dam_break_params_pe(False), pe.WcsphConfig(use_graph=True))
+    assert w.pair_weights()
+    dt = 1e-4
+    for on, steps in ((True, 7), (False, 7), (True, 13)):
+        w.set_pair_weights(on)
+        assert w.pair_weights() == on
+        w.run(dt, steps)
+        o.run(dt, steps)
+        _compare_state(w, o, f"pair weights {on}")
+    w.rebuild_grid()
+    o.rebuild_grid()
+    w.apply_xsph()
+    o.apply_xsph()
+    assert_bits_equal(w.velocities(), o.v(), "xsph after a grid rebuild")
+    assert w.status() == 0
+
+
 def test_adaptive_sound_speed_bit_exact():
     """compute_pressure's c = max(c, 10 v_max), persisted (wcsph.rs:158-169).
     With the rule on, the free-surface start accelerates quickly (c grows each
