@@ -57,8 +57,10 @@ __global__ void __launch_bounds__(kMaxPassThreads) k_density(uint32_t n, StepCon
     double rho = k.rho_self;  // 0.0 + mass * W(0)
     const ListRef vr = list_ref(l, i, kListVisit);
     // W of entry t kept at the entry's pool index for the XSPH pass, two
-    // entries per 16-byte store (a whole sector over a group's four entries)
-    double* const wp = l.wpair ? l.wpair + (vr.p - l.pool) : nullptr;
+    // entries per 16-byte store (a whole sector over a group's four entries);
+    // wrow walks the slot's rows of 16-byte groups
+    const bool keep_w = l.wpair != nullptr;
+    double* wrow = keep_w ? l.wpair + (vr.p - l.pool) : nullptr;
     double wprev = 0.0;
     for_each_loaded2_t(
         vr, [&](uint32_t, uint32_t e) { return s.pos[e & kEntrySlotMask]; },
@@ -67,9 +69,10 @@ __global__ void __launch_bounds__(kMaxPassThreads) k_density(uint32_t n, StepCon
         const double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
         const double r = sqrt(dx * dx + dy * dy + dz * dz);
         const double wij = kw<CUBIC>(r, k);
-        if (wp) {
+        if (keep_w) {
             if (t & 1u) {
-                *reinterpret_cast<double2*>(wp + (size_t)(t >> 2) * vr.step + (t & 2u)) = make_double2(wprev, wij);
+                *reinterpret_cast<double2*>(wrow + (t & 2u)) = make_double2(wprev, wij);
+                if (t & 2u) wrow += vr.step;
             } else {
                 wprev = wij;
             }
@@ -79,10 +82,8 @@ __global__ void __launch_bounds__(kMaxPassThreads) k_density(uint32_t n, StepCon
         const double f = (e & kEntryBoundary) ? k.rho0 * xj.w : k.mass;
         rho += f * wij;
     });
-    if (wp && (vr.n & 1u)) {  // the last entry's W, unpaired
-        const uint32_t t = vr.n - 1u;
-        *reinterpret_cast<double2*>(wp + (size_t)(t >> 2) * vr.step + (t & 2u)) = make_double2(wprev, 0.0);
-    }
+    if (keep_w && (vr.n & 1u))  // the last entry's W, unpaired
+        *reinterpret_cast<double2*>(wrow + ((vr.n - 1u) & 2u)) = make_double2(wprev, 0.0);
     rho = fmax(rho, 1e-12);  // wcsph.rs:152 (f64::max)
     s.vel[i].w = rho;
     // keep the cached p / rho^2 consistent with the new rho (the reference
@@ -385,19 +386,20 @@ __global__ void __launch_bounds__(kMaxPassThreads) k_xsph_w(uint32_t n, StepCons
     }
     double dvx = 0.0, dvy = 0.0, dvz = 0.0;
     const ListRef vr = list_ref(l, i, kListVisit);
-    const double* const wp = l.wpair + (vr.p - l.pool);
+    const double* wrow = l.wpair + (vr.p - l.pool);  // walks the rows as the loads advance
     struct VelW {
         double4 v;
         double w;
     };
     for_each_loaded2_t(
         vr,
-        [&](uint32_t t, uint32_t e) {
+        [&](uint32_t t, uint32_t e) {  // called for t = 0, 1, 2, ... in order
             VelW d{};
             if (!(e & kEntryBoundary)) {
                 d.v = s.vel[e & kEntrySlotMask];
-                d.w = __ldg(wp + (size_t)(t >> 2) * vr.step + (t & 3u));
+                d.w = __ldg(wrow + (t & 3u));
             }
+            if ((t & 3u) == 3u) wrow += vr.step;
             return d;
         },
         [&](uint32_t, uint32_t e, const VelW& d) {
