@@ -348,11 +348,13 @@ int pe_fluid_wcsph_shapes(PeWcsph* w, uint32_t out[4]);
 /* The list build's tile in use: centre particles per chunk (32 or 64). */
 int pe_fluid_wcsph_list_chunk(PeWcsph* w, uint32_t* out);
 /* Pair weights: the density pass keeps each neighbour entry's W(r) for the
- * XSPH pass of the same lists and positions (on by default for the f64 step;
- * a device buffer of twice the neighbour-list pool, allocated only while the
- * device has room for it and 2 GB besides). on = 0 frees it and XSPH
- * recomputes W. Results are identical either way. pe_fluid_wcsph_pair_weights
- * reports whether the buffer is in use (1) or not (0). */
+ * XSPH pass of the same lists and positions (on by default; a device buffer
+ * of twice the neighbour-list pool's bytes, the pool's bytes in the
+ * single-precision form, allocated only while the device has room for it and
+ * 2 GB besides). on = 0 frees it and XSPH recomputes W. The f64 step's
+ * results are identical either way (the single-precision form's may differ
+ * in the last bits). pe_fluid_wcsph_pair_weights reports whether the buffer
+ * is in use (1) or not (0). */
 int pe_fluid_wcsph_set_pair_weights(PeWcsph* w, int32_t on);
 int pe_fluid_wcsph_pair_weights(PeWcsph* w, int32_t* out);
 

@@ -22,26 +22,35 @@ __device__ __forceinline__ void for_each_entry(const ListRef r, F&& f) {
     }
 }
 
-// Calls f(entry, data) over a slot's list in order, where data = load(entry)
-// is issued one entry ahead: the gather of the next neighbour's state is in
-// flight while the current pair is computed.
+// Calls f(t, entry, data) over a slot's list in order (t the entry's
+// position), where data = load(t, entry) is issued one entry ahead: the
+// gather of the next neighbour's state is in flight while the current pair
+// is computed. load sees t = 0, 1, 2, ... in order.
 template <class Load, class F>
-__device__ __forceinline__ void for_each_loaded(const ListRef r, Load&& load, F&& f) {
+__device__ __forceinline__ void for_each_loaded_t(const ListRef r, Load&& load, F&& f) {
     const uint32_t n = r.n;
     if (n == 0) return;
     auto at = [&](uint32_t t) { return __ldg(r.p + (size_t)(t >> 2) * r.step + (t & 3u)); };
     uint32_t e0 = at(0), e1 = n > 1 ? at(1) : 0u;
-    auto d0 = load(e0);
+    auto d0 = load(0u, e0);
     for (uint32_t t = 0; t < n; ++t) {
         const uint32_t e = e0;
         const auto d = d0;
         if (t + 1 < n) {
             e0 = e1;
-            d0 = load(e1);
+            d0 = load(t + 1, e1);
             if (t + 2 < n) e1 = at(t + 2);
         }
-        f(e, d);
+        f(t, e, d);
     }
+}
+
+// for_each_loaded_t without the positions.
+template <class Load, class F>
+__device__ __forceinline__ void for_each_loaded(const ListRef r, Load&& load, F&& f) {
+    for_each_loaded_t(
+        r, [&](uint32_t, uint32_t e) { return load(e); },
+        [&](uint32_t, uint32_t e, const auto& d) { f(e, d); });
 }
 
 // Calls f(t, entry, data) over a slot's list in order (t the entry's

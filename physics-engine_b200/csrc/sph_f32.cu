@@ -90,22 +90,39 @@ __global__ void __launch_bounds__(kMaxPassThreads) k_density_f32(uint32_t n, F32
     const int4 ki = s.key[i];
     Kahan rho;
     rho.add(k.rho_self);
-    for_each_loaded(
-        list_ref(l, i, kListVisit),
-        [&](uint32_t e) {
+    const ListRef vr = list_ref(l, i, kListVisit);
+    // W of each entry kept for the XSPH pass, one 16-byte store per group of
+    // four entries at the group's pool index (wrow walks the slot's rows)
+    const bool keep_w = l.wpair32 != nullptr;
+    float* wrow = keep_w ? l.wpair32 + (vr.p - l.pool) : nullptr;
+    float w0 = 0.f, w1 = 0.f, w2 = 0.f;
+    for_each_loaded_t(
+        vr,
+        [&](uint32_t, uint32_t e) {
             Nb32 b;
             b.p = f.pos[e & kEntrySlotMask];
             b.key = s.key[e & kEntrySlotMask];
             return b;
         },
-        [&](uint32_t e, const Nb32& b) {
+        [&](uint32_t t, uint32_t e, const Nb32& b) {
             const float4 pj = b.p;
             const float3 d = rel(ki, pi, b.key, pj, k.cell);
-            if ((e & kEntryOriented) && !sees_fluid_f32(k, s.nout[e & kEntrySlotMask], d)) return;
             const float r = sqrtf(d.x * d.x + d.y * d.y + d.z * d.z);
             const float w = w_f32(r, k);
+            if (keep_w) {
+                switch (t & 3u) {
+                    case 0: w0 = w; break;
+                    case 1: w1 = w; break;
+                    case 2: w2 = w; break;
+                    default:
+                        *reinterpret_cast<float4*>(wrow) = make_float4(w0, w1, w2, w);
+                        wrow += vr.step;
+                }
+            }
+            if ((e & kEntryOriented) && !sees_fluid_f32(k, s.nout[e & kEntrySlotMask], d)) return;
             rho.add(((e & kEntryBoundary) ? k.rho0 * pj.w : k.mass) * w);
         });
+    if (keep_w && (vr.n & 3u)) *reinterpret_cast<float4*>(wrow) = make_float4(w0, w1, w2, 0.f);
     const float r = fmaxf(rho.s, 1e-12f);
     f.vel[i].w = r;
     s.vel[i].w = (double)r;
@@ -280,6 +297,48 @@ __global__ void __launch_bounds__(kMaxPassThreads) k_xsph_f32(uint32_t n, F32Con
     s.vel[i] = make_double4(vn.x, vn.y, vn.z, vn.w);
 }
 
+// k_xsph_f32 with each pair's W read from the density pass of the same lists
+// and positions instead of recomputed: the neighbour's velocity is the only
+// gather (16 bytes in place of 48).
+__global__ void __launch_bounds__(kMaxPassThreads) k_xsph_f32_w(uint32_t n, F32Const k, StateBufs s, F32Bufs f,
+                                                         ListBufs l, float4* __restrict__ vel_out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 vi = f.vel[i];
+    if (s.flags[i] & kFlagBoundary) {
+        vel_out[i] = vi;
+        return;
+    }
+    Kahan dx, dy, dz;
+    const ListRef vr = list_ref(l, i, kListVisit);
+    const float* wrow = l.wpair32 + (vr.p - l.pool);
+    struct VelW {
+        float4 v;
+        float w;
+    };
+    auto load = [&](uint32_t t, uint32_t e) {  // t = 0, 1, 2, ... in order
+        VelW b{};
+        if (!(e & kEntryBoundary)) {
+            b.v = f.vel[e & kEntrySlotMask];
+            b.w = __ldg(wrow + (t & 3u));
+        }
+        if ((t & 3u) == 3u) wrow += vr.step;
+        return b;
+    };
+    for_each_loaded_t(vr, load, [&](uint32_t, uint32_t e, const VelW& b) {
+        if (e & kEntryBoundary) return;
+        const float4 vj = b.v;
+        const float g = k.mass * 2.f / (vi.w + vj.w) * b.w;
+        dx.add((vj.x - vi.x) * g);
+        dy.add((vj.y - vi.y) * g);
+        dz.add((vj.z - vi.z) * g);
+    });
+    const float4 vn = make_float4(vi.x + dx.s * k.xsph_eps, vi.y + dy.s * k.xsph_eps,
+                                  vi.z + dz.s * k.xsph_eps, vi.w);
+    vel_out[i] = vn;
+    s.vel[i] = make_double4(vn.x, vn.y, vn.z, vn.w);
+}
+
 // Cell-local single-precision state from the (sorted) f64 state.
 __global__ void k_f32_from_f64(uint32_t n, double cell, StateBufs s, F32Bufs f) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -332,8 +391,11 @@ void launch_forces_f32(uint32_t n, uint32_t threads, const F32Const& k, const Ta
 }
 
 void launch_xsph_f32(uint32_t n, uint32_t threads, const F32Const& k, const StateBufs& s,
-                     const F32Bufs& f, const ListBufs& l, float4* vel_out, cudaStream_t st) {
-    if (n) k_xsph_f32<<<blocks_for(n, threads), threads, 0, st>>>(n, k, s, f, l, vel_out);
+                     const F32Bufs& f, const ListBufs& l, float4* vel_out, cudaStream_t st,
+                     bool use_w) {
+    if (!n) return;
+    if (use_w && l.wpair32) k_xsph_f32_w<<<blocks_for(n, threads), threads, 0, st>>>(n, k, s, f, l, vel_out);
+    else k_xsph_f32<<<blocks_for(n, threads), threads, 0, st>>>(n, k, s, f, l, vel_out);
 }
 
 }  // namespace pe

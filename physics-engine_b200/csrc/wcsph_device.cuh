@@ -125,9 +125,11 @@ struct ListBufs {
     unsigned long long pool_groups;   // capacity of pool in 16-byte groups (< 2^32)
     uint32_t nslots;
     // W(r) of each visit entry at the entry's own index into pool (4 *
-    // pool_groups doubles), written by the density pass for the XSPH pass of
-    // the same lists and positions; null when the world keeps none.
+    // pool_groups values), written by the density pass for the XSPH pass of
+    // the same lists and positions; null when the world keeps none. f64 for
+    // the f64 step, f32 for the single-precision form.
     double* wpair;
+    float* wpair32;
 };
 
 // List storage. The list build reserves, for each chunk of consecutive slots
@@ -209,7 +211,8 @@ void launch_forces_f32(uint32_t n, uint32_t threads, const F32Const& k, const Ta
                        const StateBufs& s, const F32Bufs& f, const ListBufs& l, float dt,
                        double4* pos_next, double4* vel_next, float* bf, cudaStream_t st);
 void launch_xsph_f32(uint32_t n, uint32_t threads, const F32Const& k, const StateBufs& s,
-                     const F32Bufs& f, const ListBufs& l, float4* vel_out, cudaStream_t st);
+                     const F32Bufs& f, const ListBufs& l, float4* vel_out, cudaStream_t st,
+                     bool use_w = false);
 
 // ----- grid build -----
 void launch_cell_ids(const GridDesc& g, const Tanks& tk, uint32_t n, const double4* pos_cur,

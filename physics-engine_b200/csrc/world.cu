@@ -209,7 +209,7 @@ World::World(const WorldParams& prm, const WorldConfig& cfg, int dim, double res
         g_.dim = dim_;
 
         f32_ = cfg_.precision == 1;
-        pair_w_on_ = cfg_.pair_weights != 0 && !f32_;
+        pair_w_on_ = cfg_.pair_weights != 0;
         if (f32_ && prm_.surface_tension_sigma != 0.0)
             throw std::invalid_argument("surface tension needs the f64 step");
         if (f32_ && prm_.kernel != 0) throw std::invalid_argument("the single-precision form is cubic-spline only");
@@ -375,6 +375,7 @@ void World::alloc_lists(unsigned long long groups) {
     lists_.pool = static_cast<uint32_t*>(p);
     lists_.pool_groups = groups;
     lists_.wpair = nullptr;
+    lists_.wpair32 = nullptr;
     w_valid_ = false;
     if (pair_w_on_) alloc_pair_weights();
     lists_valid_ = false;
@@ -382,10 +383,10 @@ void World::alloc_lists(unsigned long long groups) {
 }
 
 void World::alloc_pair_weights() {
-    if (lists_.wpair || !lists_.pool_groups) return;
+    if (pair_weights() || !lists_.pool_groups) return;
     // Kept only with room to spare: the buffer is an optimisation, so it
     // gives way to the list pool (a 512-tank batch's pool alone is ~69 GB).
-    const size_t bytes = (size_t)lists_.pool_groups * 4u * sizeof(double);
+    const size_t bytes = (size_t)lists_.pool_groups * 4u * (f32_ ? sizeof(float) : sizeof(double));
     constexpr size_t kHeadroom = 2ull << 30;
     size_t free_b = 0, total_b = 0;
     if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess || free_b < bytes + kHeadroom) {
@@ -398,26 +399,28 @@ void World::alloc_pair_weights() {
         return;
     }
     list_allocs_.push_back(w);
-    lists_.wpair = static_cast<double*>(w);
+    if (f32_) lists_.wpair32 = static_cast<float*>(w);
+    else lists_.wpair = static_cast<double*>(w);
     w_valid_ = false;
 }
 
 void World::free_pair_weights() {
-    if (!lists_.wpair) return;
+    void* const w = lists_.wpair ? (void*)lists_.wpair : (void*)lists_.wpair32;
+    if (!w) return;
     check(cudaStreamSynchronize(st_), "pair weights");
     for (auto it = list_allocs_.begin(); it != list_allocs_.end(); ++it)
-        if (*it == lists_.wpair) {
+        if (*it == w) {
             cudaFree(*it);
             list_allocs_.erase(it);
             break;
         }
     lists_.wpair = nullptr;
+    lists_.wpair32 = nullptr;
     w_valid_ = false;
 }
 
 void World::set_pair_weights(bool on) {
-    on = on && !f32_;
-    if (on == pair_w_on_ && (!on || lists_.wpair)) return;
+    if (on == pair_w_on_ && (!on || pair_weights())) return;
     pair_w_on_ = on;
     if (on) alloc_pair_weights();
     else free_pair_weights();
@@ -680,7 +683,7 @@ void World::run_density(bool visit_only) {
     prof_end();
     launches_ += 1;
     check(cudaGetLastError(), "density");
-    w_valid_ = !f32_ && lists_.wpair != nullptr;
+    w_valid_ = pair_weights();
 }
 
 void World::run_pressure() {
@@ -771,7 +774,7 @@ void World::run_xsph() {
     ensure_lists();
     prof_begin(kXsph);
     if (f32_) {
-        launch_xsph_f32((uint32_t)n_, shape_.xsph, kf_, cur_, fb_, lists_, velf_alt_, st_);
+        launch_xsph_f32((uint32_t)n_, shape_.xsph, kf_, cur_, fb_, lists_, velf_alt_, st_, w_valid_);
         prof_end();
         launches_ += 1;
         check(cudaGetLastError(), "xsph");
@@ -985,7 +988,7 @@ World::Shapes World::autotune() {
         if (f32_) launch_density_f32(n, shape_.density, kf_, cur_, fb_, lists_, st_);
         else launch_density(n, shape_.density, kc_, cur_, lists_, st_);
     });
-    w_valid_ = !f32_ && lists_.wpair != nullptr;  // the density launches wrote W for these lists
+    w_valid_ = pair_weights();  // the density launches wrote W for these lists
     pick(shape_.forces, [&] {
         if (f32_) launch_forces_f32(n, shape_.forces, kf_, tanks_, cur_, fb_, lists_, 0.f, pos_nx_, vel_nx_, nullptr, st_);
         else launch_forces(n, shape_.forces, kc_, tanks_, cur_, lists_, true, 0.0, pos_nx_, vel_nx_,

@@ -137,11 +137,12 @@ class World {
 
     // The density pass keeps each visit entry's W(r) for the XSPH pass of the
     // same lists and positions, in a buffer of twice the list pool's bytes
-    // that is kept only while the device has room for it (it follows the pool
-    // when that grows). Off, or without the buffer, XSPH recomputes W from the
-    // neighbour's position. The bits are the same either way.
+    // (the pool's bytes in the single-precision form) that is kept only while
+    // the device has room for it (it follows the pool when that grows). Off,
+    // or without the buffer, XSPH recomputes W from the neighbour's position.
+    // In the f64 step the bits are the same either way.
     void set_pair_weights(bool on);
-    bool pair_weights() const { return lists_.wpair != nullptr; }
+    bool pair_weights() const { return lists_.wpair != nullptr || lists_.wpair32 != nullptr; }
 
     // ---- learned surrogate (surrogate.cuh) ----
     // One step with the network's acceleration and density rate in place of

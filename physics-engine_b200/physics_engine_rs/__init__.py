@@ -592,8 +592,8 @@ class WcsphWorld:
 
     def set_pair_weights(self, on: bool = True):
         """Let the density pass keep each neighbour entry's W for the XSPH pass
-        (on by default for the f64 step, while the device has room for the
-        buffer); off, XSPH recomputes W. The results are identical."""
+        (on by default, while the device has room for the buffer); off, XSPH
+        recomputes W. The f64 step's results are identical either way."""
         _ok(_lib.pe_fluid_wcsph_set_pair_weights(self._w, 1 if on else 0), "set_pair_weights")
 
     def pair_weights(self) -> bool:
