@@ -52,9 +52,9 @@ FORCE_OPS_PER_PAIR = 65.0
 # DRAM bytes (read + write) of one force-pass launch per fluid particle, from
 # the ncu capture of the 262,144-particle dam break (the neighbour lists
 # dominate; traffic grows with the particle count).
-FORCE_TRAFFIC_PER_FLUID = (428.454400e6 + 20.749056e6) / 262144
+FORCE_TRAFFIC_PER_FLUID = (429.341184e6 + 22.202624e6) / 262144
 # sm__pipe_fp64_cycles_active of the force pass in the same capture
-FORCE_FP64_PIPE_ACTIVE = 0.512
+FORCE_FP64_PIPE_ACTIVE = 0.507
 # smsp__issue_active of the list build (k_nlist_both) in the same capture
 LISTS_ISSUE_ACTIVE = 0.592
 # Whole step, per fluid / per boundary particle (cell key 28 + sort 8 +
