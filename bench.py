@@ -389,6 +389,7 @@ def f32_leg(workload, local, torch, pe, timed_steps, warm, total_steps):
         "timed_steps": timed_steps, "warmup": warm, "dtype": "f32 pair arithmetic (Kahan sums), f64 grid/CFL/reductions",
         "f64_ms_per_step": ms64 / timed_steps, "speedup_vs_f64_step": ms64 / ms32,
         "gpu_launches": int(launches), "status": int(status),
+        "pair_weights": {"f32": w32.pair_weights(), "f64": w64.pair_weights()},
         "phases_ms_per_step": {k: v[0] / max(1, timed_steps) for k, v in prof32.items()},
         "error_vs_f64": {
             "after_steps": max(total_steps, warm + timed_steps),
@@ -507,7 +508,8 @@ def run_batched(args, ws, rank, local, torch, pe):
                       "phase_boundary_cost": phase_overhead(pe, local)},
         "gpu_launches": int(launches), "status": int(status),
         "neighbour_lists": {"used_gb": cap["list_groups_used"] * 16 / 1e9,
-                            "pool_gb": cap["list_groups_capacity"] * 16 / 1e9},
+                            "pool_gb": cap["list_groups_capacity"] * 16 / 1e9,
+                            "pair_weights": w.pair_weights()},
         "per_tank_loop": {"value": loop_value, "unit": UNIT, "tanks_timed": len(sample),
                           "fluid_particles_timed": loop_nf,
                           "how": "single-tank worlds stepped one after another, same steps"},
@@ -891,7 +893,8 @@ def main():
         "phases_ms_per_step": {k: v[0] / max(1, args.steps) for k, v in prof.items()},
         "neighbour_lists": {"used_gb": cap["list_groups_used"] * 16 / 1e9,
                             "pool_gb": cap["list_groups_capacity"] * 16 / 1e9,
-                            "union_stage": cap["union_capacity"], "max_union": cap["max_union"]},
+                            "union_stage": cap["union_capacity"], "max_union": cap["max_union"],
+                            "pair_weights": world.pair_weights()},
         "roofline": {"bound": "hbm", "kernel": "k_forces (force + kick + drift)",
                      "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                      "frac": achieved / hbm_peak, "peak_kind": peak_kind,
