@@ -92,3 +92,26 @@ def test_f32_is_deterministic():
     assert np.array_equal(a.velocities(), b.velocities())
     a.close()
     b.close()
+
+
+@pytest.mark.parametrize("weights", [True, False])
+def test_f32_with_and_without_pair_weights_track_f64(weights):
+    """The density pass keeps each neighbour's W for XSPH (the default) or
+    XSPH recomputes it: both stay within the f32 form's bounds, and the two
+    differ by no more than rounding (well inside the same bounds)."""
+    w64, w32, fluid = _worlds()
+    w32.set_pair_weights(weights)
+    assert w32.pair_weights() == weights
+    ref = pe.WcsphWorld(product_dam_break(20, 12, 12, box=(0.5, 0.2, 0.3)), dam_break_params_pe(),
+                        pe.WcsphConfig(precision=pe.PRECISION_F32))
+    ref.set_pair_weights(not weights)
+    for w in (w64, w32, ref):
+        w.run(DT, STEPS)
+    r64 = w64.densities()[fluid]
+    for w in (w32, ref):
+        rel = np.abs(w.densities()[fluid] - r64) / r64
+        assert rel.max() < DENSITY_REL_MAX, rel.max()
+        assert np.abs(w.positions() - w64.positions()).max() < POSITION_ABS_MAX
+    assert np.abs(w32.velocities() - ref.velocities()).max() < 1e-6
+    for w in (w64, w32, ref):
+        w.close()
