@@ -357,6 +357,13 @@ int pe_fluid_wcsph_list_chunk(PeWcsph* w, uint32_t* out);
  * is in use (1) or not (0). */
 int pe_fluid_wcsph_set_pair_weights(PeWcsph* w, int32_t on);
 int pe_fluid_wcsph_pair_weights(PeWcsph* w, int32_t* out);
+/* The buffer covers the pool's first 5/8 (1.25x the lists of a freshly sized
+ * pool). A density pass that meets a list reaching past it keeps no weights
+ * for that step and XSPH recomputes W; the next pe_fluid_wcsph_status (run
+ * polls it every 16 steps) extends the buffer to the whole pool.
+ * out = {in use (0/1), list entries covered, the last density pass met a
+ * list beyond them (0/1)}. Synchronous. */
+int pe_fluid_wcsph_pair_weight_info(PeWcsph* w, uint64_t out[3]);
 
 /* WcsphWorld::step (wcsph.rs:326). Synchronous; returns PE_ERR_BOUNDS if the
  * step raised PE_STATUS_DOMAIN or PE_STATUS_NEIGHBOUR_OVERFLOW. */

@@ -590,6 +590,14 @@ int pe_fluid_wcsph_pair_weights(PeWcsph* w, int32_t* out) {
     return PE_OK;
 }
 
+int pe_fluid_wcsph_pair_weight_info(PeWcsph* w, uint64_t out[3]) {
+    if (!w || !out) return PE_ERR_NULL;
+    return guard([&] {
+        w->world->pair_weight_info(out);
+        return PE_OK;
+    });
+}
+
 int pe_fluid_wcsph_get_params(PeWcsph* w, PeWcsphParams* out) {
     if (!w || !out) return PE_ERR_NULL;
     return guard([&] {

@@ -63,7 +63,11 @@ __global__ void __launch_bounds__(kMaxPassThreads) k_density(uint32_t n, StepCon
     // W of entry t kept at the entry's pool index for the XSPH pass, two
     // entries per 16-byte store (a whole sector over a group's four entries);
     // wrow walks the slot's rows of 16-byte groups
-    const bool keep_w = l.wpair != nullptr;
+    bool keep_w = false;
+    if (l.wpair) {
+        keep_w = w_fits(l, vr);
+        if (!keep_w) atomicOr(l.w_short, 1u);
+    }
     double* wrow = keep_w ? l.wpair + (vr.p - l.pool) : nullptr;
     double wprev = 0.0;
     for_each_loaded2_t(
@@ -335,16 +339,11 @@ __global__ void __launch_bounds__(kThreads) k_boundary_force(uint32_t n, StepCon
     s.bf[b] = make_double4(fx, fy, fz, 0.0);
 }
 
+// The XSPH sum of fluid slot i with velocity vi, each pair's W recomputed
+// from the neighbour's position.
 template <bool CUBIC>
-__global__ void __launch_bounds__(kMaxPassThreads) k_xsph(uint32_t n, StepConst kc, StateBufs s,
-                                                   ListBufs l, double4* __restrict__ vel_out) {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const double4 vi = s.vel[i];
-    if (s.flags[i] & kFlagBoundary) {
-        vel_out[i] = vi;
-        return;
-    }
+__device__ __forceinline__ double3 xsph_dv(uint32_t i, const StepConst& kc, const StateBufs& s,
+                                           const ListBufs& l, double4 vi) {
     const double4 xi = s.pos[i];
     double dvx = 0.0, dvy = 0.0, dvz = 0.0;
     for_each_loaded2(
@@ -370,8 +369,26 @@ __global__ void __launch_bounds__(kMaxPassThreads) k_xsph(uint32_t n, StepConst 
         dvy += (vj.y - vi.y) * f;
         dvz += (vj.z - vi.z) * f;
     });
-    vel_out[i] = make_double4(vi.x + dvx * kc.xsph_eps, vi.y + dvy * kc.xsph_eps,
-                              vi.z + dvz * kc.xsph_eps, vi.w);
+    return make_double3(dvx, dvy, dvz);
+}
+
+// short_only: run only if the density pass met a list beyond the pair-weight
+// buffer (the launch that follows k_xsph_w, which then did nothing).
+template <bool CUBIC>
+__global__ void __launch_bounds__(kMaxPassThreads) k_xsph(uint32_t n, StepConst kc, StateBufs s,
+                                                   ListBufs l, double4* __restrict__ vel_out,
+                                                   bool short_only) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (short_only && !__ldg(l.w_short)) return;
+    const double4 vi = s.vel[i];
+    if (s.flags[i] & kFlagBoundary) {
+        vel_out[i] = vi;
+        return;
+    }
+    const double3 dv = xsph_dv<CUBIC>(i, kc, s, l, vi);
+    vel_out[i] = make_double4(vi.x + dv.x * kc.xsph_eps, vi.y + dv.y * kc.xsph_eps,
+                              vi.z + dv.z * kc.xsph_eps, vi.w);
 }
 
 // k_xsph with each pair's W(r) read from the density pass of the same lists
@@ -379,10 +396,14 @@ __global__ void __launch_bounds__(kMaxPassThreads) k_xsph(uint32_t n, StepConst 
 // the neighbour's position: per fluid pair one 8-byte read of a stream in
 // place of a 32-byte gather, a square root and the kernel polynomial
 // (XSPH 2.04 -> 1.44 ms at 1M, density 1.16 -> 1.43 ms for the stores).
+// When the density pass met a list beyond the buffer, it does nothing and
+// the k_xsph launch after it recomputes W for every particle (a separate
+// kernel, so that this one keeps its own, smaller register count).
 __global__ void __launch_bounds__(kMaxPassThreads) k_xsph_w(uint32_t n, StepConst kc, StateBufs s,
                                                      ListBufs l, double4* __restrict__ vel_out) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    if (__ldg(l.w_short)) return;
     const double4 vi = s.vel[i];
     if (s.flags[i] & kFlagBoundary) {
         vel_out[i] = vi;
@@ -532,12 +553,10 @@ void launch_boundary_force(uint32_t n, const StepConst& k, const StateBufs& s, c
 void launch_xsph(uint32_t n, uint32_t threads, const StepConst& k, const StateBufs& s,
                  const ListBufs& l, double4* vel_out, cudaStream_t st, bool use_w) {
     if (!n) return;
-    if (use_w && l.wpair) {
-        k_xsph_w<<<blocks_for(n, threads), threads, 0, st>>>(n, k, s, l, vel_out);
-        return;
-    }
-    if (k.kernel == 0) k_xsph<true><<<blocks_for(n, threads), threads, 0, st>>>(n, k, s, l, vel_out);
-    else k_xsph<false><<<blocks_for(n, threads), threads, 0, st>>>(n, k, s, l, vel_out);
+    const bool w = use_w && l.wpair;
+    if (w) k_xsph_w<<<blocks_for(n, threads), threads, 0, st>>>(n, k, s, l, vel_out);
+    if (k.kernel == 0) k_xsph<true><<<blocks_for(n, threads), threads, 0, st>>>(n, k, s, l, vel_out, w);
+    else k_xsph<false><<<blocks_for(n, threads), threads, 0, st>>>(n, k, s, l, vel_out, w);
 }
 
 void launch_in_support_counts(uint32_t n, const StepConst& k, const StateBufs& s,

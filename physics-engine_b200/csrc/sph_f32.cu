@@ -93,7 +93,11 @@ __global__ void __launch_bounds__(kMaxPassThreads) k_density_f32(uint32_t n, F32
     const ListRef vr = list_ref(l, i, kListVisit);
     // W of each entry kept for the XSPH pass, one 16-byte store per group of
     // four entries at the group's pool index (wrow walks the slot's rows)
-    const bool keep_w = l.wpair32 != nullptr;
+    bool keep_w = false;
+    if (l.wpair32) {
+        keep_w = w_fits(l, vr);
+        if (!keep_w) atomicOr(l.w_short, 1u);
+    }
     float* wrow = keep_w ? l.wpair32 + (vr.p - l.pool) : nullptr;
     float w0 = 0.f, w1 = 0.f, w2 = 0.f;
     for_each_loaded_t(
@@ -258,10 +262,14 @@ __global__ void __launch_bounds__(kMaxPassThreads) k_forces_f32(uint32_t n, F32C
     vel_next[i] = make_double4(vx, vy, vz, vi.w);
 }
 
+// short_only: run only if the density pass met a list beyond the pair-weight
+// buffer (the launch that follows k_xsph_f32_w, which then did nothing).
 __global__ void __launch_bounds__(kMaxPassThreads) k_xsph_f32(uint32_t n, F32Const k, StateBufs s, F32Bufs f,
-                                                       ListBufs l, float4* __restrict__ vel_out) {
+                                                       ListBufs l, float4* __restrict__ vel_out,
+                                                       bool short_only) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    if (short_only && !__ldg(l.w_short)) return;
     const float4 vi = f.vel[i];
     if (s.flags[i] & kFlagBoundary) {
         vel_out[i] = vi;
@@ -304,6 +312,7 @@ __global__ void __launch_bounds__(kMaxPassThreads) k_xsph_f32_w(uint32_t n, F32C
                                                          ListBufs l, float4* __restrict__ vel_out) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    if (__ldg(l.w_short)) return;  // k_xsph_f32 runs instead
     const float4 vi = f.vel[i];
     if (s.flags[i] & kFlagBoundary) {
         vel_out[i] = vi;
@@ -394,8 +403,9 @@ void launch_xsph_f32(uint32_t n, uint32_t threads, const F32Const& k, const Stat
                      const F32Bufs& f, const ListBufs& l, float4* vel_out, cudaStream_t st,
                      bool use_w) {
     if (!n) return;
-    if (use_w && l.wpair32) k_xsph_f32_w<<<blocks_for(n, threads), threads, 0, st>>>(n, k, s, f, l, vel_out);
-    else k_xsph_f32<<<blocks_for(n, threads), threads, 0, st>>>(n, k, s, f, l, vel_out);
+    const bool w = use_w && l.wpair32;
+    if (w) k_xsph_f32_w<<<blocks_for(n, threads), threads, 0, st>>>(n, k, s, f, l, vel_out);
+    k_xsph_f32<<<blocks_for(n, threads), threads, 0, st>>>(n, k, s, f, l, vel_out, w);
 }
 
 }  // namespace pe

@@ -124,12 +124,17 @@ struct ListBufs {
     uint32_t* ncand;                  // candidates examined per slot (fluid: union size)
     unsigned long long pool_groups;   // capacity of pool in 16-byte groups (< 2^32)
     uint32_t nslots;
-    // W(r) of each visit entry at the entry's own index into pool (4 *
-    // pool_groups values), written by the density pass for the XSPH pass of
-    // the same lists and positions; null when the world keeps none. f64 for
-    // the f64 step, f32 for the single-precision form.
+    // W(r) of each visit entry at the entry's own index into pool, written by
+    // the density pass for the XSPH pass of the same lists and positions;
+    // null when the world keeps none. f64 for the f64 step, f32 for the
+    // single-precision form. The buffer holds the first w_cap entries of the
+    // pool (the list build fills the pool from its start); a density pass
+    // that meets a list reaching beyond sets *w_short, and the XSPH pass
+    // after it then recomputes W for every particle.
     double* wpair;
     float* wpair32;
+    unsigned long long w_cap;
+    uint32_t* w_short;
 };
 
 // List storage. The list build reserves, for each chunk of consecutive slots
@@ -165,6 +170,12 @@ __device__ __forceinline__ ListRef list_ref(const ListBufs& l, uint32_t s, int k
     return r;
 }
 
+// Whether a slot's visit list lies within the pair-weight buffer.
+__device__ __forceinline__ bool w_fits(const ListBufs& l, const ListRef& r) {
+    const unsigned long long rows = (r.n + 3u) >> 2;
+    return rows == 0 || (unsigned long long)(r.p - l.pool) + (rows - 1) * r.step + 4u <= l.w_cap;
+}
+
 struct DeviceScalars {
     uint32_t status;
     uint32_t nocc;                  // occupied cells
@@ -172,7 +183,7 @@ struct DeviceScalars {
     uint32_t pad_;                  // scratch flag (state import: a position changed)
     unsigned long long list_used;   // 16-byte groups the last list build asked for
     uint32_t import_bad;            // state import: a non-finite value was found
-    uint32_t pad2_;
+    uint32_t w_short;               // the density pass met a list beyond the pair-weight buffer
 };
 
 // Block size of the per-particle passes: a launch parameter, chosen by the

@@ -287,6 +287,7 @@ World::World(const WorldParams& prm, const WorldConfig& cfg, int dim, double res
         lists_.ncand = alloc<uint32_t>(N);
         insup_ = alloc<uint32_t>(N);
         sc_ = alloc<DeviceScalars>(1);
+        lists_.w_short = &sc_->w_short;
         {
             TankDesc* d_desc = alloc<TankDesc>(n_tanks_);
             uint16_t* d_slot_tank = alloc<uint16_t>(N);
@@ -376,17 +377,27 @@ void World::alloc_lists(unsigned long long groups) {
     lists_.pool_groups = groups;
     lists_.wpair = nullptr;
     lists_.wpair32 = nullptr;
+    lists_.w_cap = 0;
     w_valid_ = false;
-    if (pair_w_on_) alloc_pair_weights();
+    if (pair_w_on_) alloc_pair_weights(pair_weight_groups());
     lists_valid_ = false;
     invalidate_graph();
 }
 
-void World::alloc_pair_weights() {
-    if (pair_weights() || !lists_.pool_groups) return;
+// The list build fills the pool from its start, and a freshly sized pool is
+// twice the need (it grows when a build asks for more than 75%). The buffer
+// covers the pool's first 5/8 (1.25x the need); a build whose lists reach
+// past that is caught by the density pass (w_short: XSPH recomputes W), and
+// the next status poll extends the buffer to the whole pool.
+unsigned long long World::pair_weight_groups() const {
+    return std::min<unsigned long long>(lists_.pool_groups, (lists_.pool_groups * 5ull + 7ull) / 8ull);
+}
+
+void World::alloc_pair_weights(unsigned long long groups) {
+    if (pair_weights() || !groups) return;
     // Kept only with room to spare: the buffer is an optimisation, so it
-    // gives way to the list pool (a 512-tank batch's pool alone is ~69 GB).
-    const size_t bytes = (size_t)lists_.pool_groups * 4u * (f32_ ? sizeof(float) : sizeof(double));
+    // gives way to the list pool (a 512-tank batch's pool alone is ~55 GB).
+    const size_t bytes = (size_t)groups * 4u * (f32_ ? sizeof(float) : sizeof(double));
     constexpr size_t kHeadroom = 2ull << 30;
     size_t free_b = 0, total_b = 0;
     if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess || free_b < bytes + kHeadroom) {
@@ -401,6 +412,7 @@ void World::alloc_pair_weights() {
     list_allocs_.push_back(w);
     if (f32_) lists_.wpair32 = static_cast<float*>(w);
     else lists_.wpair = static_cast<double*>(w);
+    lists_.w_cap = groups * 4ull;
     w_valid_ = false;
 }
 
@@ -416,13 +428,23 @@ void World::free_pair_weights() {
         }
     lists_.wpair = nullptr;
     lists_.wpair32 = nullptr;
+    lists_.w_cap = 0;
     w_valid_ = false;
+}
+
+void World::pair_weight_info(uint64_t out[3]) {
+    DeviceScalars hs{};
+    check(cudaMemcpyAsync(&hs, sc_, sizeof(hs), cudaMemcpyDeviceToHost, st_), "pair weights");
+    check(cudaStreamSynchronize(st_), "pair weights");
+    out[0] = pair_weights() ? 1u : 0u;
+    out[1] = lists_.w_cap;
+    out[2] = pair_weights() && hs.w_short ? 1u : 0u;
 }
 
 void World::set_pair_weights(bool on) {
     if (on == pair_w_on_ && (!on || pair_weights())) return;
     pair_w_on_ = on;
-    if (on) alloc_pair_weights();
+    if (on) alloc_pair_weights(pair_weight_groups());
     else free_pair_weights();
     invalidate_graph();  // a captured step bakes in which XSPH kernel runs
 }
@@ -677,6 +699,7 @@ void World::ensure_lists(bool visit_only) {
 
 void World::run_density(bool visit_only) {
     ensure_lists(visit_only);
+    if (pair_weights()) check(cudaMemsetAsync(&sc_->w_short, 0, sizeof(uint32_t), st_), "memset");
     prof_begin(kDensity);
     if (f32_) launch_density_f32((uint32_t)n_, shape_.density, kf_, cur_, fb_, lists_, st_);
     else launch_density((uint32_t)n_, shape_.density, kc_, cur_, lists_, st_);
@@ -984,6 +1007,7 @@ World::Shapes World::autotune() {
         }
         field = best_t;
     };
+    if (pair_weights()) check(cudaMemsetAsync(&sc_->w_short, 0, sizeof(uint32_t), st_), "memset");
     pick(shape_.density, [&] {
         if (f32_) launch_density_f32(n, shape_.density, kf_, cur_, fb_, lists_, st_);
         else launch_density(n, shape_.density, kc_, cur_, lists_, st_);
@@ -1046,6 +1070,13 @@ uint32_t World::status() {
     if (hs.list_used * 4 > lists_.pool_groups * 3 && lists_.pool_groups < kMaxListGroups) {
         alloc_lists(2 * hs.list_used);
         lists_checked_ = false;
+    }
+    // Pair weights that a density pass found too short cover the whole pool
+    // from now on (XSPH recomputed W meanwhile).
+    if (hs.w_short && pair_w_on_ && lists_.w_cap < lists_.pool_groups * 4ull) {
+        free_pair_weights();
+        alloc_pair_weights(lists_.pool_groups);
+        invalidate_graph();
     }
     // Grow the shared-memory stage of the list build when the fluid has
     // packed more particles into a neighbourhood than it holds.

@@ -143,6 +143,9 @@ class World {
     // In the f64 step the bits are the same either way.
     void set_pair_weights(bool on);
     bool pair_weights() const { return lists_.wpair != nullptr || lists_.wpair32 != nullptr; }
+    // {in use, list entries the buffer covers, the last density pass met a
+    // list beyond them}; synchronises the stream
+    void pair_weight_info(uint64_t out[3]);
 
     // ---- learned surrogate (surrogate.cuh) ----
     // One step with the network's acceleration and density rate in place of
@@ -258,8 +261,9 @@ class World {
     bool lists_valid_ = false;   // neighbour lists match the grid and positions
     bool pair_w_on_ = false;     // keep lists_.wpair (set_pair_weights)
     bool w_valid_ = false;       // lists_.wpair holds W of the current lists and positions
-    void alloc_pair_weights();
+    void alloc_pair_weights(unsigned long long groups);
     void free_pair_weights();
+    unsigned long long pair_weight_groups() const;
     bool lists_checked_ = false; // list capacity verified for the current positions
     bool lists_sized_ = false;   // the first list sizing has been done
     bool lists_full_ = false;    // the last build wrote upper and lower lists too

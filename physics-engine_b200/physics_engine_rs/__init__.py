@@ -226,6 +226,7 @@ def load_library():
         "pe_fluid_wcsph_list_chunk": (C.c_int, [vp, C.POINTER(C.c_uint32)]),
         "pe_fluid_wcsph_set_pair_weights": (C.c_int, [vp, C.c_int32]),
         "pe_fluid_wcsph_pair_weights": (C.c_int, [vp, C.POINTER(C.c_int32)]),
+        "pe_fluid_wcsph_pair_weight_info": (C.c_int, [vp, vp]),
         "pe_fluid_wcsph_kernel_launches": (C.c_int, [vp, C.POINTER(u64), i32]),
         "pe_fluid_wcsph_profile": (C.c_int, [vp, i32]),
         "pe_fluid_wcsph_profile_read": (C.c_int, [vp, C.POINTER(_Profile), i32]),
@@ -601,6 +602,13 @@ class WcsphWorld:
         c = C.c_int32(0)
         _ok(_lib.pe_fluid_wcsph_pair_weights(self._w, C.byref(c)), "pair_weights")
         return bool(c.value)
+
+    def pair_weight_info(self) -> dict:
+        """{in_use, entries (list entries the buffer covers), short (the last
+        density pass met a list beyond them, so XSPH recomputed W)}."""
+        out = np.zeros(3, np.uint64)
+        _ok(_lib.pe_fluid_wcsph_pair_weight_info(self._w, _ptr(out)), "pair_weight_info")
+        return {"in_use": bool(out[0]), "entries": int(out[1]), "short": bool(out[2])}
 
     def close(self):
         if getattr(self, "_w", None) and _lib is not None:

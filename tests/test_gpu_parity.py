@@ -114,6 +114,41 @@ def test_pair_weights_on_and_off_bit_exact():
     assert w.status() == 0
 
 
+def test_pair_weights_outgrown_by_the_lists_bit_exact():
+    """A lattice spaced 1.25 dx with the mass of dx collapses: its lists grow
+    by ~75% in 40 steps, past the pair-weight buffer (1.25x the lists the pool
+    was sized for; a small first guess of the pool makes the first build size
+    it to twice the need). A density pass that meets lists beyond the buffer
+    keeps no weights and XSPH recomputes W; the status poll of each step()
+    then extends the buffer. The state follows the oracle bit for bit
+    throughout."""
+    dx = 0.01
+    rho0, mass = 1000.0, pe.mass_from_spacing(1000.0, dx, 3)
+    ps = pe.Particles(3, rho0, mass, 2 * dx)
+    os_ = O.Scene(3, rho0, mass, 2 * dx)
+    for s in (ps, os_):
+        s.fill_box((dx, dx, dx), 12, 8, 8, 1.25 * dx)
+        s.fill_box_boundary((0.0, 0.0, 0.0), (0.3, 0.15, 0.2), dx, 1)
+    w = pe.WcsphWorld(ps, dam_break_params_pe(False), pe.WcsphConfig(max_neighbours=16))
+    o = O.World(os_, O.dam_break_params(materialize=False))
+    w.step(1e-4)
+    o.step(1e-4)
+    info0 = w.pair_weight_info()
+    assert info0["in_use"] and not info0["short"]
+    short_steps, grew = 0, False
+    for k in range(1, 45):
+        w.step(1e-4)
+        o.step(1e-4)
+        info = w.pair_weight_info()
+        short_steps += info["short"]
+        grew = grew or info["entries"] > info0["entries"]
+        if k in (20, 44):
+            _compare_state(w, o, f"collapse step {k + 1}")
+    assert short_steps > 0 and grew
+    assert w.pair_weights()
+    assert w.status() & ~pe.STATUS_SLOW_UNION == 0
+
+
 def test_adaptive_sound_speed_bit_exact():
     """compute_pressure's c = max(c, 10 v_max), persisted (wcsph.rs:158-169).
     With the rule on, the free-surface start accelerates quickly (c grows each
