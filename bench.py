@@ -469,6 +469,7 @@ def run_batched(args, ws, rank, local, torch, pe):
     launches = w.kernel_launches()
     status = w.status()
     cap = w.capacity_info()
+    pair_weights = w.pair_weights()
     ms = max_over_ranks(ms, torch)
     value = job_throughput(nf, args.steps, ms, ws)
     w.close()
@@ -509,7 +510,7 @@ def run_batched(args, ws, rank, local, torch, pe):
         "gpu_launches": int(launches), "status": int(status),
         "neighbour_lists": {"used_gb": cap["list_groups_used"] * 16 / 1e9,
                             "pool_gb": cap["list_groups_capacity"] * 16 / 1e9,
-                            "pair_weights": w.pair_weights()},
+                            "pair_weights": pair_weights},
         "per_tank_loop": {"value": loop_value, "unit": UNIT, "tanks_timed": len(sample),
                           "fluid_particles_timed": loop_nf,
                           "how": "single-tank worlds stepped one after another, same steps"},
