@@ -799,14 +799,14 @@ void World::run_xsph() {
     if (f32_) {
         launch_xsph_f32((uint32_t)n_, shape_.xsph, kf_, cur_, fb_, lists_, velf_alt_, st_, w_valid_);
         prof_end();
-        launches_ += 1;
+        launches_ += w_valid_ ? 2 : 1;  // with weights: the weight-reading kernel and its fallback
         check(cudaGetLastError(), "xsph");
         std::swap(fb_.vel, velf_alt_);
         return;
     }
     launch_xsph((uint32_t)n_, shape_.xsph, kc_, cur_, lists_, vel_nx_, st_, w_valid_);
     prof_end();
-    launches_ += 1;
+    launches_ += w_valid_ ? 2 : 1;  // with weights: the weight-reading kernel and its fallback
     check(cudaGetLastError(), "xsph");
     std::swap(cur_.vel, vel_nx_);
     // the swapped-out buffer of the alternate state must stay a valid full copy
