@@ -1052,6 +1052,7 @@ World::Shapes World::autotune() {
         check(cudaMemsetAsync(&sc_->list_used, 0, sizeof(unsigned long long), st_), "memset");
         launch_nlist(g_, tanks_, kc_, ucap_, nl_blocks_, occ_, cell_start_, cur_, lists_, sc_, st_, !lists_full_,
                      list_chunk_);
+        w_valid_ = false;  // the pair weights follow the old layout
     }
     check(cudaGetLastError(), "autotune");
     event_pool_.push_back(a);

@@ -114,6 +114,23 @@ def test_pair_weights_on_and_off_bit_exact():
     assert w.status() == 0
 
 
+def test_autotune_between_density_and_xsph_bit_exact():
+    """The autotuner rebuilds the lists in the shape it picks, which moves
+    them in the pool: the pair weights the density pass kept no longer match,
+    and the XSPH pass after it must recompute W."""
+    w, o = _pair(**SMALL)
+    for name in ("rebuild_grid", "compute_density"):
+        getattr(w, name)()
+        getattr(o, name)()
+    w.autotune()
+    w.apply_xsph()
+    o.apply_xsph()
+    assert_bits_equal(w.velocities(), o.v(), "xsph after autotune")
+    w.step(1e-4)
+    o.step(1e-4)
+    _compare_state(w, o, "step after autotune")
+
+
 def test_pair_weights_outgrown_by_the_lists_bit_exact():
     """A lattice spaced 1.25 dx with the mass of dx collapses: its lists grow
     by ~75% in 40 steps, past the pair-weight buffer (1.25x the lists the pool
