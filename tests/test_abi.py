@@ -205,3 +205,24 @@ def test_rng_uniform_is_the_jitter_generator():
     p.push_fluid((0.0, 0.0, 0.0))
     p.jitter_fluid(0x5EED5EED, 1e-4)
     assert np.array_equal(p.arrays()["x"][0], u)
+
+
+def test_handle_entry_points_reject_null_handles():
+    """pe-ffi convention: a NULL handle is PE_ERR_NULL, checked before any
+    device work (so it holds on a machine without a GPU)."""
+    lib = C.CDLL(pe.library_path())
+    out = (C.c_uint64 * 8)()
+    i32 = C.c_int32(0)
+    u32 = C.c_uint32(0)
+    calls = [
+        (lib.pe_fluid_wcsph_set_pair_weights, (None, C.c_int32(1))),
+        (lib.pe_fluid_wcsph_pair_weights, (None, C.byref(i32))),
+        (lib.pe_fluid_wcsph_pair_weight_info, (None, out)),
+        (lib.pe_fluid_wcsph_list_chunk, (None, C.byref(u32))),
+        (lib.pe_fluid_wcsph_step, (None, C.c_double(1e-4))),
+        (lib.pe_fluid_wcsph_run, (None, C.c_double(1e-4), C.c_uint64(1))),
+        (lib.pe_fluid_wcsph_shapes, (None, out)),
+    ]
+    for fn, args in calls:
+        fn.restype = C.c_int
+        assert fn(*args) == pe.PE_ERR_NULL, fn.__name__
