@@ -54,11 +54,16 @@ __device__ __forceinline__ float dwdr_over_r_f32(float r, float inv_r, const F32
     return dwdq * k.inv_h * inv_r;
 }
 
-__device__ __forceinline__ float3 rel(const int4& ki, const float4& pi, const int4& kj,
-                                      const float4& pj, float cell) {
-    return make_float3((float)(kj.x - ki.x) * cell + (pj.x - pi.x),
-                       (float)(kj.y - ki.y) * cell + (pj.y - pi.y),
-                       (float)(kj.z - ki.z) * cell + (pj.z - pi.z));
+// The pair vector x_j - x_i of two particles in the same or adjacent cells:
+// their keys differ by -1, 0 or 1 per axis, which the keys mod 4 (cm, two
+// bits per axis) determine, so a neighbour's full key need not be read.
+__device__ __forceinline__ float3 rel(uint32_t ci, const float4& pi, uint32_t cj, const float4& pj,
+                                      float cell) {
+    const int dx = (int)(((cj & 3u) - (ci & 3u) + 1u) & 3u) - 1;
+    const int dy = (int)((((cj >> 2) & 3u) - ((ci >> 2) & 3u) + 1u) & 3u) - 1;
+    const int dz = (int)((((cj >> 4) & 3u) - ((ci >> 4) & 3u) + 1u) & 3u) - 1;
+    return make_float3((float)dx * cell + (pj.x - pi.x), (float)dy * cell + (pj.y - pi.y),
+                       (float)dz * cell + (pj.z - pi.z));
 }
 
 // particles.rs:126 boundary_sees_fluid for an oriented sample b seen from a
@@ -74,7 +79,7 @@ __device__ __forceinline__ bool sees_fluid_f32(const F32Const& k, const double4&
 // A neighbour's loop state, gathered one entry ahead of its use.
 struct Nb32 {
     float4 p;
-    int4 key;
+    uint32_t km;  // cell key mod 4 (F32Bufs.kmod)
     float4 v;
 };
 
@@ -87,7 +92,7 @@ __global__ void __launch_bounds__(kMaxPassThreads) k_density_f32(uint32_t n, F32
         return;
     }
     const float4 pi = f.pos[i];
-    const int4 ki = s.key[i];
+    const uint32_t ci = f.kmod[i];
     Kahan rho;
     rho.add(k.rho_self);
     const ListRef vr = list_ref(l, i, kListVisit);
@@ -105,12 +110,12 @@ __global__ void __launch_bounds__(kMaxPassThreads) k_density_f32(uint32_t n, F32
         [&](uint32_t, uint32_t e) {
             Nb32 b;
             b.p = f.pos[e & kEntrySlotMask];
-            b.key = s.key[e & kEntrySlotMask];
+            b.km = f.kmod[e & kEntrySlotMask];
             return b;
         },
         [&](uint32_t t, uint32_t e, const Nb32& b) {
             const float4 pj = b.p;
-            const float3 d = rel(ki, pi, b.key, pj, k.cell);
+            const float3 d = rel(ci, pi, b.km, pj, k.cell);
             const float r = sqrtf(d.x * d.x + d.y * d.y + d.z * d.z);
             const float w = w_f32(r, k);
             if (keep_w) {
@@ -203,18 +208,19 @@ __global__ void __launch_bounds__(kMaxPassThreads) k_forces_f32(uint32_t n, F32C
     const float4 pi = f.pos[i];
     const float4 vi = f.vel[i];
     const int4 ki = s.key[i];
+    const uint32_t ci = f.kmod[i];
     Kahan ax, ay, az;
     auto load = [&](uint32_t e) {
         Nb32 b;
         b.p = f.pos[e & kEntrySlotMask];
-        b.key = s.key[e & kEntrySlotMask];
+        b.km = f.kmod[e & kEntrySlotMask];
         b.v = f.vel[e & kEntrySlotMask];
         return b;
     };
     for_each_loaded(list_ref(l, i, kListVisit), load, [&](uint32_t e, const Nb32& b) {
         const uint32_t j = e & kEntrySlotMask;
         const float4 pj = b.p;
-        const float3 d = rel(ki, pi, b.key, pj, k.cell);  // x_j - x_i
+        const float3 d = rel(ci, pi, b.km, pj, k.cell);  // x_j - x_i
         const float r2 = d.x * d.x + d.y * d.y + d.z * d.z;
         if (r2 < 1e-30f) return;
         const float inv_r = rsqrtf(r2);
@@ -276,13 +282,13 @@ __global__ void __launch_bounds__(kMaxPassThreads) k_xsph_f32(uint32_t n, F32Con
         return;
     }
     const float4 pi = f.pos[i];
-    const int4 ki = s.key[i];
+    const uint32_t ci = f.kmod[i];
     Kahan dx, dy, dz;
     auto load = [&](uint32_t e) {
         Nb32 b{};
         if (!(e & kEntryBoundary)) {
             b.p = f.pos[e & kEntrySlotMask];
-            b.key = s.key[e & kEntrySlotMask];
+            b.km = f.kmod[e & kEntrySlotMask];
             b.v = f.vel[e & kEntrySlotMask];
         }
         return b;
@@ -290,7 +296,7 @@ __global__ void __launch_bounds__(kMaxPassThreads) k_xsph_f32(uint32_t n, F32Con
     for_each_loaded(list_ref(l, i, kListVisit), load, [&](uint32_t e, const Nb32& b) {
         if (e & kEntryBoundary) return;
         const float4 pj = b.p;
-        const float3 d = rel(ki, pi, b.key, pj, k.cell);
+        const float3 d = rel(ci, pi, b.km, pj, k.cell);
         const float r = sqrtf(d.x * d.x + d.y * d.y + d.z * d.z);
         const float w = w_f32(r, k);
         const float4 vj = b.v;
@@ -357,6 +363,7 @@ __global__ void k_f32_from_f64(uint32_t n, double cell, StateBufs s, F32Bufs f) 
     const bool fluid = !(s.flags[i] & kFlagBoundary);
     f.pos[i] = make_float4((float)(p.x - (double)kk.x * cell), (float)(p.y - (double)kk.y * cell),
                            (float)(p.z - (double)kk.z * cell), fluid ? 0.f : (float)p.w);
+    f.kmod[i] = (uint8_t)(((uint32_t)kk.x & 3u) | (((uint32_t)kk.y & 3u) << 2) | (((uint32_t)kk.z & 3u) << 4));
     const double4 v = s.vel[i];
     f.vel[i] = make_float4((float)v.x, (float)v.y, (float)v.z, (float)v.w);
 }

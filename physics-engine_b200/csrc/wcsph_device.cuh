@@ -210,6 +210,7 @@ struct F32Const {
 struct F32Bufs {
     float4* pos;  // cell-local position, w = p / rho^2 (fluid) or psi (boundary)
     float4* vel;  // velocity, w = rho
+    uint8_t* kmod;  // cell key mod 4 per axis, two bits each (x | y << 2 | z << 4)
 };
 
 void launch_f32_from_f64(uint32_t n, double cell, const StateBufs& s, const F32Bufs& f,

@@ -317,6 +317,7 @@ World::World(const WorldParams& prm, const WorldConfig& cfg, int dim, double res
         if (f32_) {
             fb_.pos = alloc<float4>(N);
             fb_.vel = alloc<float4>(N);
+            fb_.kmod = alloc<uint8_t>(N);
             velf_alt_ = alloc<float4>(N);
             bf32_ = alloc<float>(4 * N);
         }
